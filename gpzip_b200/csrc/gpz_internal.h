@@ -1,0 +1,97 @@
+// gpz_internal.h -- layouts shared by the sm_100a kernels and the host runtime.
+//
+// A batch is a list of members (independent gzip members, 128 KiB each in
+// parity mode, as gpu.rs:150-160 and gpu.rs:193-208 of the reference cut
+// them).  Every member is split into 4 KiB tiles, which are both the
+// reference's hash segments (lz77_hash.rs:64-69, SEG_LOG2 = 12) and the unit
+// of the walk / encode stages.
+#pragma once
+#include <cstdint>
+
+#define GPZ_SEG_LOG2 12
+#define GPZ_SEG (1u << GPZ_SEG_LOG2)
+#define GPZ_WIN_SEGS 9                      // own segment + 8 back (window-bound proof)
+#define GPZ_WIN_BYTES (GPZ_WIN_SEGS * GPZ_SEG + 320)
+#define GPZ_KEY_SLOTS 8192
+#define GPZ_MAX_MATCH 258u
+#define GPZ_WINDOW 32768u
+#define GPZ_NLIT 286
+#define GPZ_NDIST 30
+#define GPZ_NSYM (GPZ_NLIT + GPZ_NDIST)
+#define GPZ_EXITS 258                       // entry offsets a walk can have into a tile
+#define GPZ_MAX_HEADER_WORDS 160            // dynamic block header <= 4498 bits
+
+// Status words of the decoupled look-backs.
+#define GPZ_ST_AGG 0x40000000u
+#define GPZ_ST_INCL 0x80000000u
+#define GPZ_ST_MASK 0xC0000000u
+
+// Error bits reported through BatchParams::err.
+#define GPZ_ERRBIT_SPIN 1u      // a bounded look-back wait expired
+#define GPZ_ERRBIT_BITS 2u      // emitted bit count disagreed with the plan
+#define GPZ_ERRBIT_HUFF 4u      // code construction failed (never expected)
+
+struct MemberDesc {
+    uint64_t in_off;     // first input byte of the member in the batch input (16-byte aligned)
+    uint32_t len;        // member length in bytes
+    uint32_t tile_base;  // index of the member's first tile
+    uint32_t ntiles;     // ceil(len / 4096)
+    uint32_t level;      // accepted and ignored, as the reference GPU codec does (gpu.rs:223)
+    uint64_t out_slot;   // caller-visible ordinal (used by the serving queue)
+};
+
+struct TileDesc {
+    uint32_t member;
+    uint32_t seg;
+};
+
+struct MemberOut {
+    uint64_t gz_off;         // byte offset of this member's gzip member in the batch output
+    uint32_t deflate_bytes;  // DEFLATE payload bytes
+    uint32_t crc;            // CRC-32 of the member input
+    uint32_t total_bits;     // DEFLATE bits incl. header and EOB
+    uint32_t header_bits;
+    uint32_t len;            // ISIZE (member input length)
+    uint32_t pad;
+};
+
+// Everything a batch launch needs; passed by value to every kernel.
+struct BatchParams {
+    const uint8_t* in;
+    const MemberDesc* members;
+    const TileDesc* tiles;
+    uint32_t* pp;             // per-position packed tokens, indexed like `in`
+    uint32_t* tok;            // walked tokens, tile-sparse, indexed like `in`
+    uint32_t* out_words;      // gzip stream of the batch, as 32-bit words
+    uint32_t* tile_status;    // walk look-back status per tile
+    uint16_t* tile_exit;      // [tile][GPZ_EXITS] exit offset into the next tile
+    uint16_t* tile_hist;      // [tile][GPZ_NSYM] symbol counts of the tile's tokens
+    uint32_t* tile_ntok;      // tokens per tile
+    uint32_t* tile_crc;       // zero-init CRC of each tile's bytes
+    uint32_t* tile_bitoff;    // tile's first token bit within its member's DEFLATE stream
+    uint32_t* member_codes;   // [member][GPZ_NSYM] reversed code | len << 16
+    MemberOut* member_out;
+    unsigned long long* member_status;  // output look-back: flag<<62 | value
+    uint32_t* counters;       // [0..3] tile claims per stage, [4] member claims
+    uint32_t* err;
+    uint32_t nmembers;
+    uint32_t ntiles;
+    uint64_t out_base;        // byte offset added to every member's gz_off
+};
+
+enum { GPZ_CNT_LOOKUP = 0, GPZ_CNT_WALK = 1, GPZ_CNT_HUFF = 2, GPZ_CNT_EMIT = 3, GPZ_NCOUNTERS = 8 };
+
+// Per-stage launch geometry chosen by the autotuner (threads per CTA, CTAs).
+struct LaunchShape {
+    int lookup_threads;
+    int lookup_grid;   // 0 = one CTA per tile
+    int walk_threads;
+    int walk_grid;
+    int emit_threads;
+    int emit_grid;
+};
+
+// Kernel launchers (gpz_kernels.cu).
+int gpz_launch_batch(const BatchParams& bp, const LaunchShape& ls, void* stream);
+int gpz_kernel_smem_setup();
+size_t gpz_lookup_smem_bytes();

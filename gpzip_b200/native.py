@@ -1,0 +1,260 @@
+"""ctypes binding of the C ABI in include/gpz.h (libgpz.so, built for sm_100a).
+
+There is no fallback: if the shared library is missing or no CUDA device is
+usable, loading or creating a context raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgpz.so")
+
+GPZ_OK = 0
+STATUS = {0: "GPZ_OK", 1: "GPZ_E_NOMEM", 2: "GPZ_E_ADMISSION", 3: "GPZ_E_TIMEOUT", 4: "GPZ_E_CUDA",
+          5: "GPZ_E_ARG", 6: "GPZ_E_SPACE", 7: "GPZ_E_INTERNAL", 8: "GPZ_E_BUSY", 9: "GPZ_E_PENDING"}
+GPZ_E_PENDING = 9
+GPZ_E_BUSY = 8
+GPZ_FLAG_NO_GRAPHS = 1
+GPZ_FLAG_NO_AUTOTUNE = 2
+
+# Every symbol include/gpz.h declares.
+EXPORTS = [
+    "gpz_config_default", "gpz_create", "gpz_destroy", "gpz_bound", "gpz_bound_ctx", "gpz_compress_chunk",
+    "gpz_compress_batch", "gpz_compress_batch_plain", "gpz_compress_device", "gpz_frame_host",
+    "gpz_debug_chunk", "gpz_submit", "gpz_poll", "gpz_serve_stats_get", "gpz_strerror", "gpz_last_error",
+    "gpz_get_shape", "gpz_set_shape", "gpz_last_launches",
+]
+
+
+class GpzError(RuntimeError):
+    def __init__(self, status: int, msg: str = ""):
+        self.status = status
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+
+
+class Config(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("member_bytes", ctypes.c_size_t), ("pool_bytes", ctypes.c_size_t),
+                ("batch_bytes", ctypes.c_size_t), ("streams", ctypes.c_int), ("flags", ctypes.c_int)]
+
+
+class Desc(ctypes.Structure):
+    _fields_ = [("in_", ctypes.c_void_p), ("n", ctypes.c_size_t), ("level", ctypes.c_int)]
+
+
+class Out(ctypes.Structure):
+    _fields_ = [("out", ctypes.c_void_p), ("out_cap", ctypes.c_size_t), ("out_len", ctypes.c_size_t),
+                ("status", ctypes.c_int)]
+
+
+class Shape(ctypes.Structure):
+    _fields_ = [("lookup_threads", ctypes.c_int), ("lookup_grid", ctypes.c_int), ("walk_threads", ctypes.c_int),
+                ("walk_grid", ctypes.c_int), ("emit_threads", ctypes.c_int), ("emit_grid", ctypes.c_int)]
+
+
+class ServeStats(ctypes.Structure):
+    _fields_ = [("completed", ctypes.c_uint64), ("rejected", ctypes.c_uint64), ("batches", ctypes.c_uint64),
+                ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double), ("p999_ms", ctypes.c_double),
+                ("max_queue_ms", ctypes.c_double), ("bytes_in", ctypes.c_uint64), ("bytes_out", ctypes.c_uint64)]
+
+
+_lib = None
+
+
+def load(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Load libgpz.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing: build it with `python -m gpzip_b200.build`")
+    L = ctypes.CDLL(path)
+    vp, sz, u64p = ctypes.c_void_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_uint64)
+    L.gpz_config_default.argtypes = [ctypes.POINTER(Config)]
+    L.gpz_config_default.restype = None
+    L.gpz_create.argtypes = [ctypes.POINTER(Config), ctypes.POINTER(vp)]
+    L.gpz_create.restype = ctypes.c_int
+    L.gpz_destroy.argtypes = [vp]
+    L.gpz_destroy.restype = None
+    L.gpz_bound.argtypes = [sz]
+    L.gpz_bound.restype = sz
+    L.gpz_bound_ctx.argtypes = [vp, sz]
+    L.gpz_bound_ctx.restype = sz
+    L.gpz_compress_chunk.argtypes = [vp, vp, sz, ctypes.c_int, vp, sz, ctypes.POINTER(sz)]
+    L.gpz_compress_chunk.restype = ctypes.c_int
+    L.gpz_compress_batch.argtypes = [vp, ctypes.POINTER(Desc), sz, ctypes.POINTER(Out)]
+    L.gpz_compress_batch.restype = ctypes.c_int
+    L.gpz_compress_batch_plain.argtypes = [vp, ctypes.POINTER(Desc), sz, ctypes.POINTER(Out)]
+    L.gpz_compress_batch_plain.restype = ctypes.c_int
+    L.gpz_compress_device.argtypes = [vp, vp, u64p, u64p, sz, vp, sz, u64p, vp]
+    L.gpz_compress_device.restype = ctypes.c_int
+    L.gpz_frame_host.argtypes = [vp, vp, sz]
+    L.gpz_frame_host.restype = ctypes.c_int
+    L.gpz_debug_chunk.argtypes = [vp, vp, sz, vp, vp, ctypes.POINTER(sz), vp, sz, ctypes.POINTER(sz)]
+    L.gpz_debug_chunk.restype = ctypes.c_int
+    L.gpz_submit.argtypes = [vp, ctypes.POINTER(Desc), ctypes.POINTER(ctypes.c_uint64)]
+    L.gpz_submit.restype = ctypes.c_int
+    L.gpz_poll.argtypes = [vp, ctypes.c_uint64, ctypes.POINTER(Out), ctypes.c_int]
+    L.gpz_poll.restype = ctypes.c_int
+    L.gpz_serve_stats_get.argtypes = [vp, ctypes.POINTER(ServeStats)]
+    L.gpz_serve_stats_get.restype = ctypes.c_int
+    L.gpz_strerror.argtypes = [ctypes.c_int]
+    L.gpz_strerror.restype = ctypes.c_char_p
+    L.gpz_last_error.argtypes = [vp]
+    L.gpz_last_error.restype = ctypes.c_char_p
+    L.gpz_get_shape.argtypes = [vp, ctypes.POINTER(Shape)]
+    L.gpz_get_shape.restype = ctypes.c_int
+    L.gpz_set_shape.argtypes = [vp, ctypes.POINTER(Shape)]
+    L.gpz_set_shape.restype = ctypes.c_int
+    L.gpz_last_launches.argtypes = [vp]
+    L.gpz_last_launches.restype = ctypes.c_uint64
+    _lib = L
+    return L
+
+
+def _u8(data) -> np.ndarray:
+    if isinstance(data, np.ndarray):
+        return np.ascontiguousarray(data, dtype=np.uint8).reshape(-1)
+    return np.frombuffer(bytes(data), dtype=np.uint8)
+
+
+def _p(a: np.ndarray):
+    return ctypes.c_void_p(a.ctypes.data) if a.size else ctypes.c_void_p(0)
+
+
+class Context:
+    """One gpz_ctx (device pool, streams, launch shapes) on one CUDA device."""
+
+    def __init__(self, device: int = 0, member_bytes: int = 128 * 1024, pool_bytes: int = 0,
+                 batch_bytes: int = 0, flags: int = 0):
+        L = load()
+        cfg = Config()
+        L.gpz_config_default(ctypes.byref(cfg))
+        cfg.device, cfg.member_bytes, cfg.pool_bytes = device, member_bytes, pool_bytes
+        cfg.batch_bytes, cfg.flags = batch_bytes, flags
+        h = ctypes.c_void_p()
+        rc = L.gpz_create(ctypes.byref(cfg), ctypes.byref(h))
+        if rc != GPZ_OK:
+            raise GpzError(rc, "gpz_create")
+        self._h = h
+        self.member_bytes = member_bytes
+        self.L = L
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.L.gpz_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc: int, what: str):
+        if rc != GPZ_OK:
+            raise GpzError(rc, f"{what}: {self.L.gpz_last_error(self._h).decode()}")
+
+    def bound(self, n: int) -> int:
+        return self.L.gpz_bound_ctx(self._h, n)
+
+    def compress_chunk(self, data, level: int = 5) -> bytes:
+        a = _u8(data)
+        cap = self.bound(a.size)
+        out = np.empty(cap, dtype=np.uint8)
+        n = ctypes.c_size_t()
+        self._check(self.L.gpz_compress_chunk(self._h, _p(a), a.size, level, _p(out), cap, ctypes.byref(n)),
+                    "gpz_compress_chunk")
+        return out[:n.value].tobytes()
+
+    def _batch(self, fn, items, level: int = 5):
+        arrs = [_u8(x) for x in items]
+        k = len(arrs)
+        descs = (Desc * max(k, 1))()
+        outs = (Out * max(k, 1))()
+        bufs = []
+        for i, a in enumerate(arrs):
+            descs[i].in_ = a.ctypes.data if a.size else None
+            descs[i].n = a.size
+            descs[i].level = level
+            b = np.empty(self.bound(a.size), dtype=np.uint8)
+            bufs.append(b)
+            outs[i].out = b.ctypes.data
+            outs[i].out_cap = b.size
+        self._check(fn(self._h, descs, k, outs), fn.__name__)
+        return [bufs[i][:outs[i].out_len].tobytes() for i in range(k)]
+
+    def compress_batch(self, items, level: int = 5):
+        return self._batch(self.L.gpz_compress_batch, items, level)
+
+    def compress_batch_plain(self, items, level: int = 5):
+        return self._batch(self.L.gpz_compress_batch_plain, items, level)
+
+    def debug_chunk(self, data):
+        """(pp, tokens, gzip bytes) of one chunk through the device path."""
+        a = _u8(data)
+        pp = np.zeros(max(a.size, 1), dtype=np.uint32)
+        tok = np.zeros(max(a.size, 1), dtype=np.uint32)
+        ntok = ctypes.c_size_t()
+        cap = self.bound(a.size)
+        out = np.empty(cap, dtype=np.uint8)
+        olen = ctypes.c_size_t()
+        self._check(self.L.gpz_debug_chunk(self._h, _p(a), a.size, _p(pp), _p(tok), ctypes.byref(ntok), _p(out),
+                                           cap, ctypes.byref(olen)), "gpz_debug_chunk")
+        return pp[:a.size], tok[:ntok.value], out[:olen.value].tobytes()
+
+    def compress_device(self, d_in: int, offs, lens, d_out: int, out_cap: int, stream: int = 0):
+        """Device-resident pass; returns (count+1) output offsets."""
+        k = len(offs)
+        o = (ctypes.c_uint64 * k)(*offs)
+        l = (ctypes.c_uint64 * k)(*lens)
+        r = (ctypes.c_uint64 * (k + 1))()
+        self._check(self.L.gpz_compress_device(self._h, ctypes.c_void_p(d_in), o, l, k, ctypes.c_void_p(d_out),
+                                               out_cap, r, ctypes.c_void_p(stream or None)), "gpz_compress_device")
+        return list(r)
+
+    def frame_host(self, host_out: np.ndarray):
+        self._check(self.L.gpz_frame_host(self._h, _p(host_out), host_out.size), "gpz_frame_host")
+
+    def get_shape(self) -> Shape:
+        s = Shape()
+        self._check(self.L.gpz_get_shape(self._h, ctypes.byref(s)), "gpz_get_shape")
+        return s
+
+    def set_shape(self, s: Shape):
+        self._check(self.L.gpz_set_shape(self._h, ctypes.byref(s)), "gpz_set_shape")
+
+    def last_launches(self) -> int:
+        return self.L.gpz_last_launches(self._h)
+
+    def submit(self, data, level: int = 5) -> int:
+        a = _u8(data)
+        d = Desc(a.ctypes.data if a.size else None, a.size, level)
+        t = ctypes.c_uint64()
+        rc = self.L.gpz_submit(self._h, ctypes.byref(d), ctypes.byref(t))
+        if rc != GPZ_OK:
+            raise GpzError(rc, "gpz_submit")
+        return t.value
+
+    def poll(self, ticket: int, cap: int, wait_ms: int = 0):
+        buf = np.empty(cap, dtype=np.uint8)
+        o = Out(buf.ctypes.data, cap, 0, 0)
+        rc = self.L.gpz_poll(self._h, ticket, ctypes.byref(o), wait_ms)
+        if rc == GPZ_E_PENDING:
+            return None
+        self._check(rc, "gpz_poll")
+        return buf[:o.out_len].tobytes()
+
+    def serve_stats(self) -> dict:
+        s = ServeStats()
+        self._check(self.L.gpz_serve_stats_get(self._h, ctypes.byref(s)), "gpz_serve_stats_get")
+        return {f: getattr(s, f) for f, _ in ServeStats._fields_}

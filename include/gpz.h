@@ -1,0 +1,168 @@
+/*
+ * gpz.h -- C ABI of the B200 (sm_100a) gzip compression path.
+ *
+ * Drop-in boundary for the reference's chunk-codec interface
+ * (skmtkytr/gpzip):
+ *   - ChunkFn = Arc<dyn Fn(&[u8]) -> io::Result<Vec<u8>>>
+ *       crates/gpzip-codec-cpu/src/parallel.rs:21
+ *   - GpuBackend::gzip_chunk_fn / encode_one
+ *       crates/gpzip-codec-gpu/src/gpu.rs:193-208, 271-287
+ *   - BatchedLz77::submit (the batching channel this replaces)
+ *       crates/gpzip-codec-gpu/src/gpu/batch.rs:74-85
+ * Plain pointers and sizes only; no CUDA or torch types cross the boundary.
+ *
+ * Output of every compress call is a concatenation of RFC 1952 gzip members,
+ * one per `member_bytes` slice of the input (131072 by default, matching
+ * GpuBackend's chunk_size at gpu.rs:160), each carrying one dynamic-Huffman
+ * RFC 1951 block whose bytes equal the reference's encode_block_fast output
+ * for the reference's segmented-hash + lazy-walk tokens.
+ *
+ * Errors are status codes, never aborts.  All entry points are thread safe.
+ * There is no CPU fallback: without a usable CUDA device gpz_create fails.
+ */
+#ifndef GPZ_H
+#define GPZ_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define GPZ_API __attribute__((visibility("default")))
+#else
+#define GPZ_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define GPZ_OK 0
+#define GPZ_E_NOMEM 1       /* device or pinned allocation failed */
+#define GPZ_E_ADMISSION 2   /* request does not fit the device pool cap */
+#define GPZ_E_TIMEOUT 3     /* a bounded device wait expired */
+#define GPZ_E_CUDA 4        /* CUDA runtime error */
+#define GPZ_E_ARG 5         /* invalid argument */
+#define GPZ_E_SPACE 6       /* output buffer too small */
+#define GPZ_E_INTERNAL 7    /* device self-check failed (bit plan mismatch) */
+#define GPZ_E_BUSY 8        /* serving queue full, retry later */
+#define GPZ_E_PENDING 9     /* ticket not finished yet */
+
+typedef struct gpz_ctx gpz_ctx;
+
+typedef struct gpz_config {
+    int device;            /* CUDA device ordinal */
+    size_t member_bytes;   /* input bytes per gzip member: 131072 (default, the reference's
+                              sub-chunk) up to 2097152 (whole-chunk mode); multiple of 4096 */
+    size_t pool_bytes;     /* device pool cap in bytes (0: 40 GiB) */
+    size_t batch_bytes;    /* input bytes per device pass (0: 256 MiB) */
+    int streams;           /* reserved (0) */
+    int flags;             /* GPZ_FLAG_* */
+} gpz_config;
+
+#define GPZ_FLAG_NO_GRAPHS 1    /* launch kernels directly instead of per-bucket CUDA graphs */
+#define GPZ_FLAG_NO_AUTOTUNE 2  /* keep the default launch shapes */
+
+typedef struct gpz_desc {
+    const uint8_t* in;   /* one chunk or file */
+    size_t n;
+    int level;           /* accepted and ignored, as the reference GPU codec does (gpu.rs:223) */
+} gpz_desc;
+
+typedef struct gpz_out {
+    uint8_t* out;        /* caller-owned */
+    size_t out_cap;
+    size_t out_len;      /* written bytes */
+    int status;          /* GPZ_OK or an error for this item */
+} gpz_out;
+
+/* Fill *cfg with defaults (device 0, 131072-byte members). */
+GPZ_API void gpz_config_default(gpz_config* cfg);
+
+/* Create a context on cfg->device (NULL: defaults).  Replaces
+ * GpuBackend::try_init (gpu.rs:125-167). */
+GPZ_API int gpz_create(const gpz_config* cfg, gpz_ctx** out);
+GPZ_API void gpz_destroy(gpz_ctx* ctx);
+
+/* Worst-case output size of one compress call on n input bytes with
+ * 131072-byte members; gpz_bound_ctx uses the context's member size. */
+GPZ_API size_t gpz_bound(size_t n);
+GPZ_API size_t gpz_bound_ctx(const gpz_ctx* ctx, size_t n);
+
+/* One chunk -> concatenated gzip members.  Blocking.  The ChunkFn of
+ * gpu.rs:193-208: n <= member_bytes (including 0) gives one member. */
+GPZ_API int gpz_compress_chunk(gpz_ctx* ctx, const uint8_t* in, size_t n, int level, uint8_t* out,
+                       size_t out_cap, size_t* out_len);
+
+/* Many chunks or files of uneven size in one batched device pass (the
+ * persistent kernels fed by the device descriptor queue).  outs[i] receives
+ * the gzip stream of d[i].  Returns GPZ_OK if every item succeeded, else the
+ * first failing item's status (each item's status is also set). */
+GPZ_API int gpz_compress_batch(gpz_ctx* ctx, const gpz_desc* d, size_t count, gpz_out* outs);
+
+/* Same, one device pass per chunk with a host synchronisation in between:
+ * the plain one-launch-per-chunk path the batched path is measured against. */
+GPZ_API int gpz_compress_batch_plain(gpz_ctx* ctx, const gpz_desc* d, size_t count, gpz_out* outs);
+
+/* Device-resident batch.  d_in holds `count` inputs at 16-byte aligned device
+ * offsets in_off[i] with lengths in_len[i] (host arrays).  The gzip streams
+ * are written back to back into d_out (device, out_cap bytes) with member
+ * headers and trailers left for the host: header_trailer (host, may be NULL)
+ * receives, per member, its 18 framing bytes' offsets and values through
+ * gpz_member_frames.  out_off (host, count+1 entries) receives each input's
+ * byte range.  stream: a cudaStream_t (NULL: the context's stream).  Blocks
+ * until the device pass finishes. */
+GPZ_API int gpz_compress_device(gpz_ctx* ctx, const void* d_in, const uint64_t* in_off, const uint64_t* in_len,
+                        size_t count, void* d_out, size_t out_cap, uint64_t* out_off, void* stream);
+
+/* After gpz_compress_device: write the 10-byte headers and 8-byte trailers of
+ * the last device batch into host_out, a host copy of d_out. */
+GPZ_API int gpz_frame_host(gpz_ctx* ctx, uint8_t* host_out, size_t cap);
+
+/* Parity hooks.  Run one chunk and also return the per-position packed
+ * tokens (pp, n entries, length<<16 | distance-or-byte; lz77_hash.rs:54-62)
+ * and the walked token stream of all members back to back (tokens, up to n
+ * entries, *ntok set).  Any of pp / tokens / out may be NULL. */
+GPZ_API int gpz_debug_chunk(gpz_ctx* ctx, const uint8_t* in, size_t n, uint32_t* pp, uint32_t* tokens,
+                    size_t* ntok, uint8_t* out, size_t out_cap, size_t* out_len);
+
+/* Serving: submit a request (the input is copied before return), poll for
+ * its result.  gpz_poll returns GPZ_E_PENDING until the gzip stream is ready;
+ * wait_ms > 0 blocks up to that long.  The result is copied into o->out. */
+GPZ_API int gpz_submit(gpz_ctx* ctx, const gpz_desc* d, uint64_t* ticket);
+GPZ_API int gpz_poll(gpz_ctx* ctx, uint64_t ticket, gpz_out* o, int wait_ms);
+
+/* Serving statistics since the context started (latencies in ms). */
+typedef struct gpz_serve_stats {
+    uint64_t completed;
+    uint64_t rejected;
+    uint64_t batches;
+    double p50_ms, p99_ms, p999_ms;
+    double max_queue_ms;
+    uint64_t bytes_in, bytes_out;
+} gpz_serve_stats;
+GPZ_API int gpz_serve_stats_get(gpz_ctx* ctx, gpz_serve_stats* st);
+
+GPZ_API const char* gpz_strerror(int status);
+
+/* Last CUDA / device diagnostic of this context (static storage). */
+GPZ_API const char* gpz_last_error(gpz_ctx* ctx);
+
+/* Launch geometry in use: threads per CTA for lookup / walk / emit and the
+ * persistent grid sizes (0 = one CTA per tile).  Set by the autotuner; may
+ * be overridden for experiments. */
+typedef struct gpz_shape {
+    int lookup_threads, lookup_grid;
+    int walk_threads, walk_grid;
+    int emit_threads, emit_grid;
+} gpz_shape;
+GPZ_API int gpz_get_shape(gpz_ctx* ctx, gpz_shape* s);
+GPZ_API int gpz_set_shape(gpz_ctx* ctx, const gpz_shape* s);
+
+/* Number of kernel launches the last compress call issued. */
+GPZ_API uint64_t gpz_last_launches(gpz_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,156 @@
+"""ctypes front end for the C oracle (TEST INFRASTRUCTURE).
+
+Loads oracle/libgpz_oracle.so (built by oracle/Makefile) and exposes numpy /
+bytes helpers.  Only tests, the smoke check and the CPU-baseline leg of the
+benchmark import this module; the CUDA product path never does.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgpz_oracle.so")
+MEMBER_BYTES = 128 * 1024
+
+_lib = None
+
+
+def build() -> str:
+    """Compile the oracle with its Makefile (gcc; no CUDA needed)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        u8p = ctypes.c_void_p
+        L.gpzo_hash3.argtypes = [u8p, ctypes.c_uint32]
+        L.gpzo_hash3.restype = ctypes.c_uint32
+        L.gpzo_match_find.argtypes = [u8p, ctypes.c_uint32, u8p]
+        L.gpzo_match_find.restype = ctypes.c_int
+        L.gpzo_greedy_walk.argtypes = [u8p, u8p, ctypes.c_uint32, u8p]
+        L.gpzo_greedy_walk.restype = ctypes.c_size_t
+        L.gpzo_build_code_lengths.argtypes = [u8p, ctypes.c_int, ctypes.c_int, u8p]
+        L.gpzo_build_code_lengths.restype = ctypes.c_int
+        L.gpzo_encode_block_fast.argtypes = [u8p, ctypes.c_size_t, u8p, ctypes.c_size_t]
+        L.gpzo_encode_block_fast.restype = ctypes.c_size_t
+        L.gpzo_crc32.argtypes = [u8p, ctypes.c_size_t]
+        L.gpzo_crc32.restype = ctypes.c_uint32
+        L.gpzo_gzip_member.argtypes = [u8p, ctypes.c_uint32, u8p, ctypes.c_size_t]
+        L.gpzo_gzip_member.restype = ctypes.c_size_t
+        L.gpzo_gzip_chunk.argtypes = [u8p, ctypes.c_size_t, ctypes.c_size_t, u8p, ctypes.c_size_t,
+                                      ctypes.c_int]
+        L.gpzo_gzip_chunk.restype = ctypes.c_size_t
+        L.gpzo_member_bound.argtypes = [ctypes.c_size_t]
+        L.gpzo_member_bound.restype = ctypes.c_size_t
+        L.gpzo_brute_lz77.argtypes = [u8p, ctypes.c_uint32, ctypes.c_uint32, u8p]
+        L.gpzo_brute_lz77.restype = None
+        L.gpzcpu_gzip_chunks.argtypes = [u8p, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_int,
+                                         ctypes.c_int, u8p, ctypes.c_size_t]
+        L.gpzcpu_gzip_chunks.restype = ctypes.c_size_t
+        _lib = L
+    return _lib
+
+
+def _u8(data) -> np.ndarray:
+    if isinstance(data, np.ndarray):
+        return np.ascontiguousarray(data, dtype=np.uint8)
+    return np.frombuffer(bytes(data), dtype=np.uint8)
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p) if a.size else ctypes.c_void_p(0)
+
+
+def match_find(data) -> np.ndarray:
+    """Per-position packed tokens (u32 per input byte)."""
+    a = _u8(data)
+    pp = np.zeros(max(a.size, 1), dtype=np.uint32)
+    if a.size and lib().gpzo_match_find(_ptr(a), a.size, _ptr(pp)) != 0:
+        raise MemoryError("oracle match_find allocation failed")
+    return pp[:a.size]
+
+
+def brute_lz77(data, window: int = 4096) -> np.ndarray:
+    a = _u8(data)
+    pp = np.zeros(max(a.size, 1), dtype=np.uint32)
+    if a.size:
+        lib().gpzo_brute_lz77(_ptr(a), a.size, window, _ptr(pp))
+    return pp[:a.size]
+
+
+def greedy_walk(pp: np.ndarray, data) -> np.ndarray:
+    a = _u8(data)
+    pp = np.ascontiguousarray(pp, dtype=np.uint32)
+    out = np.zeros(max(a.size, 1), dtype=np.uint32)
+    k = lib().gpzo_greedy_walk(_ptr(pp), _ptr(a), a.size, _ptr(out)) if a.size else 0
+    return out[:k]
+
+
+def tokens(data) -> np.ndarray:
+    """Walked token stream for one member."""
+    return greedy_walk(match_find(data), data)
+
+
+def build_code_lengths(freq, max_bits: int):
+    f = np.ascontiguousarray(freq, dtype=np.uint32)
+    lens = np.zeros(f.size, dtype=np.uint8)
+    ok = lib().gpzo_build_code_lengths(_ptr(f), f.size, max_bits, _ptr(lens))
+    return lens if ok else None
+
+
+def encode_block_fast(toks: np.ndarray) -> bytes:
+    t = np.ascontiguousarray(toks, dtype=np.uint32)
+    cap = 1100 + 2 * t.size * 6 + 64
+    out = np.zeros(cap, dtype=np.uint8)
+    k = lib().gpzo_encode_block_fast(_ptr(t), t.size, _ptr(out), cap)
+    if k == 0:
+        raise RuntimeError("oracle encode overflow")
+    return out[:k].tobytes()
+
+
+def crc32(data) -> int:
+    a = _u8(data)
+    return lib().gpzo_crc32(_ptr(a), a.size)
+
+
+def gzip_member(data) -> bytes:
+    a = _u8(data)
+    cap = lib().gpzo_member_bound(a.size)
+    out = np.zeros(cap, dtype=np.uint8)
+    k = lib().gpzo_gzip_member(_ptr(a), a.size, _ptr(out), cap)
+    if k == 0:
+        raise RuntimeError("oracle gzip_member failed")
+    return out[:k].tobytes()
+
+
+def gzip_chunk(data, member_bytes: int = MEMBER_BYTES, threads: int = 1) -> bytes:
+    """gzip_chunk_fn: concatenated members of member_bytes each."""
+    a = _u8(data)
+    nmem = max(1, -(-a.size // member_bytes))
+    cap = nmem * lib().gpzo_member_bound(member_bytes)
+    out = np.zeros(cap, dtype=np.uint8)
+    k = lib().gpzo_gzip_chunk(_ptr(a), a.size, member_bytes, _ptr(out), cap, threads)
+    if k == 0:
+        raise RuntimeError("oracle gzip_chunk failed")
+    return out[:k].tobytes()
+
+
+def cpu_gzip_chunks(data, chunk: int = 2 << 20, level: int = 5, threads: int = 1) -> bytes:
+    """gpzip-cpu-equivalent: zlib 1.3 gzip member per chunk, all threads."""
+    a = _u8(data)
+    nch = max(1, -(-a.size // chunk))
+    cap = a.size + a.size // 100 + 1024 * nch + 4096
+    out = np.zeros(cap, dtype=np.uint8)
+    k = lib().gpzcpu_gzip_chunks(_ptr(a), a.size, chunk, level, threads, _ptr(out), cap)
+    if k == 0:
+        raise RuntimeError("cpu gzip failed")
+    return out[:k].tobytes()
