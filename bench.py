@@ -1,0 +1,354 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 gzip compression path (one JSON line on rank 0).
+
+Workload (default): the 64 MiB synthetic log stream (seed 1) as a one-file
+ustar archive (512 + 64 MiB + 1,024 bytes), cut into 2 MiB chunks (32 full +
+a 1,536-byte tail), each chunk compressed into 128 KiB gzip members -- the
+reference's `--backend gpu` behaviour on its single-stream throughput config.
+
+* ``value``: input GB/s with inputs resident in HBM (device ABI call
+  gpz_compress_device per step; L2 flushed between steps, steps timed with
+  CUDA events on the launching stream, max over ranks).
+* ``e2e``: the same metric through the public host API gpz_compress_batch
+  (host buffers in, host gzip streams out; copies inside the timed region).
+* ``roofline``: the dominant kernel's algorithmic bytes per launch
+  ((1 + ratio) x input bytes) over its CUDA-event duration, against the
+  measured HBM copy bandwidth; ``traffic`` from the committed ncu capture.
+* ``cpu_baseline``: the CPU port of the same path (oracle, all host threads)
+  on a bounded sample; ``gpzip_cpu_equiv``: zlib 1.3 level 5 per 2 MiB chunk
+  on all host threads (the reference's gpzip-cpu path).
+
+``--impl reference`` times the CPU port instead (rank 0 only).
+Multi-GPU (torchrun): every rank compresses its own copy of the workload
+(members are independent; no collective on the data path): weak scaling.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from gpzip_b200 import workloads as W  # noqa: E402
+
+METRIC = "input GB/s/B200 at bit-exact tokens"
+MEMBER = 128 * 1024
+CHUNK = 2 << 20
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="logs", choices=["logs", "text", "binary"])
+    ap.add_argument("--cpu-sample-mib", type=int, default=8)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baselines (quick runs)")
+    ap.add_argument("--device-only", action="store_true",
+                    help="only the device-resident steps (no e2e, no CPU baselines): for profiling")
+    return ap.parse_args()
+
+
+def workload(name: str):
+    if name == "logs":
+        data = W.config_logs_tar()
+        desc = "logs-64MiB-ustar (seed 1): 32x2MiB chunks + 1536 B tail"
+    elif name == "text":
+        data = W.config_text()
+        desc = "text-8MiB (seed 0): 4x2MiB chunks"
+    else:
+        data = W.config_binary()
+        desc = "binary-272MiB (seed 2): 136x2MiB chunks"
+    return data, desc
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def committed_traffic():
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        return json.load(open(p))
+    return {}
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join("/tmp", f"gpz_clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        self.proc.wait()
+        self.f.close()
+        sm, mx, reasons = [], None, set()
+        names = ["active", "hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names[1:], parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def inflate_all(gz: bytes) -> bytes:
+    import zlib
+    out, rest = b"", gz
+    while rest:
+        d = zlib.decompressobj(31)
+        out += d.decompress(rest)
+        rest = d.unused_data
+    return out
+
+
+def cpu_port_rate(data: np.ndarray, sample_mib: int, threads: int):
+    """The CPU port of the reference GPU path (oracle) on a bounded sample."""
+    from oracle import oracle as O
+    sample = data[: min(data.size, sample_mib << 20)]
+    spans = W.chunk_spans(sample.size, CHUNK)
+    t0 = time.perf_counter()
+    outs = [O.gzip_chunk(sample[o:o + n], MEMBER, threads=threads) for o, n in spans]
+    dt = time.perf_counter() - t0
+    return sample.size / dt / 1e9, sum(len(x) for x in outs) / sample.size, sample.size
+
+
+def cpu_zlib_rate(data: np.ndarray, threads: int):
+    from oracle import oracle as O
+    t0 = time.perf_counter()
+    gz = O.cpu_gzip_chunks(data, CHUNK, 5, threads=threads)
+    dt = time.perf_counter() - t0
+    return data.size / dt / 1e9, len(gz) / data.size
+
+
+def run_reference(args, rank: int):
+    """--impl reference: the CPU port of the path on all host threads."""
+    if rank != 0:
+        return
+    data, desc = workload(args.workload)
+    threads = os.cpu_count() or 1
+    sample_mib = args.cpu_sample_mib
+    for _ in range(max(0, min(args.warmup, 1))):
+        cpu_port_rate(data, 2, threads)
+    rates = []
+    ratio = None
+    for _ in range(args.steps):
+        r, ratio, nbytes = cpu_port_rate(data, sample_mib, threads)
+        rates.append(r)
+    value = statistics.median(rates)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 5), "unit": "GB/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(nbytes / (value * 1e9) * 1e3, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic (seeded generators standing in for the reference's corpora)",
+        "config": {"workload": desc, "chunk_bytes": CHUNK, "member_bytes": MEMBER, "level": 5},
+        "cpu_baseline": {"value": round(value, 5), "unit": "GB/s", "cores": threads, "kind": "port",
+                         "sample": f"first {sample_mib} MiB of the workload per step, members on all host threads"},
+        "e2e": {"value": round(value, 5), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "ratio": round(ratio, 5),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    from gpzip_b200 import native
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    data, desc = workload(args.workload)
+    spans = W.chunk_spans(data.size, CHUNK)
+    offs, lens, pos = [], [], 0
+    for o, n in spans:
+        offs.append(pos)
+        lens.append(n)
+        pos += (n + 15) // 16 * 16
+    packed = np.zeros(pos + 64, dtype=np.uint8)
+    for (o, n), po in zip(spans, offs):
+        packed[po:po + n] = data[o:o + n]
+
+    ctx = native.Context(device=local, member_bytes=MEMBER, flags=native.GPZ_FLAG_STAGE_TIMING)
+    d_in = torch.from_numpy(packed).to(f"cuda:{local}")
+    out_cap = ctx.bound(data.size) + 64 * len(spans)
+    d_out = torch.empty(out_cap, dtype=torch.uint8, device=f"cuda:{local}")
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=f"cuda:{local}")
+    stream = torch.cuda.current_stream()
+
+    def step():
+        return ctx.compress_device(d_in.data_ptr(), offs, lens, d_out.data_ptr(), out_cap, stream.cuda_stream)
+
+    # correctness of the device path on this workload: every member inflates
+    # back to its chunk, and one chunk is byte-compared with the oracle
+    oo = step()
+    host = d_out[:oo[-1]].cpu().numpy().copy()
+    ctx.frame_host(host)
+    parity = "unchecked"
+    if rank == 0:
+        from oracle import oracle as O
+        gz_all = host.tobytes()
+        ok = inflate_all(gz_all) == data.tobytes()
+        first = gz_all[oo[0]:oo[1]]
+        same = first == O.gzip_chunk(data[spans[0][0]:spans[0][0] + spans[0][1]], MEMBER, threads=8)
+        parity = "ok" if (ok and same) else f"FAILED (inflate={ok}, oracle_chunk0={same})"
+    ratio = oo[-1] / data.size
+
+    for _ in range(args.warmup):
+        step()
+    barrier()
+    clocks = Clocks(local)
+    clocks.start()
+    times, stages = [], np.zeros(4)
+    for _ in range(args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+        stages += np.array(ctx.stage_times())
+    barrier()
+    clk = clocks.stop()
+    launches = ctx.last_launches() * args.steps
+    total_ms = float(sum(times))
+    t = torch.tensor([total_ms], device=f"cuda:{local}", dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = float(t.item())
+    value = data.size * args.steps * world / (max_ms / 1e3) / 1e9
+
+    # end to end through the public host API (host buffers, copies inside)
+    host_chunks = [np.ascontiguousarray(data[o:o + n]) for o, n in spans]
+    for _ in range(0 if args.device_only else min(args.warmup, 2)):
+        ctx.compress_batch(host_chunks)
+    barrier()
+    e_times = []
+    e2e_out = 0
+    for _ in range(1 if args.device_only else max(2, args.steps // 2)):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        outs = ctx.compress_batch(host_chunks)
+        e1.record(stream)
+        e1.synchronize()
+        e_times.append(e0.elapsed_time(e1))
+        e2e_out = sum(len(x) for x in outs)
+    et = torch.tensor([sum(e_times)], device=f"cuda:{local}", dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(et, op=dist.ReduceOp.MAX)
+    e2e_value = data.size * len(e_times) * world / (float(et.item()) / 1e3) / 1e9
+
+    stage_ms = stages / args.steps
+    names = ["k_lookup", "k_walk", "k_huff", "k_emit"]
+    dom = int(np.argmax(stage_ms))
+    peak, peak_kind = measured_peaks()
+    algo_bytes = data.size * (1.0 + ratio)
+    achieved = algo_bytes / (stage_ms[dom] / 1e3) / 1e9
+    tr = committed_traffic().get(names[dom])
+    traffic = round(tr["dram_bytes_per_input_byte"] * data.size) if tr else None
+
+    cpu = None
+    zl = None
+    if rank == 0 and not (args.no_cpu or args.device_only):
+        threads = os.cpu_count() or 1
+        r, cr, nb = cpu_port_rate(data, args.cpu_sample_mib, threads)
+        cpu = {"value": round(r, 5), "unit": "GB/s", "cores": threads, "kind": "port",
+               "sample": f"first {args.cpu_sample_mib} MiB of the workload (CPU port of the reference GPU "
+                         f"path, members on {threads} host threads)", "ratio": round(cr, 5)}
+        zr, zratio = cpu_zlib_rate(data, threads)
+        zl = {"value": round(zr, 4), "unit": "GB/s", "cores": threads, "ratio": round(zratio, 5),
+              "what": "gpzip-cpu equivalent: zlib 1.3 level 5, one gzip member per 2 MiB chunk"}
+
+    if world > 1:
+        dist.barrier()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 4), "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(max_ms / args.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic (seeded generators standing in for the reference's corpora)",
+            "config": {"workload": desc, "bytes": int(data.size), "chunk_bytes": CHUNK, "member_bytes": MEMBER,
+                       "members": sum(-(-n // MEMBER) for _, n in spans), "level": 5,
+                       "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": round(achieved, 2), "peak": peak,
+                         "unit": "GB/s", "frac": round(achieved / peak, 5), "traffic": traffic,
+                         "peak_kind": peak_kind, "algorithmic_bytes_per_launch": int(algo_bytes)},
+            "stage_ms": {n: round(float(x), 4) for n, x in zip(names, stage_ms)},
+            "cpu_baseline": cpu,
+            "gpzip_cpu_equiv": zl,
+            "e2e": {"value": round(e2e_value, 4), "unit": "GB/s", "h2d_bytes_per_step": int(data.size),
+                    "d2h_bytes_per_step": int(e2e_out), "api": "gpz_compress_batch (host buffers)"},
+            "gpu_launches": int(launches),
+            "clocks": clk,
+            "ratio": round(ratio, 5),
+            "parity": parity,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

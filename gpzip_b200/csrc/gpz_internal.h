@@ -92,6 +92,7 @@ struct LaunchShape {
 };
 
 // Kernel launchers (gpz_kernels.cu).
-int gpz_launch_batch(const BatchParams& bp, const LaunchShape& ls, void* stream);
+// events: NULL or 5 cudaEvent_t recorded before each stage and after the last.
+int gpz_launch_batch(const BatchParams& bp, const LaunchShape& ls, void* stream, void* const* events);
 int gpz_kernel_smem_setup();
 size_t gpz_lookup_smem_bytes();

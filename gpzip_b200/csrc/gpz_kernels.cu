@@ -1113,25 +1113,33 @@ static void launch_lookup(const BatchParams& bp, int grid, cudaStream_t s) {
     k_lookup<T><<<grid, T, LookupSmem::kBytes, s>>>(bp);
 }
 
-int gpz_launch_batch(const BatchParams& bp, const LaunchShape& ls, void* stream) {
+int gpz_launch_batch(const BatchParams& bp, const LaunchShape& ls, void* stream, void* const* events) {
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    auto mark = [&](int i) {
+        if (events) cudaEventRecord(static_cast<cudaEvent_t>(events[i]), s);
+    };
     auto grid_of = [&](int g, uint32_t items) { return g > 0 ? g : (int)(items ? items : 1u); };
+    mark(0);
     const int gl = grid_of(ls.lookup_grid, bp.ntiles);
     switch (ls.lookup_threads) {
         case 256: launch_lookup<256>(bp, gl, s); break;
         case 1024: launch_lookup<1024>(bp, gl, s); break;
         default: launch_lookup<512>(bp, gl, s); break;
     }
+    mark(1);
     const int gw = grid_of(ls.walk_grid, bp.ntiles);
     switch (ls.walk_threads) {
         case 256: k_walk<256><<<gw, 256, 0, s>>>(bp); break;
         default: k_walk<512><<<gw, 512, 0, s>>>(bp); break;
     }
+    mark(2);
     k_huff<<<bp.nmembers ? (int)bp.nmembers : 1, kHuffThreads, 0, s>>>(bp);
+    mark(3);
     const int ge = grid_of(ls.emit_grid, bp.ntiles);
     switch (ls.emit_threads) {
         case 256: k_emit<256><<<ge, 256, 0, s>>>(bp); break;
         default: k_emit<512><<<ge, 512, 0, s>>>(bp); break;
     }
+    mark(4);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }

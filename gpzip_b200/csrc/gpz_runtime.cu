@@ -76,6 +76,9 @@ struct gpz_ctx {
     MemberOut* h_mout = nullptr;
     size_t h_mout_cap = 0;
     uint32_t* h_err = nullptr;
+    // per-stage CUDA events of the last pass (GPZ_FLAG_STAGE_TIMING)
+    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    float stage_ms[4] = {0, 0, 0, 0};
 };
 
 namespace {
@@ -230,12 +233,16 @@ int run_device(gpz_ctx* c, const uint8_t* d_in, uint8_t* d_out, cudaStream_t s) 
     bp.nmembers = (uint32_t)nm;
     bp.ntiles = (uint32_t)nt;
     bp.out_base = 0;
-    if (gpz_launch_batch(bp, c->shape, s) != 0) return fail(c, GPZ_E_CUDA, "kernel launch", cudaGetLastError());
+    const bool timing = (c->flags & GPZ_FLAG_STAGE_TIMING) && c->ev[0];
+    if (gpz_launch_batch(bp, c->shape, s, timing ? reinterpret_cast<void* const*>(c->ev) : nullptr) != 0)
+        return fail(c, GPZ_E_CUDA, "kernel launch", cudaGetLastError());
     c->launches = 4;
     CU(c, cudaMemcpyAsync(c->h_mout, c->d_mout.p, nm * sizeof(MemberOut), cudaMemcpyDeviceToHost, s));
     CU(c, cudaMemcpyAsync(c->h_err, bp.err, 4, cudaMemcpyDeviceToHost, s));
     CU(c, cudaStreamSynchronize(s));
     c->mout.assign(c->h_mout, c->h_mout + nm);
+    if (timing)
+        for (int i = 0; i < 4; i++) cudaEventElapsedTime(&c->stage_ms[i], c->ev[i], c->ev[i + 1]);
     const uint32_t err = *c->h_err;
     if (err & GPZ_ERRBIT_SPIN) return fail(c, GPZ_E_TIMEOUT, "bounded device wait expired");
     if (err) return fail(c, GPZ_E_INTERNAL, "device self-check failed");
@@ -392,6 +399,13 @@ int gpz_create(const gpz_config* cfg, gpz_ctx** out) {
         gpz_destroy(c);
         return GPZ_E_CUDA;
     }
+    if (c->flags & GPZ_FLAG_STAGE_TIMING)
+        for (auto& e : c->ev)
+            if (cudaEventCreate(&e) != cudaSuccess) {
+                cudaGetLastError();
+                gpz_destroy(c);
+                return GPZ_E_CUDA;
+            }
     *out = c;
     return GPZ_OK;
 }
@@ -410,6 +424,8 @@ void gpz_destroy(gpz_ctx* c) {
     if (c->h_tiles) cudaFreeHost(c->h_tiles);
     if (c->h_mout) cudaFreeHost(c->h_mout);
     if (c->h_err) cudaFreeHost(c->h_err);
+    for (auto& e : c->ev)
+        if (e) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -547,6 +563,13 @@ int gpz_set_shape(gpz_ctx* c, const gpz_shape* s) {
 }
 
 uint64_t gpz_last_launches(gpz_ctx* c) { return c ? c->launches : 0; }
+
+int gpz_stage_times(gpz_ctx* c, float* ms4) {
+    if (!c || !ms4 || !(c->flags & GPZ_FLAG_STAGE_TIMING)) return GPZ_E_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    for (int i = 0; i < 4; i++) ms4[i] = c->stage_ms[i];
+    return GPZ_OK;
+}
 
 int gpz_submit(gpz_ctx*, const gpz_desc*, uint64_t*) { return GPZ_E_ARG; }
 int gpz_poll(gpz_ctx*, uint64_t, gpz_out*, int) { return GPZ_E_ARG; }

@@ -20,13 +20,14 @@ GPZ_E_PENDING = 9
 GPZ_E_BUSY = 8
 GPZ_FLAG_NO_GRAPHS = 1
 GPZ_FLAG_NO_AUTOTUNE = 2
+GPZ_FLAG_STAGE_TIMING = 4
 
 # Every symbol include/gpz.h declares.
 EXPORTS = [
     "gpz_config_default", "gpz_create", "gpz_destroy", "gpz_bound", "gpz_bound_ctx", "gpz_compress_chunk",
     "gpz_compress_batch", "gpz_compress_batch_plain", "gpz_compress_device", "gpz_frame_host",
     "gpz_debug_chunk", "gpz_submit", "gpz_poll", "gpz_serve_stats_get", "gpz_strerror", "gpz_last_error",
-    "gpz_get_shape", "gpz_set_shape", "gpz_last_launches",
+    "gpz_get_shape", "gpz_set_shape", "gpz_last_launches", "gpz_stage_times",
 ]
 
 
@@ -111,6 +112,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.gpz_set_shape.restype = ctypes.c_int
     L.gpz_last_launches.argtypes = [vp]
     L.gpz_last_launches.restype = ctypes.c_uint64
+    L.gpz_stage_times.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
+    L.gpz_stage_times.restype = ctypes.c_int
     _lib = L
     return L
 
@@ -235,6 +238,12 @@ class Context:
 
     def last_launches(self) -> int:
         return self.L.gpz_last_launches(self._h)
+
+    def stage_times(self):
+        """Device ms of lookup, walk, Huffman plan, emit in the last pass."""
+        a = (ctypes.c_float * 4)()
+        self._check(self.L.gpz_stage_times(self._h, a), "gpz_stage_times")
+        return list(a)
 
     def submit(self, data, level: int = 5) -> int:
         a = _u8(data)

@@ -62,6 +62,7 @@ typedef struct gpz_config {
 
 #define GPZ_FLAG_NO_GRAPHS 1    /* launch kernels directly instead of per-bucket CUDA graphs */
 #define GPZ_FLAG_NO_AUTOTUNE 2  /* keep the default launch shapes */
+#define GPZ_FLAG_STAGE_TIMING 4 /* record CUDA events around each stage (gpz_stage_times) */
 
 typedef struct gpz_desc {
     const uint8_t* in;   /* one chunk or file */
@@ -106,12 +107,12 @@ GPZ_API int gpz_compress_batch_plain(gpz_ctx* ctx, const gpz_desc* d, size_t cou
 
 /* Device-resident batch.  d_in holds `count` inputs at 16-byte aligned device
  * offsets in_off[i] with lengths in_len[i] (host arrays).  The gzip streams
- * are written back to back into d_out (device, out_cap bytes) with member
- * headers and trailers left for the host: header_trailer (host, may be NULL)
- * receives, per member, its 18 framing bytes' offsets and values through
- * gpz_member_frames.  out_off (host, count+1 entries) receives each input's
- * byte range.  stream: a cudaStream_t (NULL: the context's stream).  Blocks
- * until the device pass finishes. */
+ * are written back to back into d_out (device, out_cap >= the bound) with the
+ * 10-byte member headers and 8-byte trailers left as gaps for the host
+ * (gpz_frame_host fills them in a host copy).  out_off (host, count+1
+ * entries) receives each input's start offset and, last, the total length.
+ * stream: a cudaStream_t (NULL: the context's stream).  Blocks until the
+ * device pass finishes. */
 GPZ_API int gpz_compress_device(gpz_ctx* ctx, const void* d_in, const uint64_t* in_off, const uint64_t* in_len,
                         size_t count, void* d_out, size_t out_cap, uint64_t* out_off, void* stream);
 
@@ -161,6 +162,10 @@ GPZ_API int gpz_set_shape(gpz_ctx* ctx, const gpz_shape* s);
 
 /* Number of kernel launches the last compress call issued. */
 GPZ_API uint64_t gpz_last_launches(gpz_ctx* ctx);
+
+/* Device time of each stage of the last device pass, in ms: lookup, walk,
+ * Huffman plan, emit.  Needs GPZ_FLAG_STAGE_TIMING at gpz_create. */
+GPZ_API int gpz_stage_times(gpz_ctx* ctx, float* ms4);
 
 #ifdef __cplusplus
 }
