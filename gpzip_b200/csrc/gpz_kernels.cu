@@ -179,40 +179,37 @@ struct LookupSmem {
     static constexpr size_t kKeys = kWin + GPZ_WIN_BYTES;
     static constexpr size_t kNew = kKeys + GPZ_KEY_SLOTS * 4;
     static constexpr size_t kOld = kNew + GPZ_SEG * 4;
-    static constexpr size_t kCrcTab = kOld + GPZ_SEG * 4;
-    static constexpr size_t kWarp = kCrcTab + 8 * 256 * 4;
-    static constexpr size_t kBytes = kWarp + 64 * 4;
+    static constexpr size_t kBits = kOld + GPZ_SEG * 4;
+    static constexpr size_t kBytes = kBits + 65536 / 8;
 };
 
+// One CTA per 4 KiB tile S of a member (persistent over tiles).  The window
+// [S-8, S] plus 320 bytes of lookahead is staged in shared memory.  The
+// reference's dense seg_oldest / seg_newest tables (65536 x num_segs each)
+// are never materialised: only the hashes the tile itself queries matter, so
+// the tile's own keys go into a small open-addressed table (dense ids) and,
+// for each segment S-1 .. S-8 in the reference's order, the oldest / newest
+// positions of exactly those keys are rebuilt with shared-memory atomics.
+// Segments more than 8 back are never reachable: their nearest position is
+// more than 32768 bytes from any p in S, which try_candidate rejects.
+//
+// The per-segment entries are kept with atomicMin only, tagged so that
+// stale values from the previous (higher) segment lose and read as absent:
+//   oldest:  q + 1                       (valid iff <= qbase + 4096)
+//   newest:  2*qbase + 4095 - q          (valid iff <= qbase + 4095)
+// which saves clearing the arrays between segments.
 template <int T>
 __global__ void __launch_bounds__(T, (T >= 1024 ? 1 : 2)) k_lookup(BatchParams bp) {
     constexpr int PER = GPZ_SEG / T;
-    constexpr int CRC_BYTES = GPZ_SEG / T;  // bytes each thread folds into the tile CRC
     extern __shared__ __align__(16) uint8_t smem[];
     uint8_t* win = smem + LookupSmem::kWin;
     uint32_t* w32 = reinterpret_cast<uint32_t*>(win);
     uint32_t* keytab = reinterpret_cast<uint32_t*>(smem + LookupSmem::kKeys);
     uint32_t* cnew = reinterpret_cast<uint32_t*>(smem + LookupSmem::kNew);
     uint32_t* cold = reinterpret_cast<uint32_t*>(smem + LookupSmem::kOld);
-    uint32_t* crctab = reinterpret_cast<uint32_t*>(smem + LookupSmem::kCrcTab);
-    uint32_t* wsum = reinterpret_cast<uint32_t*>(smem + LookupSmem::kWarp);
+    uint32_t* kbits = reinterpret_cast<uint32_t*>(smem + LookupSmem::kBits);  // presence of each hash
     __shared__ uint32_t s_tile, s_nkeys;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-
-    // slice-by-8 CRC tables
-    for (int i = tid; i < 256; i += T) {
-        uint32_t c = (uint32_t)i;
-        for (int k = 0; k < 8; k++) c = (c & 1u) ? kCrcPoly ^ (c >> 1) : c >> 1;
-        crctab[i] = c;
-    }
-    __syncthreads();
-    for (int i = tid; i < 256; i += T) {
-        uint32_t c = crctab[i];
-        for (int s = 1; s < 8; s++) {
-            c = crctab[c & 0xFFu] ^ (c >> 8);
-            crctab[s * 256 + i] = c;
-        }
-    }
+    const int tid = threadIdx.x, lane = tid & 31;
 
     for (;;) {
         __syncthreads();
@@ -236,45 +233,17 @@ __global__ void __launch_bounds__(T, (T >= 1024 ? 1 : 2)) k_lookup(BatchParams b
             const uint32_t nvec = (wvalid + 15u) >> 4;
             for (uint32_t i = tid; i < nvec; i += T) dst[i] = __ldg(src + i);
             for (int i = tid; i < GPZ_KEY_SLOTS; i += T) keytab[i] = kEmpty;
+            for (int i = tid; i < 65536 / 32; i += T) kbits[i] = 0u;
+            for (int i = tid; i < GPZ_SEG; i += T) {
+                cnew[i] = kEmpty;
+                cold[i] = kEmpty;
+            }
             if (tid == 0) s_nkeys = 0;
             __syncthreads();
             const uint32_t zend = min((uint32_t)GPZ_WIN_BYTES, (nvec << 4) + 32u);
             for (uint32_t i = wvalid + tid; i < zend; i += T) win[i] = 0;
         }
         __syncthreads();
-
-        // ---- tile CRC (zero-init CRC of the cnt tile bytes; the tile is
-        // viewed as 4096 bytes with leading zeros, which a zero-init CRC
-        // ignores, so every thread folds a fixed-size slice)
-        {
-            const uint32_t pad = GPZ_SEG - cnt;
-            uint32_t c = 0;
-            const uint32_t v0 = tid * CRC_BYTES;
-            if (pad == 0 && (CRC_BYTES % 8) == 0) {
-#pragma unroll
-                for (int q = 0; q < CRC_BYTES; q += 8) {
-                    uint32_t lo = w32[(pl0 + v0 + q) >> 2] ^ c, hi = w32[((pl0 + v0 + q) >> 2) + 1];
-                    c = crctab[7 * 256 + (lo & 0xFFu)] ^ crctab[6 * 256 + ((lo >> 8) & 0xFFu)] ^
-                        crctab[5 * 256 + ((lo >> 16) & 0xFFu)] ^ crctab[4 * 256 + (lo >> 24)] ^
-                        crctab[3 * 256 + (hi & 0xFFu)] ^ crctab[2 * 256 + ((hi >> 8) & 0xFFu)] ^
-                        crctab[1 * 256 + ((hi >> 16) & 0xFFu)] ^ crctab[hi >> 24];
-                }
-            } else {
-                for (int q = 0; q < CRC_BYTES; q++) {
-                    uint32_t v = v0 + q;
-                    uint32_t byte = v >= pad ? win[pl0 + v - pad] : 0u;
-                    c = crctab[(c ^ byte) & 0xFFu] ^ (c >> 8);
-                }
-            }
-            // combine neighbours: crc(A||B) = crc(A) * x^(8|B|) + crc(B)
-#pragma unroll
-            for (int s = 1, k = 0; s < 32; s <<= 1, k++) {
-                uint32_t other = __shfl_down_sync(0xFFFFFFFFu, c, s);
-                uint32_t comb = gf2_mulmod(c, x8pow((uint32_t)(CRC_BYTES * s))) ^ other;
-                if ((lane & (2 * s - 1)) == 0) c = comb;
-            }
-            if (lane == 0) wsum[warp] = c;
-        }
 
         // ---- insert the tile's own hash keys (p + 2 < n)
         uint32_t info[PER];  // slot | h << 13, or kEmpty
@@ -290,6 +259,7 @@ __global__ void __launch_bounds__(T, (T >= 1024 ? 1 : 2)) k_lookup(BatchParams b
                     uint32_t old = atomicCAS(&keytab[s], kEmpty, h);
                     if (old == kEmpty) {
                         own |= 1u << k;
+                        atomicOr(&kbits[h >> 5], 1u << (h & 31u));
                         break;
                     }
                     if (old == h) break;
@@ -299,12 +269,6 @@ __global__ void __launch_bounds__(T, (T >= 1024 ? 1 : 2)) k_lookup(BatchParams b
             }
         }
         __syncthreads();
-        if (tid == 0) {
-            const int nw = T / 32;
-            uint32_t c = wsum[0];
-            for (int w = 1; w < nw; w++) c = gf2_mulmod(c, x8pow((uint32_t)(CRC_BYTES * 32))) ^ wsum[w];
-            bp.tile_crc[t] = c;
-        }
         // dense ids for the distinct keys (warp-aggregated)
 #pragma unroll
         for (int k = 0; k < PER; k++) {
@@ -319,7 +283,6 @@ __global__ void __launch_bounds__(T, (T >= 1024 ? 1 : 2)) k_lookup(BatchParams b
             }
         }
         __syncthreads();
-        const uint32_t nkeys = s_nkeys;
         uint32_t myid[PER];
         uint32_t best[PER];
 #pragma unroll
@@ -330,11 +293,10 @@ __global__ void __launch_bounds__(T, (T >= 1024 ? 1 : 2)) k_lookup(BatchParams b
 
         // ---- own segment: the newest entry is always >= p (p itself is in
         // the table), so only the oldest can be a candidate
-        for (uint32_t i = tid; i < nkeys; i += T) cold[i] = kEmpty;
-        __syncthreads();
 #pragma unroll
         for (int k = 0; k < PER; k++) {
             const uint32_t id = myid[k];
+            if (!__ballot_sync(0xFFFFFFFFu, id != kEmpty)) continue;
             const uint32_t grp = __match_any_sync(0xFFFFFFFFu, id == kEmpty ? 0x10000u + lane : id);
             if (id != kEmpty && lane == __ffs(grp) - 1) atomicMin(&cold[id], start + tid + k * T + 1u);
         }
@@ -343,38 +305,35 @@ __global__ void __launch_bounds__(T, (T >= 1024 ? 1 : 2)) k_lookup(BatchParams b
         for (int k = 0; k < PER; k++)
             if (myid[k] != kEmpty) try_cand(win, w32, cold[myid[k]], start + tid + k * T, n, w0, best[k]);
 
-        // ---- segments S-1 .. S-8: build their oldest/newest entries for
-        // the tile's keys in shared memory, then try newest, then oldest
-        // while best < 16 (lz77_hash_lookup.wgsl:138-166)
+        // ---- segments S-1 .. S-8 in the reference's order: newest, then
+        // oldest while best < 16 (lz77_hash_lookup.wgsl:138-166)
         for (uint32_t back = 1; back <= 8u && back <= S; back++) {
             const uint32_t qbase = (S - back) << GPZ_SEG_LOG2;
-            __syncthreads();
-            for (uint32_t i = tid; i < nkeys; i += T) {
-                cnew[i] = 0u;
-                cold[i] = kEmpty;
-            }
-            __syncthreads();
+            __syncthreads();  // the previous segment's reads are done
 #pragma unroll
             for (int k = 0; k < PER; k++) {
                 const uint32_t i = tid + k * T, q = qbase + i;
                 uint32_t id = kEmpty;
                 if (q + 2u < n) {
                     const uint32_t h = hash_at(w32, q - w0);
-                    uint32_t s = key_slot(h);
-                    for (;;) {
-                        const uint32_t wv = keytab[s];
-                        if (wv == kEmpty) break;
-                        if ((wv & 0xFFFFu) == h) {
-                            id = wv >> 16;
-                            break;
+                    if ((kbits[h >> 5] >> (h & 31u)) & 1u) {
+                        uint32_t s = key_slot(h);
+                        for (;;) {
+                            const uint32_t wv = keytab[s];
+                            if (wv == kEmpty) break;
+                            if ((wv & 0xFFFFu) == h) {
+                                id = wv >> 16;
+                                break;
+                            }
+                            s = (s + 1u) & (GPZ_KEY_SLOTS - 1);
                         }
-                        s = (s + 1u) & (GPZ_KEY_SLOTS - 1);
                     }
                 }
+                if (!__ballot_sync(0xFFFFFFFFu, id != kEmpty)) continue;
                 const uint32_t grp = __match_any_sync(0xFFFFFFFFu, id == kEmpty ? 0x10000u + lane : id);
                 if (id != kEmpty) {
                     if (lane == __ffs(grp) - 1) atomicMin(&cold[id], q + 1u);
-                    if (lane == 31 - __clz(grp)) atomicMax(&cnew[id], q + 1u);
+                    if (lane == 31 - __clz(grp)) atomicMin(&cnew[id], 2u * qbase + 4095u - q);
                 }
             }
             __syncthreads();
@@ -383,11 +342,12 @@ __global__ void __launch_bounds__(T, (T >= 1024 ? 1 : 2)) k_lookup(BatchParams b
                 const uint32_t id = myid[k];
                 if (id == kEmpty) continue;
                 const uint32_t p = start + tid + k * T;
-                const uint32_t rn = cnew[id];
+                const uint32_t en = cnew[id];
+                const uint32_t rn = en <= qbase + 4095u ? 2u * qbase + 4096u - en : 0u;  // q + 1, or absent
                 try_cand(win, w32, rn, p, n, w0, best[k]);
                 if ((best[k] >> 16) < 16u) {
                     const uint32_t ro = cold[id];
-                    if (ro != rn) try_cand(win, w32, ro, p, n, w0, best[k]);
+                    if (ro <= qbase + GPZ_SEG && ro != rn) try_cand(win, w32, ro, p, n, w0, best[k]);
                 }
             }
         }
@@ -574,6 +534,7 @@ __global__ void __launch_bounds__(T) k_walk(BatchParams bp) {
 // ================================================================== k_huff
 
 constexpr int kHuffThreads = 320;
+constexpr int kCrcSlices = 256;  // threads folding member bytes into the CRC
 
 struct TreeScratch {
     uint32_t w[GPZ_NLIT];
@@ -693,14 +654,32 @@ struct HuffSmem {
     uint32_t hdr[GPZ_MAX_HEADER_WORDS + 2];
     uint32_t tile_bits[512];
     uint32_t red[32];
+    uint32_t crctab[8 * 256];
+    uint32_t crcv[kCrcSlices];
+    uint32_t crcx[8];
     unsigned long long gz_off;
-    uint32_t member, hbits, total, nrle, nlit, ndist, ok;
+    uint32_t member, hbits, total, nrle, nlit, ndist, ok, crc;
 };
 
 __global__ void __launch_bounds__(kHuffThreads) k_huff(BatchParams bp) {
     __shared__ HuffSmem sm;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     constexpr int NW = kHuffThreads / 32;
+
+    // slice-by-8 CRC tables: crctab[k][b] = CRC of byte b followed by k zeros
+    for (int i = tid; i < 256; i += kHuffThreads) {
+        uint32_t c = (uint32_t)i;
+        for (int k = 0; k < 8; k++) c = (c & 1u) ? kCrcPoly ^ (c >> 1) : c >> 1;
+        sm.crctab[i] = c;
+    }
+    __syncthreads();
+    for (int i = tid; i < 256; i += kHuffThreads) {
+        uint32_t c = sm.crctab[i];
+        for (int k = 1; k < 8; k++) {
+            c = sm.crctab[c & 0xFFu] ^ (c >> 8);
+            sm.crctab[k * 256 + i] = c;
+        }
+    }
 
     for (;;) {
         __syncthreads();
@@ -718,6 +697,50 @@ __global__ void __launch_bounds__(kHuffThreads) k_huff(BatchParams bp) {
             sm.freq[tid] = f + (tid == 256 ? 1u : 0u);
         }
         if (tid == 0) sm.ok = 1;
+
+        // CRC-32 of the member (crc32fast at deflate.rs:974).  The aligned
+        // 8-byte words are cut into kCrcSlices equal slices, front-padded
+        // with zero words (which a zero-init CRC ignores); each slice is
+        // folded with slice-by-8, then the slices are combined pairwise,
+        // crc(A||B) = crc(A) * x^(8|B|) + crc(B), in a tree.
+        {
+            const uint32_t L = md.len, W = L >> 3;
+            const uint32_t per = (W + kCrcSlices - 1) / kCrcSlices;
+            const uint32_t padw = per * kCrcSlices - W;
+            if (tid < kCrcSlices) {
+                const uint2* words = reinterpret_cast<const uint2*>(bp.in + md.in_off);
+                uint32_t c = 0;
+                for (uint32_t v = tid * per; v < (tid + 1) * per; v++) {
+                    if (v < padw) continue;
+                    const uint2 w = __ldg(words + (v - padw));
+                    const uint32_t lo = w.x ^ c, hi = w.y;
+                    c = sm.crctab[7 * 256 + (lo & 0xFFu)] ^ sm.crctab[6 * 256 + ((lo >> 8) & 0xFFu)] ^
+                        sm.crctab[5 * 256 + ((lo >> 16) & 0xFFu)] ^ sm.crctab[4 * 256 + (lo >> 24)] ^
+                        sm.crctab[3 * 256 + (hi & 0xFFu)] ^ sm.crctab[2 * 256 + ((hi >> 8) & 0xFFu)] ^
+                        sm.crctab[1 * 256 + ((hi >> 16) & 0xFFu)] ^ sm.crctab[hi >> 24];
+                }
+                sm.crcv[tid] = c;
+            }
+            if (tid == 0) {
+                uint32_t x = x8pow(8u * per);
+                for (int j = 0; j < 8; j++) {
+                    sm.crcx[j] = x;
+                    x = gf2_mulmod(x, x);
+                }
+            }
+            __syncthreads();
+            for (int j = 0; j < 8; j++) {
+                const int span = 1 << j;
+                if (tid < kCrcSlices && (tid & (2 * span - 1)) == 0)
+                    sm.crcv[tid] = gf2_mulmod(sm.crcv[tid], sm.crcx[j]) ^ sm.crcv[tid + span];
+                __syncthreads();
+            }
+            if (tid == 0) {
+                uint32_t c = sm.crcv[0];
+                for (uint32_t i = W << 3; i < L; i++) c = sm.crctab[(c ^ bp.in[md.in_off + i]) & 0xFFu] ^ (c >> 8);
+                sm.crc = ~(gf2_mulmod(0xFFFFFFFFu, x8pow(L)) ^ c);
+            }
+        }
         __syncthreads();
 
         // litlen (warp 0) and distance (warp 1) code lengths, 15-bit limit
@@ -867,36 +890,44 @@ __global__ void __launch_bounds__(kHuffThreads) k_huff(BatchParams bp) {
             uint32_t tot = sm.hbits;
             for (int w = 0; w < NW; w++) tot += sm.red[w];
             sm.total = tot;
-            // place the member in the batch output: decoupled look-back over
-            // members on (18 + DEFLATE bytes)
-            const unsigned long long agg = 18ull + ((tot + 7u) >> 3);
+        }
+        __syncthreads();
+        // place the member in the batch output: decoupled look-back over
+        // members on (18 + DEFLATE bytes), 32 predecessors per step
+        if (warp == 0) {
+            const unsigned long long agg = 18ull + ((sm.total + 7u) >> 3);
+            const unsigned long long vmask = (1ull << 62) - 1ull;
             unsigned long long excl = 0;
-            if (m == 0) {
-                atomicExch(&bp.member_status[m], (2ull << 62) | agg);
-            } else {
-                atomicExch(&bp.member_status[m], (1ull << 62) | agg);
-                uint32_t j = m - 1u, spins = 0;
-                for (;;) {
-                    const unsigned long long s = ld_volatile64(&bp.member_status[j]);
-                    const unsigned long long f = s >> 62, v = s & ((1ull << 62) - 1ull);
-                    if (f == 2ull) {
-                        excl += v;
-                        break;
-                    }
-                    if (f == 1ull) {
-                        excl += v;
-                        j--;
-                        continue;
-                    }
+            if (lane == 0) atomicExch(&bp.member_status[m], ((m == 0 ? 2ull : 1ull) << 62) | agg);
+            long long j = (long long)m - 1;
+            uint32_t spins = 0;
+            while (j >= 0) {
+                const long long idx = j - lane;
+                const unsigned long long st = idx >= 0 ? ld_volatile64(&bp.member_status[idx]) : (2ull << 62);
+                const uint32_t f = (uint32_t)(st >> 62);
+                const uint32_t incl = __ballot_sync(0xFFFFFFFFu, f == 2u);
+                const uint32_t zero = __ballot_sync(0xFFFFFFFFu, f == 0u);
+                const int first = incl ? __ffs(incl) - 1 : 32;
+                const uint32_t before = first == 32 ? 0xFFFFFFFFu : ((1u << first) - 1u);
+                if (zero & before) {
                     if (++spins > kSpinLimit) {
-                        atomicOr(bp.err, GPZ_ERRBIT_SPIN);
+                        if (lane == 0) atomicOr(bp.err, GPZ_ERRBIT_SPIN);
                         break;
                     }
                     __nanosleep(64);
+                    continue;
                 }
-                atomicExch(&bp.member_status[m], (2ull << 62) | (excl + agg));
+                unsigned long long v = (lane <= first) ? (st & vmask) : 0ull;
+#pragma unroll
+                for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+                excl += v;
+                if (first < 32) break;
+                j -= 32;
             }
-            sm.gz_off = bp.out_base + excl;
+            if (lane == 0) {
+                if (m > 0) atomicExch(&bp.member_status[m], (2ull << 62) | (excl + agg));
+                sm.gz_off = bp.out_base + excl;
+            }
         }
         __syncthreads();
 
@@ -957,16 +988,10 @@ __global__ void __launch_bounds__(kHuffThreads) k_huff(BatchParams bp) {
             const uint32_t s = (uint32_t)(e0 & 31u);
             atomicOr(&outw[e0 >> 5], eob << s);
             if (s + eob_len > 32u) atomicOr(&outw[(e0 >> 5) + 1], eob >> (32u - s));
-            // CRC-32 of the member from its tiles' zero-init CRCs
-            uint32_t st = 0xFFFFFFFFu;
-            for (uint32_t j = 0; j < md.ntiles; j++) {
-                const uint32_t len = min(GPZ_SEG, md.len - (j << GPZ_SEG_LOG2));
-                st = gf2_mulmod(st, len == GPZ_SEG ? c_x8pow2[12] : x8pow(len)) ^ bp.tile_crc[md.tile_base + j];
-            }
             MemberOut mo;
             mo.gz_off = sm.gz_off;
             mo.deflate_bytes = (sm.total + 7u) >> 3;
-            mo.crc = ~st;
+            mo.crc = sm.crc;
             mo.total_bits = sm.total;
             mo.header_bits = sm.hbits;
             mo.len = md.len;
