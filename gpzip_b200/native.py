@@ -27,7 +27,7 @@ EXPORTS = [
     "gpz_config_default", "gpz_create", "gpz_destroy", "gpz_bound", "gpz_bound_ctx", "gpz_compress_chunk",
     "gpz_compress_batch", "gpz_compress_batch_plain", "gpz_compress_device", "gpz_frame_host",
     "gpz_debug_chunk", "gpz_submit", "gpz_poll", "gpz_serve_stats_get", "gpz_strerror", "gpz_last_error",
-    "gpz_get_shape", "gpz_set_shape", "gpz_last_launches", "gpz_stage_times",
+    "gpz_get_shape", "gpz_set_shape", "gpz_last_launches", "gpz_stage_times", "gpz_compress_member_static",
 ]
 
 
@@ -114,6 +114,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.gpz_last_launches.restype = ctypes.c_uint64
     L.gpz_stage_times.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
     L.gpz_stage_times.restype = ctypes.c_int
+    L.gpz_compress_member_static.argtypes = [vp, sz, vp, sz, ctypes.POINTER(sz), vp]
+    L.gpz_compress_member_static.restype = ctypes.c_int
     _lib = L
     return L
 

@@ -163,6 +163,30 @@ GPZ_API int gpz_set_shape(gpz_ctx* ctx, const gpz_shape* s);
 /* Number of kernel launches the last compress call issued. */
 GPZ_API uint64_t gpz_last_launches(gpz_ctx* ctx);
 
+/* Largest input gpz_compress_member_static accepts (one 128 KiB member). */
+#define GPZ_STATIC_MAX_BYTES 131072
+
+/* Allocation-free compression of one member.  No counterpart in the
+ * reference: it exists for callers that cannot allocate GPU memory when they
+ * compress (their device memory is fully reserved by another allocator, or
+ * the path must not take cudaMalloc / cudaFree, which can synchronise the
+ * device).  All working memory is one fixed device array of about 1.5 MB
+ * inside this library, held by every GPU that loads it until process exit.
+ * d_in (n <= GPZ_STATIC_MAX_BYTES bytes, any alignment) and d_out (out_cap
+ * bytes; gpz_bound(n) always suffices) are device memory on the calling
+ * thread's current device; d_out receives one complete gzip member, byte for
+ * byte what gpz_compress_chunk returns for the same input, and *out_len its
+ * length.  Larger n returns GPZ_E_ARG; a short d_out returns GPZ_E_SPACE.
+ * The first call on a device resolves the array's address and sets kernel
+ * attributes, so make that first call before any stream capture begins.  The
+ * call runs on `stream` (a cudaStream_t, NULL for the legacy default stream)
+ * and returns after that stream has finished it.  Calls share the array:
+ * calls whose device work overlaps race, so callers on one device are
+ * serialised here and should not overlap it with their own device-side
+ * reuse of d_out. */
+GPZ_API int gpz_compress_member_static(const uint8_t* d_in, size_t n, uint8_t* d_out, size_t out_cap,
+                                       size_t* out_len, void* stream);
+
 /* Device time of each stage of the last device pass, in ms: lookup, walk,
  * Huffman plan, emit.  Needs GPZ_FLAG_STAGE_TIMING at gpz_create. */
 GPZ_API int gpz_stage_times(gpz_ctx* ctx, float* ms4);
