@@ -12,22 +12,16 @@
 #define GPZ_SEG (1u << GPZ_SEG_LOG2)
 #define GPZ_WIN_SEGS 9                      // own segment + 8 back (window-bound proof)
 #define GPZ_WIN_BYTES (GPZ_WIN_SEGS * GPZ_SEG + 320)
-#define GPZ_KEY_SLOTS 8192
 #define GPZ_MAX_MATCH 258u
 #define GPZ_WINDOW 32768u
 #define GPZ_NLIT 286
 #define GPZ_NDIST 30
 #define GPZ_NSYM (GPZ_NLIT + GPZ_NDIST)
 #define GPZ_EXITS 258                       // entry offsets a walk can have into a tile
-#define GPZ_MAX_HEADER_WORDS 160            // dynamic block header <= 4498 bits
-
-// Status words of the decoupled look-backs.
-#define GPZ_ST_AGG 0x40000000u
-#define GPZ_ST_INCL 0x80000000u
-#define GPZ_ST_MASK 0xC0000000u
+#define GPZ_HDR_WORDS 144                   // dynamic block header <= 4498 bits, + slack
 
 // Error bits reported through BatchParams::err.
-#define GPZ_ERRBIT_SPIN 1u      // a bounded look-back wait expired
+#define GPZ_ERRBIT_SPIN 1u      // a bounded wait expired
 #define GPZ_ERRBIT_BITS 2u      // emitted bit count disagreed with the plan
 #define GPZ_ERRBIT_HUFF 4u      // code construction failed (never expected)
 
@@ -61,17 +55,20 @@ struct BatchParams {
     const MemberDesc* members;
     const TileDesc* tiles;
     uint32_t* pp;             // per-position packed tokens, indexed like `in`
+    uint16_t* seg_keys;       // [tile][4096] distinct hashes of the segment, ascending
+    uint32_t* seg_on;         // [tile][4096] newest offset | oldest offset << 16, per distinct hash
+    uint16_t* seg_posid;      // [tile][4096] rank of each position's hash (0xFFFF: none)
+    uint32_t* seg_nkeys;      // [tile] distinct hashes in the segment
     uint32_t* tok;            // walked tokens, tile-sparse, indexed like `in`
     uint32_t* out_words;      // gzip stream of the batch, as 32-bit words
-    uint32_t* tile_status;    // walk look-back status per tile
+    uint32_t* tile_entry;     // walk entry offset into each tile
     uint16_t* tile_exit;      // [tile][GPZ_EXITS] exit offset into the next tile
     uint16_t* tile_hist;      // [tile][GPZ_NSYM] symbol counts of the tile's tokens
     uint32_t* tile_ntok;      // tokens per tile
-    uint32_t* tile_crc;       // zero-init CRC of each tile's bytes
     uint32_t* tile_bitoff;    // tile's first token bit within its member's DEFLATE stream
     uint32_t* member_codes;   // [member][GPZ_NSYM] reversed code | len << 16
+    uint32_t* member_hdr;     // [member][GPZ_HDR_WORDS] dynamic block header bits
     MemberOut* member_out;
-    unsigned long long* member_status;  // output look-back: flag<<62 | value
     uint32_t* counters;       // [0..3] tile claims per stage, [4] member claims
     uint32_t* err;
     uint32_t nmembers;
@@ -79,7 +76,15 @@ struct BatchParams {
     uint64_t out_base;        // byte offset added to every member's gz_off
 };
 
-enum { GPZ_CNT_LOOKUP = 0, GPZ_CNT_WALK = 1, GPZ_CNT_HUFF = 2, GPZ_CNT_EMIT = 3, GPZ_NCOUNTERS = 8 };
+enum {
+    GPZ_CNT_LOOKUP = 0,
+    GPZ_CNT_EXIT = 1,
+    GPZ_CNT_MARK = 2,
+    GPZ_CNT_HUFF = 3,
+    GPZ_CNT_EMIT = 4,
+    GPZ_CNT_SEGSORT = 5,
+    GPZ_NCOUNTERS = 8
+};
 
 // Per-stage launch geometry chosen by the autotuner (threads per CTA, CTAs).
 struct LaunchShape {

@@ -27,7 +27,6 @@ namespace {
 
 constexpr uint32_t kEmpty = 0xFFFFFFFFu;
 constexpr uint32_t kCrcPoly = 0xEDB88320u;
-constexpr uint32_t kSpinLimit = 1u << 22;  // x >= 64 ns per try: a few hundred ms, then error
 
 // x^(8 * 2^k) mod P, reflected, k = 0..31 (filled by gpz_kernel_smem_setup).
 __constant__ uint32_t c_x8pow2[32];
@@ -79,18 +78,6 @@ __device__ uint32_t x8pow(uint32_t n) {
         if (n & 1u) r = gf2_mulmod(r, c_x8pow2[k]);
     return r;
 }
-
-__device__ __forceinline__ uint32_t ld32u(const uint32_t* w, uint32_t off) {
-    return __funnelshift_r(w[off >> 2], w[(off >> 2) + 1], (off & 3u) * 8u);
-}
-
-// hash3 of lz77_hash_build.wgsl:36-43 on bytes at window offset o.
-__device__ __forceinline__ uint32_t hash_at(const uint32_t* w, uint32_t o) {
-    uint32_t x = __byte_perm(ld32u(w, o), 0u, 0x4012);  // b0<<16 | b1<<8 | b2
-    return (x * 0x9E3779B1u) >> 16;
-}
-
-__device__ __forceinline__ uint32_t key_slot(uint32_t h) { return (h * 0x85EBCA6Bu) >> 19; }
 
 // Match length at window offsets a < b, capped at limit: 16 bytes per step,
 // first difference from the lowest set bit of the XOR (__clz of the
@@ -167,49 +154,135 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* warp_s
     return r;
 }
 
-__device__ __forceinline__ uint32_t ld_volatile(const uint32_t* p) { return *(volatile const uint32_t*)p; }
-__device__ __forceinline__ unsigned long long ld_volatile64(const unsigned long long* p) {
-    return *(volatile const unsigned long long*)p;
+
+// =============================================================== k_segtab
+
+// The reference's dense seg_oldest / seg_newest tables (65536 x num_segs,
+// lz77_hash_build.wgsl:45-54) are never materialised.  Instead every 4 KiB
+// segment is summarised once: its distinct hashes, each with its oldest and
+// newest offset -- exactly the two values the reference's atomicMin /
+// atomicMax leave in table[h][seg] -- and, for every position, the dense id
+// of its hash.  Built in shared memory with an open-addressed table.
+// Positions with p + 2 >= n have no hash, as in the reference build.
+constexpr int kSlots = 8192;
+constexpr size_t kSegtabSmem = 3 * kSlots * 4;
+
+__device__ __forceinline__ uint32_t slot_of(uint32_t h) { return (h * 0x85EBCA6Bu) >> 19; }
+
+template <int T>
+__global__ void __launch_bounds__(T, 2) k_segtab(BatchParams bp) {
+    constexpr int PER = GPZ_SEG / T;
+    constexpr int SPT = kSlots / T;  // slots per thread in the compaction
+    extern __shared__ __align__(16) uint8_t smem[];
+    uint32_t* keyt = reinterpret_cast<uint32_t*>(smem);
+    uint32_t* oldt = keyt + kSlots;
+    uint32_t* newt = oldt + kSlots;
+    __shared__ uint32_t wsum[32];
+    __shared__ uint32_t s_tile;
+    const int tid = threadIdx.x, lane = tid & 31;
+    for (;;) {
+        __syncthreads();
+        if (tid == 0) s_tile = atomicAdd(&bp.counters[GPZ_CNT_SEGSORT], 1u);
+        __syncthreads();
+        const uint32_t t = s_tile;
+        if (t >= bp.ntiles) break;
+        const TileDesc td = bp.tiles[t];
+        const MemberDesc md = bp.members[td.member];
+        const uint32_t n = md.len, start = td.seg << GPZ_SEG_LOG2;
+        const uint32_t cnt = min(GPZ_SEG, n - start);
+        const uint8_t* src = bp.in + md.in_off + start;
+        for (int i = tid; i < kSlots; i += T) {
+            keyt[i] = kEmpty;
+            oldt[i] = kEmpty;
+            newt[i] = 0u;
+        }
+        __syncthreads();
+        uint32_t slot[PER];
+#pragma unroll
+        for (int k = 0; k < PER; k++) {
+            const uint32_t i = tid + k * T;
+            slot[k] = kEmpty;
+            if (i < cnt && start + i + 2u < n) {
+                const uint32_t x = ((uint32_t)src[i] << 16) | ((uint32_t)src[i + 1] << 8) | (uint32_t)src[i + 2];
+                const uint32_t h = (x * 0x9E3779B1u) >> 16;  // hash3, lz77_hash_build.wgsl:36-43
+                uint32_t sl = slot_of(h);
+                for (int probe = 0; probe < kSlots; probe++) {
+                    const uint32_t old = atomicCAS(&keyt[sl], kEmpty, h);
+                    if (old == kEmpty || old == h) break;
+                    sl = (sl + 1u) & (kSlots - 1);
+                }
+                slot[k] = sl;
+            }
+            // lanes of a warp hold consecutive positions: one atomic per run
+            // of equal slots for the oldest (its first lane), one for the
+            // newest (its last lane)
+            const uint32_t prev = __shfl_up_sync(0xFFFFFFFFu, slot[k], 1);
+            const uint32_t next = __shfl_down_sync(0xFFFFFFFFu, slot[k], 1);
+            if (slot[k] != kEmpty) {
+                if (lane == 0 || prev != slot[k]) atomicMin(&oldt[slot[k]], i);
+                if (lane == 31 || next != slot[k]) atomicMax(&newt[slot[k]], i);
+            }
+        }
+        __syncthreads();
+        // dense ids of the occupied slots, in slot order
+        uint32_t occ = 0;
+#pragma unroll
+        for (int q = 0; q < SPT; q++) occ += keyt[tid * SPT + q] != kEmpty;
+        uint32_t nkeys;
+        uint32_t id = block_excl_scan<T>(occ, wsum, &nkeys);
+        uint16_t* keys = bp.seg_keys + (size_t)t * GPZ_SEG;
+        uint32_t* on = bp.seg_on + (size_t)t * GPZ_SEG;
+#pragma unroll
+        for (int q = 0; q < SPT; q++) {
+            const uint32_t sl = tid * SPT + q, kv = keyt[sl];
+            if (kv == kEmpty) continue;
+            keys[id] = (uint16_t)kv;
+            on[id] = newt[sl] | (oldt[sl] << 16);
+            oldt[sl] = id;  // slot -> id from here on
+            id++;
+        }
+        __syncthreads();
+        uint16_t* pos_id = bp.seg_posid + (size_t)t * GPZ_SEG;
+#pragma unroll
+        for (int k = 0; k < PER; k++) {
+            const uint32_t i = tid + k * T;
+            if (i < cnt) pos_id[i] = slot[k] == kEmpty ? (uint16_t)0xFFFFu : (uint16_t)oldt[slot[k]];
+        }
+        if (tid == 0) bp.seg_nkeys[t] = nkeys;
+    }
 }
 
 // ================================================================ k_lookup
 
 struct LookupSmem {
     static constexpr size_t kWin = 0;
-    static constexpr size_t kKeys = kWin + GPZ_WIN_BYTES;
-    static constexpr size_t kNew = kKeys + GPZ_KEY_SLOTS * 4;
-    static constexpr size_t kOld = kNew + GPZ_SEG * 4;
-    static constexpr size_t kBits = kOld + GPZ_SEG * 4;
-    static constexpr size_t kBytes = kBits + 65536 / 8;
+    static constexpr size_t kCand = kWin + GPZ_WIN_BYTES;  // [9][4096] newest | oldest << 16
+    static constexpr size_t kOwnTab = kCand + 9 * GPZ_SEG * 4;
+    static constexpr size_t kBytes = kOwnTab + kSlots * 4;
 };
 
 // One CTA per 4 KiB tile S of a member (persistent over tiles).  The window
 // [S-8, S] plus 320 bytes of lookahead is staged in shared memory.  The
-// reference's dense seg_oldest / seg_newest tables (65536 x num_segs each)
-// are never materialised: only the hashes the tile itself queries matter, so
-// the tile's own keys go into a small open-addressed table (dense ids) and,
-// for each segment S-1 .. S-8 in the reference's order, the oldest / newest
-// positions of exactly those keys are rebuilt with shared-memory atomics.
-// Segments more than 8 back are never reachable: their nearest position is
-// more than 32768 bytes from any p in S, which try_candidate rejects.
-//
-// The per-segment entries are kept with atomicMin only, tagged so that
-// stale values from the previous (higher) segment lose and read as absent:
-//   oldest:  q + 1                       (valid iff <= qbase + 4096)
-//   newest:  2*qbase + 4095 - q          (valid iff <= qbase + 4095)
-// which saves clearing the arrays between segments.
+// tile's distinct hashes go into a shared-memory table; the distinct hashes
+// of segments S-1 .. S-8 are looked up in it, which gives, for every hash of
+// the tile, the newest and oldest position in each of those segments: the
+// reference's table[h][seg] entries, for exactly the hashes this tile
+// queries.  Segments more than 8 back are never reachable: their nearest
+// position is more than 32768 bytes from any p in S, which try_candidate
+// rejects.  Then every position runs the reference's candidate sequence on
+// its own (lz77_hash_lookup.wgsl:138-166): own segment (the newest is always
+// >= p, so only the oldest), then S-1 .. S-8, newest, then oldest while
+// best < 16.
 template <int T>
-__global__ void __launch_bounds__(T, (T >= 1024 ? 1 : 2)) k_lookup(BatchParams bp) {
+__global__ void __launch_bounds__(T, 1) k_lookup(BatchParams bp) {
     constexpr int PER = GPZ_SEG / T;
     extern __shared__ __align__(16) uint8_t smem[];
     uint8_t* win = smem + LookupSmem::kWin;
     uint32_t* w32 = reinterpret_cast<uint32_t*>(win);
-    uint32_t* keytab = reinterpret_cast<uint32_t*>(smem + LookupSmem::kKeys);
-    uint32_t* cnew = reinterpret_cast<uint32_t*>(smem + LookupSmem::kNew);
-    uint32_t* cold = reinterpret_cast<uint32_t*>(smem + LookupSmem::kOld);
-    uint32_t* kbits = reinterpret_cast<uint32_t*>(smem + LookupSmem::kBits);  // presence of each hash
-    __shared__ uint32_t s_tile, s_nkeys;
-    const int tid = threadIdx.x, lane = tid & 31;
+    uint32_t* cand = reinterpret_cast<uint32_t*>(smem + LookupSmem::kCand);
+    uint32_t* owntab = reinterpret_cast<uint32_t*>(smem + LookupSmem::kOwnTab);
+    __shared__ uint32_t s_tile;
+    const int tid = threadIdx.x;
 
     for (;;) {
         __syncthreads();
@@ -224,273 +297,221 @@ __global__ void __launch_bounds__(T, (T >= 1024 ? 1 : 2)) k_lookup(BatchParams b
         const uint32_t w0 = S >= 8u ? (S - 8u) << GPZ_SEG_LOG2 : 0u;
         const uint32_t wvalid = min(n - w0, (uint32_t)GPZ_WIN_BYTES);
         const uint32_t pl0 = start - w0;
+        const uint32_t nback = min(S, 8u);
+        const uint32_t nown = min(bp.seg_nkeys[t], GPZ_SEG);
 
         // ---- stage the window [w0, w0 + wvalid) (16-byte vectors; members
-        // are 16-byte aligned and padded in the batch input)
+        // are 16-byte aligned and padded in the batch input); own-segment
+        // entries; candidate rows cleared
         {
             const uint4* src = reinterpret_cast<const uint4*>(bp.in + md.in_off + w0);
             uint4* dst = reinterpret_cast<uint4*>(win);
             const uint32_t nvec = (wvalid + 15u) >> 4;
             for (uint32_t i = tid; i < nvec; i += T) dst[i] = __ldg(src + i);
-            for (int i = tid; i < GPZ_KEY_SLOTS; i += T) keytab[i] = kEmpty;
-            for (int i = tid; i < 65536 / 32; i += T) kbits[i] = 0u;
-            for (int i = tid; i < GPZ_SEG; i += T) {
-                cnew[i] = kEmpty;
-                cold[i] = kEmpty;
-            }
-            if (tid == 0) s_nkeys = 0;
+            const uint32_t* go = bp.seg_on + (size_t)t * GPZ_SEG;
+            for (uint32_t i = tid; i < nown; i += T) cand[i] = go[i];
+            for (uint32_t i = tid; i < nback * GPZ_SEG; i += T) cand[GPZ_SEG + i] = kEmpty;
+            for (int i = tid; i < kSlots; i += T) owntab[i] = kEmpty;
             __syncthreads();
             const uint32_t zend = min((uint32_t)GPZ_WIN_BYTES, (nvec << 4) + 32u);
             for (uint32_t i = wvalid + tid; i < zend; i += T) win[i] = 0;
+            const uint16_t* gk = bp.seg_keys + (size_t)t * GPZ_SEG;
+            for (uint32_t i = tid; i < nown; i += T) {
+                const uint32_t h = gk[i];
+                uint32_t sl = slot_of(h);
+                for (int probe = 0; probe < kSlots; probe++) {
+                    if (atomicCAS(&owntab[sl], kEmpty, h | (i << 16)) == kEmpty) break;
+                    sl = (sl + 1u) & (kSlots - 1);
+                }
+            }
+        }
+        uint32_t myid[PER];
+        const uint16_t* gpos = bp.seg_posid + (size_t)t * GPZ_SEG;
+#pragma unroll
+        for (int k = 0; k < PER; k++) {
+            const uint32_t i = tid + k * T;
+            myid[k] = i < cnt ? (uint32_t)gpos[i] : 0xFFFFu;
         }
         __syncthreads();
 
-        // ---- insert the tile's own hash keys (p + 2 < n)
-        uint32_t info[PER];  // slot | h << 13, or kEmpty
-        uint32_t own = 0;
-#pragma unroll
-        for (int k = 0; k < PER; k++) {
-            const uint32_t i = tid + k * T, p = start + i;
-            info[k] = kEmpty;
-            if (i < cnt && p + 2u < n) {
-                const uint32_t h = hash_at(w32, pl0 + i);
-                uint32_t s = key_slot(h);
-                for (;;) {
-                    uint32_t old = atomicCAS(&keytab[s], kEmpty, h);
-                    if (old == kEmpty) {
-                        own |= 1u << k;
-                        atomicOr(&kbits[h >> 5], 1u << (h & 31u));
+        // ---- join: the distinct hashes of segments S-1 .. S-8 probe the
+        // tile's table (each segment writes its own candidate row)
+        for (uint32_t back = 1; back <= nback; back++) {
+            const uint32_t ts = t - back;  // a member's tiles are consecutive
+            const uint32_t ns = min(bp.seg_nkeys[ts], GPZ_SEG);
+            const uint16_t* gk = bp.seg_keys + (size_t)ts * GPZ_SEG;
+            const uint32_t* go = bp.seg_on + (size_t)ts * GPZ_SEG;
+            uint32_t* cb = cand + back * GPZ_SEG;
+            for (uint32_t j = tid; j < ns; j += T) {
+                const uint32_t h = gk[j];
+                uint32_t sl = slot_of(h);
+                for (int probe = 0; probe < kSlots; probe++) {
+                    const uint32_t wv = owntab[sl];
+                    if (wv == kEmpty) break;
+                    if ((wv & 0xFFFFu) == h) {
+                        cb[(wv >> 16) & (GPZ_SEG - 1)] = go[j];
                         break;
                     }
-                    if (old == h) break;
-                    s = (s + 1u) & (GPZ_KEY_SLOTS - 1);
+                    sl = (sl + 1u) & (kSlots - 1);
                 }
-                info[k] = s | (h << 13);
             }
         }
         __syncthreads();
-        // dense ids for the distinct keys (warp-aggregated)
-#pragma unroll
-        for (int k = 0; k < PER; k++) {
-            const bool o = (own >> k) & 1u;
-            const uint32_t m = __ballot_sync(0xFFFFFFFFu, o);
-            uint32_t base = 0;
-            if (lane == 0 && m) base = atomicAdd(&s_nkeys, __popc(m));
-            base = __shfl_sync(0xFFFFFFFFu, base, 0);
-            if (o) {
-                const uint32_t id = base + __popc(m & ((1u << lane) - 1u));
-                keytab[info[k] & (GPZ_KEY_SLOTS - 1)] = (info[k] >> 13) | (id << 16);
-            }
-        }
-        __syncthreads();
-        uint32_t myid[PER];
-        uint32_t best[PER];
-#pragma unroll
-        for (int k = 0; k < PER; k++) {
-            myid[k] = info[k] == kEmpty ? kEmpty : keytab[info[k] & (GPZ_KEY_SLOTS - 1)] >> 16;
-            best[k] = 0;
-        }
 
-        // ---- own segment: the newest entry is always >= p (p itself is in
-        // the table), so only the oldest can be a candidate
-#pragma unroll
-        for (int k = 0; k < PER; k++) {
-            const uint32_t id = myid[k];
-            if (!__ballot_sync(0xFFFFFFFFu, id != kEmpty)) continue;
-            const uint32_t grp = __match_any_sync(0xFFFFFFFFu, id == kEmpty ? 0x10000u + lane : id);
-            if (id != kEmpty && lane == __ffs(grp) - 1) atomicMin(&cold[id], start + tid + k * T + 1u);
-        }
-        __syncthreads();
-#pragma unroll
-        for (int k = 0; k < PER; k++)
-            if (myid[k] != kEmpty) try_cand(win, w32, cold[myid[k]], start + tid + k * T, n, w0, best[k]);
-
-        // ---- segments S-1 .. S-8 in the reference's order: newest, then
-        // oldest while best < 16 (lz77_hash_lookup.wgsl:138-166)
-        for (uint32_t back = 1; back <= 8u && back <= S; back++) {
-            const uint32_t qbase = (S - back) << GPZ_SEG_LOG2;
-            __syncthreads();  // the previous segment's reads are done
-#pragma unroll
-            for (int k = 0; k < PER; k++) {
-                const uint32_t i = tid + k * T, q = qbase + i;
-                uint32_t id = kEmpty;
-                if (q + 2u < n) {
-                    const uint32_t h = hash_at(w32, q - w0);
-                    if ((kbits[h >> 5] >> (h & 31u)) & 1u) {
-                        uint32_t s = key_slot(h);
-                        for (;;) {
-                            const uint32_t wv = keytab[s];
-                            if (wv == kEmpty) break;
-                            if ((wv & 0xFFFFu) == h) {
-                                id = wv >> 16;
-                                break;
-                            }
-                            s = (s + 1u) & (GPZ_KEY_SLOTS - 1);
-                        }
-                    }
-                }
-                if (!__ballot_sync(0xFFFFFFFFu, id != kEmpty)) continue;
-                const uint32_t grp = __match_any_sync(0xFFFFFFFFu, id == kEmpty ? 0x10000u + lane : id);
-                if (id != kEmpty) {
-                    if (lane == __ffs(grp) - 1) atomicMin(&cold[id], q + 1u);
-                    if (lane == 31 - __clz(grp)) atomicMin(&cnew[id], 2u * qbase + 4095u - q);
-                }
-            }
-            __syncthreads();
-#pragma unroll
-            for (int k = 0; k < PER; k++) {
-                const uint32_t id = myid[k];
-                if (id == kEmpty) continue;
-                const uint32_t p = start + tid + k * T;
-                const uint32_t en = cnew[id];
-                const uint32_t rn = en <= qbase + 4095u ? 2u * qbase + 4096u - en : 0u;  // q + 1, or absent
-                try_cand(win, w32, rn, p, n, w0, best[k]);
-                if ((best[k] >> 16) < 16u) {
-                    const uint32_t ro = cold[id];
-                    if (ro <= qbase + GPZ_SEG && ro != rn) try_cand(win, w32, ro, p, n, w0, best[k]);
-                }
-            }
-        }
-
-        // ---- per-position packed tokens
+        // ---- every position walks its candidates in the reference's order
         uint32_t* dst = bp.pp + md.in_off + start;
 #pragma unroll
         for (int k = 0; k < PER; k++) {
             const uint32_t i = tid + k * T;
-            if (i < cnt) dst[i] = (best[k] >> 16) ? best[k] : (uint32_t)win[pl0 + i];
+            if (i >= cnt) continue;
+            const uint32_t id = myid[k], p = start + i;
+            uint32_t best = 0;
+            if (id != 0xFFFFu) {
+                try_cand(win, w32, start + (cand[id] >> 16) + 1u, p, n, w0, best);
+                for (uint32_t back = 1; back <= nback; back++) {
+                    const uint32_t on = cand[back * GPZ_SEG + id];
+                    if (on == kEmpty) continue;
+                    const uint32_t qb = (S - back) << GPZ_SEG_LOG2;
+                    const uint32_t rn = qb + (on & 0xFFFFu) + 1u;
+                    try_cand(win, w32, rn, p, n, w0, best);
+                    if ((best >> 16) < 16u) {
+                        const uint32_t ro = qb + (on >> 16) + 1u;
+                        if (ro != rn) try_cand(win, w32, ro, p, n, w0, best);
+                    }
+                }
+            }
+            dst[i] = (best >> 16) ? best : (uint32_t)win[pl0 + i];
         }
     }
 }
 
 // ================================================================== k_walk
 
-struct WalkSmem {
-    uint32_t pps[GPZ_SEG + 1];
-    uint16_t nxt[GPZ_SEG];
-    uint16_t J[2][GPZ_SEG + GPZ_EXITS];
-    uint8_t mark[GPZ_SEG];
-    uint32_t hist[GPZ_NSYM];
-    uint32_t wsum[32];
-    uint32_t tile, entry;
+// The lazy walk of lz77.rs:260-284 visits p, next(p), next(next(p)), ...
+// where next(p) depends only on pp[p] and pp[p+1].  Each 4 KiB tile is walked
+// independently by pointer jumping over next links: k_walk_exit computes,
+// for every position a walk can enter the tile at (its first 258 positions),
+// where it leaves; k_chain strings the tiles of a member together (entry of
+// tile b+1 = exit of tile b at its entry); k_walk_mark then marks the visited
+// positions from the known entry and emits them in order.
+
+struct WalkLinks {
+    uint32_t pps[GPZ_SEG + 1];              // pp of the tile and one lookahead
+    uint16_t nxt[GPZ_SEG];                  // next position, tile-relative
+    uint16_t J[2][GPZ_SEG + GPZ_EXITS];     // doubled links, absorbing past the tile
 };
 
 template <int T>
-__global__ void __launch_bounds__(T) k_walk(BatchParams bp) {
-    constexpr int PER = GPZ_SEG / T;
-    __shared__ WalkSmem sm;
-    const int tid = threadIdx.x;
+__device__ void walk_links(const BatchParams& bp, const MemberDesc& md, uint32_t start, uint32_t cnt, WalkLinks& w) {
+    const uint32_t n = md.len;
+    const uint32_t* ppg = bp.pp + md.in_off + start;
+    for (uint32_t i = threadIdx.x; i < cnt; i += T) w.pps[i] = ppg[i];
+    if (threadIdx.x == 0) w.pps[cnt] = (start + cnt < n) ? ppg[cnt] : 0u;
+    for (uint32_t i = cnt + threadIdx.x; i < cnt + GPZ_EXITS; i += T) {
+        w.J[0][i] = (uint16_t)i;
+        w.J[1][i] = (uint16_t)i;
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < cnt; i += T) {
+        const uint32_t l = w.pps[i] >> 16;
+        uint32_t nx = i + 1u;
+        if (l) {
+            const uint32_t l1 = w.pps[i + 1] >> 16;
+            const bool demote = (start + i + 1u < n) && l1 != 0u && l1 > l;  // lz77.rs:273-278
+            if (!demote) nx = i + l;
+        }
+        w.nxt[i] = (uint16_t)nx;
+        w.J[0][i] = (uint16_t)nx;
+    }
+    __syncthreads();
+}
 
+template <int T>
+__global__ void __launch_bounds__(T) k_walk_exit(BatchParams bp) {
+    __shared__ WalkLinks w;
+    __shared__ uint32_t s_tile;
+    const int tid = threadIdx.x;
     for (;;) {
         __syncthreads();
-        if (tid == 0) sm.tile = atomicAdd(&bp.counters[GPZ_CNT_WALK], 1u);
+        if (tid == 0) s_tile = atomicAdd(&bp.counters[GPZ_CNT_EXIT], 1u);
         __syncthreads();
-        const uint32_t t = sm.tile;
+        const uint32_t t = s_tile;
         if (t >= bp.ntiles) break;
         const TileDesc td = bp.tiles[t];
         const MemberDesc md = bp.members[td.member];
-        const uint32_t n = md.len, b = td.seg, start = b << GPZ_SEG_LOG2;
-        const uint32_t cnt = min(GPZ_SEG, n - start);
-        const uint32_t* ppg = bp.pp + md.in_off + start;
-
-        for (uint32_t i = tid; i < cnt; i += T) sm.pps[i] = ppg[i];
-        if (tid == 0) sm.pps[cnt] = (start + cnt < n) ? ppg[cnt] : 0u;
-        for (int i = tid; i < GPZ_NSYM; i += T) sm.hist[i] = 0;
-        for (uint32_t i = cnt + tid; i < cnt + GPZ_EXITS; i += T) {
-            sm.J[0][i] = (uint16_t)i;
-            sm.J[1][i] = (uint16_t)i;
-        }
-        __syncthreads();
-
-        // next-position links (lz77.rs:265-281)
-        for (uint32_t i = tid; i < cnt; i += T) {
-            const uint32_t t0 = sm.pps[i], l = t0 >> 16;
-            uint32_t nx = i + 1u;
-            if (l) {
-                const uint32_t l1 = sm.pps[i + 1] >> 16;
-                const bool demote = (start + i + 1u < n) && l1 != 0u && l1 > l;
-                if (!demote) nx = i + l;
-            }
-            sm.nxt[i] = (uint16_t)nx;
-            sm.J[0][i] = (uint16_t)nx;
-        }
-        __syncthreads();
-
-        // pointer jumping: J = next^(2^r), absorbing at >= cnt
+        if (td.seg + 1u == md.ntiles) continue;  // the member's last tile has no successor
+        const uint32_t start = td.seg << GPZ_SEG_LOG2, cnt = GPZ_SEG;
+        walk_links<T>(bp, md, start, cnt, w);
         int cur = 0;
         for (int r = 0; r < 16; r++) {
             int ch = 0;
             for (uint32_t i = tid; i < cnt; i += T) {
-                const uint32_t j = sm.J[cur][i];
-                const uint32_t nj = j < cnt ? sm.J[cur][j] : j;
-                sm.J[cur ^ 1][i] = (uint16_t)nj;
+                const uint32_t j = w.J[cur][i];
+                const uint32_t nj = j < cnt ? w.J[cur][j] : j;
+                w.J[cur ^ 1][i] = (uint16_t)nj;
                 ch |= nj != j;
             }
             cur ^= 1;
             if (!__syncthreads_or(ch)) break;
         }
+        for (int e = tid; e < GPZ_EXITS; e += T)
+            bp.tile_exit[(size_t)t * GPZ_EXITS + e] = (uint16_t)(w.J[cur][e] - cnt);
+    }
+}
 
-        // publish the exit table (entry offset -> entry offset into the
-        // next tile); the member's last tile has no successor
-        const bool last = b + 1u == md.ntiles;
-        if (!last)
-            for (int e = tid; e < GPZ_EXITS; e += T)
-                bp.tile_exit[(size_t)t * GPZ_EXITS + e] = (uint16_t)(sm.J[cur][e] - cnt);
-        __threadfence();
-        __syncthreads();
-        if (tid == 0) {
-            uint32_t e = 0;
-            if (b > 0) {
-                atomicExch(&bp.tile_status[t], GPZ_ST_AGG);
-                uint32_t j = t - 1u, spins = 0;
-                for (;;) {
-                    const uint32_t s = ld_volatile(&bp.tile_status[j]);
-                    if (s & GPZ_ST_INCL) {
-                        e = s & 0xFFFFu;
-                        break;
-                    }
-                    if ((s & GPZ_ST_AGG) && j > md.tile_base) {
-                        j--;
-                        continue;
-                    }
-                    if (++spins > kSpinLimit) {
-                        atomicOr(bp.err, GPZ_ERRBIT_SPIN);
-                        e = 0;
-                        break;
-                    }
-                    __nanosleep(64);
-                }
-                __threadfence();
-                for (uint32_t k = j + 1u; k < t; k++) {
-                    e = bp.tile_exit[(size_t)k * GPZ_EXITS + min(e, (uint32_t)GPZ_EXITS - 1u)];
-                }
-            }
-            sm.entry = e;
-            const uint32_t nexte = e < cnt ? (uint32_t)sm.J[cur][e] - cnt : e - cnt;
-            __threadfence();
-            atomicExch(&bp.tile_status[t], GPZ_ST_INCL | (nexte & 0xFFFFu));
-        }
-        __syncthreads();
-        const uint32_t entry = sm.entry;
+// Entry offset of every tile: one thread per member follows the exit tables.
+__global__ void k_chain(BatchParams bp) {
+    const uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= bp.nmembers) return;
+    const MemberDesc md = bp.members[m];
+    uint32_t e = 0;
+    for (uint32_t b = 0; b < md.ntiles; b++) {
+        const uint32_t t = md.tile_base + b;
+        bp.tile_entry[t] = e;
+        if (b + 1u < md.ntiles) e = bp.tile_exit[(size_t)t * GPZ_EXITS + min(e, (uint32_t)GPZ_EXITS - 1u)];
+    }
+}
 
-        // mark the positions the walk visits, by doubling from the entry:
-        // before round r the marks are next^k(entry), k < 2^r
-        for (uint32_t i = tid; i < cnt; i += T) {
-            sm.mark[i] = 0xFF;
-            sm.J[0][i] = sm.nxt[i];
-        }
+struct MarkSmem {
+    WalkLinks w;
+    uint8_t mark[GPZ_SEG];
+    uint32_t hist[GPZ_NSYM];
+    uint32_t wsum[32];
+    uint32_t tile;
+};
+
+template <int T>
+__global__ void __launch_bounds__(T) k_walk_mark(BatchParams bp) {
+    constexpr int PER = GPZ_SEG / T;
+    __shared__ MarkSmem sm;
+    const int tid = threadIdx.x;
+    for (;;) {
         __syncthreads();
+        if (tid == 0) sm.tile = atomicAdd(&bp.counters[GPZ_CNT_MARK], 1u);
+        __syncthreads();
+        const uint32_t t = sm.tile;
+        if (t >= bp.ntiles) break;
+        const TileDesc td = bp.tiles[t];
+        const MemberDesc md = bp.members[td.member];
+        const uint32_t n = md.len, start = td.seg << GPZ_SEG_LOG2;
+        const uint32_t cnt = min(GPZ_SEG, n - start);
+        for (int i = tid; i < GPZ_NSYM; i += T) sm.hist[i] = 0;
+        for (uint32_t i = tid; i < cnt; i += T) sm.mark[i] = 0xFF;
+        walk_links<T>(bp, md, start, cnt, sm.w);
+        const uint32_t entry = bp.tile_entry[t];
         if (tid == 0 && entry < cnt) sm.mark[entry] = 0;
         __syncthreads();
-        cur = 0;
+        // before round r the marked positions are next^k(entry), k < 2^r
+        int cur = 0;
         for (int r = 0; r < 16; r++) {
             int add = 0;
             for (uint32_t i = tid; i < cnt; i += T) {
-                const uint32_t j = sm.J[cur][i];
+                const uint32_t j = sm.w.J[cur][i];
                 if (sm.mark[i] <= (uint32_t)r && j < cnt) {
                     sm.mark[j] = (uint8_t)(r + 1);
                     add = 1;
                 }
-                sm.J[cur ^ 1][i] = (uint16_t)(j < cnt ? sm.J[cur][j] : j);
+                sm.w.J[cur ^ 1][i] = (uint16_t)(j < cnt ? sm.w.J[cur][j] : j);
             }
             cur ^= 1;
             if (!__syncthreads_or(add)) break;
@@ -513,9 +534,9 @@ __global__ void __launch_bounds__(T) k_walk(BatchParams bp) {
         for (int k = 0; k < PER; k++) {
             if (!((vis >> k) & 1u)) continue;
             const uint32_t i = i0 + k;
-            uint32_t tv = sm.pps[i];
+            uint32_t tv = sm.w.pps[i];
             const uint32_t l = tv >> 16;
-            if (l && sm.nxt[i] == i + 1u) tv = bp.in[md.in_off + start + i];  // lazy demotion
+            if (l && sm.w.nxt[i] == i + 1u) tv = bp.in[md.in_off + start + i];  // lazy demotion to a literal
             tg[idx++] = tv;
             if ((tv >> 16) == 0) {
                 atomicAdd(&sm.hist[tv & 0xFFu], 1u);
@@ -533,35 +554,57 @@ __global__ void __launch_bounds__(T) k_walk(BatchParams bp) {
 
 // ================================================================== k_huff
 
-constexpr int kHuffThreads = 320;
+constexpr int kHuffThreads = 256;
 constexpr int kCrcSlices = 256;  // threads folding member bytes into the CRC
 
 struct TreeScratch {
+    uint32_t key[512];  // (weight << 9 | symbol), sorted; unused = 0xFFFFFFFF
     uint32_t w[GPZ_NLIT];
-    uint16_t order[GPZ_NLIT];
-    uint16_t lparent[GPZ_NLIT];
     uint32_t ifreq[GPZ_NLIT];
+    uint16_t lparent[GPZ_NLIT];
     uint16_t iparent[GPZ_NLIT];
-    uint16_t idepth[GPZ_NLIT];
+    uint16_t dep[2][GPZ_NLIT];
+    uint16_t anc[2][GPZ_NLIT];
 };
+
+__device__ __forceinline__ void warp_bitonic_sort(uint32_t* key, int npad) {
+    const int lane = threadIdx.x & 31;
+    for (int size = 2; size <= npad; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int i = lane; i < npad / 2; i += 32) {
+                const int lo = 2 * i - (i & (stride - 1)), hi = lo + stride;
+                const bool up = (lo & size) == 0;
+                const uint32_t a = key[lo], b = key[hi];
+                if ((a > b) == up) {
+                    key[lo] = b;
+                    key[hi] = a;
+                }
+            }
+            __syncwarp();
+        }
+    }
+}
 
 // try_build_code_lengths (huffman.rs:26-60) for one alphabet, run by one
 // warp.  standard_huffman's min-heap on (freq, id) is evaluated as a
 // two-queue merge: leaves sorted by (freq, id), internal nodes in creation
 // order; a leaf wins a tie with an internal node because its id is smaller.
+// Depths (huffman.rs:102-117) come from pointer jumping over parent links.
 __device__ bool warp_code_lengths(const uint32_t* freq, int nsym, int max_bits, uint8_t* lens, TreeScratch& s) {
     const int lane = threadIdx.x & 31;
     int used = 0, only = -1;
     for (int i = lane; i < nsym; i += 32) {
-        s.w[i] = freq[i];
+        const uint32_t f = freq[i];
+        s.w[i] = f;
         lens[i] = 0;
-    }
-    __syncwarp();
-    for (int i = 0; i < nsym; i++)
-        if (s.w[i]) {
+        if (f) {
             used++;
             only = i;
         }
+    }
+    used = __reduce_add_sync(0xFFFFFFFFu, used);
+    only = __reduce_max_sync(0xFFFFFFFFu, only + 1) - 1;
+    __syncwarp();
     if (used == 0) return true;
     if (used == 1) {
         if (lane == 0) lens[only] = 1;
@@ -571,43 +614,60 @@ __device__ bool warp_code_lengths(const uint32_t* freq, int nsym, int max_bits, 
     int required = 0;
     while ((1 << required) < used) required++;
     if (required > max_bits) return false;
+    int npad = 32;
+    while (npad < nsym) npad <<= 1;
+    const int nint = used - 1, root = nint - 1;
     for (int iter = 0; iter < 64; iter++) {
-        for (int i = lane; i < nsym; i += 32) {
-            const uint32_t wi = s.w[i];
-            if (!wi) continue;
-            int r = 0;
-            for (int j = 0; j < nsym; j++) {
-                const uint32_t wj = s.w[j];
-                r += wj && (wj < wi || (wj == wi && j < i));
-            }
-            s.order[r] = (uint16_t)i;
-        }
+        for (int i = lane; i < npad; i += 32) s.key[i] = (i < nsym && s.w[i]) ? ((s.w[i] << 9) | (uint32_t)i) : 0xFFFFFFFFu;
         __syncwarp();
-        int mx = 0;
+        warp_bitonic_sort(s.key, npad);
         if (lane == 0) {
-            int li = 0, ii = 0, nint = 0;
-            for (int k = 0; k < used - 1; k++) {
-                uint32_t f[2];
+            const uint32_t INF = 0xFFFFFFFFu;
+            int li = 0, ii = 0, ni = 0;
+            uint32_t lf = s.key[0] >> 9, fi = INF;
+            for (int k = 0; k < nint; k++) {
+                uint32_t f2[2];
+#pragma unroll
                 for (int q = 0; q < 2; q++) {
-                    if (li < used && (ii >= nint || s.w[s.order[li]] <= s.ifreq[ii])) {
-                        f[q] = s.w[s.order[li]];
-                        s.lparent[li++] = (uint16_t)nint;
+                    if (li < used && lf <= fi) {
+                        f2[q] = lf;
+                        s.lparent[li++] = (uint16_t)ni;
+                        lf = li < used ? (s.key[li] >> 9) : INF;
                     } else {
-                        f[q] = s.ifreq[ii];
-                        s.iparent[ii++] = (uint16_t)nint;
+                        f2[q] = fi;
+                        s.iparent[ii++] = (uint16_t)ni;
+                        fi = ii < ni ? s.ifreq[ii] : INF;
                     }
                 }
-                s.ifreq[nint++] = f[0] + f[1];
-            }
-            s.idepth[nint - 1] = 0;
-            for (int j = nint - 2; j >= 0; j--) s.idepth[j] = (uint16_t)(s.idepth[s.iparent[j]] + 1);
-            for (int k = 0; k < used; k++) {
-                int d = s.idepth[s.lparent[k]] + 1;
-                lens[s.order[k]] = (uint8_t)d;
-                mx = d > mx ? d : mx;
+                const uint32_t nf = f2[0] + f2[1];
+                s.ifreq[ni] = nf;
+                if (ii == ni) fi = nf;
+                ni++;
             }
         }
-        mx = __shfl_sync(0xFFFFFFFFu, mx, 0);
+        __syncwarp();
+        for (int j = lane; j < nint; j += 32) {
+            s.anc[0][j] = (uint16_t)(j == root ? root : s.iparent[j]);
+            s.dep[0][j] = (uint16_t)(j == root ? 0 : 1);
+        }
+        __syncwarp();
+        int cur = 0;
+        for (int r = 0; r < 9; r++) {
+            for (int j = lane; j < nint; j += 32) {
+                const int a = s.anc[cur][j];
+                s.dep[cur ^ 1][j] = (uint16_t)(s.dep[cur][j] + s.dep[cur][a]);
+                s.anc[cur ^ 1][j] = s.anc[cur][a];
+            }
+            cur ^= 1;
+            __syncwarp();
+        }
+        int mx = 0;
+        for (int k = lane; k < used; k += 32) {
+            const int d = s.dep[cur][s.lparent[k]] + 1;
+            lens[s.key[k] & 511u] = (uint8_t)d;
+            mx = d > mx ? d : mx;
+        }
+        mx = __reduce_max_sync(0xFFFFFFFFu, mx);
         __syncwarp();
         if (mx <= max_bits) return true;
         for (int i = lane; i < nsym; i += 32)
@@ -619,23 +679,37 @@ __device__ bool warp_code_lengths(const uint32_t* freq, int nsym, int max_bits, 
 
 __device__ __forceinline__ uint32_t rev_code(uint32_t code, uint32_t bits) { return bits ? __brev(code) >> (32u - bits) : 0u; }
 
-// canonical_codes (huffman.rs:122-152), packed as reversed code | len << 16.
-__device__ void canonical_packed(const uint8_t* lens, int nsym, uint32_t* out) {
-    uint32_t bl_count[16] = {0}, next_code[16] = {0};
-    int max_bits = 0;
-    for (int i = 0; i < nsym; i++) {
-        bl_count[lens[i]]++;
-        max_bits = lens[i] > max_bits ? lens[i] : max_bits;
+// canonical_codes (huffman.rs:122-152) by one warp, packed as reversed code
+// | len << 16: per-length counts and ranks from ballots over 32 symbols.
+__device__ void warp_canonical(const uint8_t* lens, int nsym, uint32_t* out) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t lt = (1u << lane) - 1u;
+    uint32_t cnt[16];
+#pragma unroll
+    for (int L = 0; L < 16; L++) cnt[L] = 0;
+    for (int base = 0; base < nsym; base += 32) {
+        const uint32_t l = base + lane < nsym ? lens[base + lane] : 0u;
+#pragma unroll
+        for (int L = 1; L < 16; L++) cnt[L] += __popc(__ballot_sync(0xFFFFFFFFu, l == (uint32_t)L));
     }
-    bl_count[0] = 0;
+    uint32_t next[16];
     uint32_t code = 0;
-    for (int bits = 1; bits <= max_bits; bits++) {
-        code = (code + bl_count[bits - 1]) << 1;
-        next_code[bits] = code;
+    next[0] = 0;
+#pragma unroll
+    for (int bits = 1; bits < 16; bits++) {
+        code = (code + (bits > 1 ? cnt[bits - 1] : 0u)) << 1;
+        next[bits] = code;
     }
-    for (int s = 0; s < nsym; s++) {
-        const uint32_t l = lens[s];
-        out[s] = l ? (rev_code(next_code[l]++, l) | (l << 16)) : 0u;
+    for (int base = 0; base < nsym; base += 32) {
+        const uint32_t l = base + lane < nsym ? lens[base + lane] : 0u;
+        uint32_t mine = 0;
+#pragma unroll
+        for (int L = 1; L < 16; L++) {
+            const uint32_t m = __ballot_sync(0xFFFFFFFFu, l == (uint32_t)L);
+            if (l == (uint32_t)L) mine = next[L] + __popc(m & lt);
+            next[L] += __popc(m);
+        }
+        if (base + lane < nsym) out[base + lane] = l ? (rev_code(mine, l) | (l << 16)) : 0u;
     }
 }
 
@@ -651,16 +725,18 @@ struct HuffSmem {
     uint32_t meta_freq[19];
     uint8_t meta_lens[19];
     uint32_t meta_codes[19];
-    uint32_t hdr[GPZ_MAX_HEADER_WORDS + 2];
+    uint32_t hdr[GPZ_HDR_WORDS];
     uint32_t tile_bits[512];
     uint32_t red[32];
     uint32_t crctab[8 * 256];
     uint32_t crcv[kCrcSlices];
     uint32_t crcx[8];
-    unsigned long long gz_off;
     uint32_t member, hbits, total, nrle, nlit, ndist, ok, crc;
 };
 
+// Per member: code lengths and codes, the dynamic block header
+// (deflate.rs:830-932), the exact bit plan of every tile, the member's
+// DEFLATE size and its CRC-32.  Members are independent: no waiting.
 __global__ void __launch_bounds__(kHuffThreads) k_huff(BatchParams bp) {
     __shared__ HuffSmem sm;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -690,11 +766,11 @@ __global__ void __launch_bounds__(kHuffThreads) k_huff(BatchParams bp) {
         const MemberDesc md = bp.members[m];
 
         // member symbol counts = sum of its tiles' histograms, + EOB
-        if (tid < GPZ_NSYM) {
+        for (int q = tid; q < GPZ_NSYM; q += kHuffThreads) {
             uint32_t f = 0;
-            const uint16_t* h = bp.tile_hist + (size_t)md.tile_base * GPZ_NSYM + tid;
+            const uint16_t* h = bp.tile_hist + (size_t)md.tile_base * GPZ_NSYM + q;
             for (uint32_t j = 0; j < md.ntiles; j++) f += h[(size_t)j * GPZ_NSYM];
-            sm.freq[tid] = f + (tid == 256 ? 1u : 0u);
+            sm.freq[q] = f + (q == 256 ? 1u : 0u);
         }
         if (tid == 0) sm.ok = 1;
 
@@ -712,8 +788,8 @@ __global__ void __launch_bounds__(kHuffThreads) k_huff(BatchParams bp) {
                 uint32_t c = 0;
                 for (uint32_t v = tid * per; v < (tid + 1) * per; v++) {
                     if (v < padw) continue;
-                    const uint2 w = __ldg(words + (v - padw));
-                    const uint32_t lo = w.x ^ c, hi = w.y;
+                    const uint2 wv = __ldg(words + (v - padw));
+                    const uint32_t lo = wv.x ^ c, hi = wv.y;
                     c = sm.crctab[7 * 256 + (lo & 0xFFu)] ^ sm.crctab[6 * 256 + ((lo >> 8) & 0xFFu)] ^
                         sm.crctab[5 * 256 + ((lo >> 16) & 0xFFu)] ^ sm.crctab[4 * 256 + (lo >> 24)] ^
                         sm.crctab[3 * 256 + (hi & 0xFFu)] ^ sm.crctab[2 * 256 + ((hi >> 8) & 0xFFu)] ^
@@ -741,7 +817,6 @@ __global__ void __launch_bounds__(kHuffThreads) k_huff(BatchParams bp) {
                 sm.crc = ~(gf2_mulmod(0xFFFFFFFFu, x8pow(L)) ^ c);
             }
         }
-        __syncthreads();
 
         // litlen (warp 0) and distance (warp 1) code lengths, 15-bit limit
         if (warp < 2) {
@@ -752,30 +827,38 @@ __global__ void __launch_bounds__(kHuffThreads) k_huff(BatchParams bp) {
         }
         __syncthreads();
 
-        // fix-ups (deflate.rs:854-867), codes, trims, RLE (deflate.rs:254-326)
-        if (tid == 0) {
+        // fix-ups (deflate.rs:854-867)
+        if (warp == 0) {
             uint8_t* ll = sm.lens;
             uint8_t* dl = sm.lens + GPZ_NLIT;
-            int used_d = 0, only = -1, used_l = 0;
-            for (int i = 0; i < GPZ_NDIST; i++)
-                if (dl[i]) {
-                    if (only < 0) only = i;
-                    used_d++;
+            const uint32_t dm = __ballot_sync(0xFFFFFFFFu, lane < GPZ_NDIST && dl[lane] != 0);
+            int used_l = 0;
+            for (int i = lane; i < GPZ_NLIT; i += 32) used_l += ll[i] != 0;
+            used_l = __reduce_add_sync(0xFFFFFFFFu, used_l);
+            __syncwarp();
+            if (lane == 0) {
+                if (dm == 0) {
+                    dl[0] = 1;
+                    dl[1] = 1;
+                } else if (__popc(dm) == 1) {
+                    const int only = __ffs(dm) - 1;
+                    dl[only] = 1;
+                    dl[1 - (only < 1 ? only : 1)] = 1;
                 }
-            if (used_d == 0) {
-                dl[0] = 1;
-                dl[1] = 1;
-            } else if (used_d == 1) {
-                dl[only] = 1;
-                dl[1 - (only < 1 ? only : 1)] = 1;
+                if (used_l < 2) {
+                    ll[0] = 1;
+                    ll[256] = 1;
+                }
             }
-            for (int i = 0; i < GPZ_NLIT; i++) used_l += ll[i] != 0;
-            if (used_l < 2) {
-                ll[0] = 1;
-                ll[256] = 1;
-            }
-            canonical_packed(ll, GPZ_NLIT, sm.codes);
-            canonical_packed(dl, GPZ_NDIST, sm.codes + GPZ_NLIT);
+            __syncwarp();
+        }
+        __syncthreads();
+        // canonical codes (warps 0, 1); trims + RLE (deflate.rs:254-335) on warp 2
+        if (warp == 0) warp_canonical(sm.lens, GPZ_NLIT, sm.codes);
+        else if (warp == 1) warp_canonical(sm.lens + GPZ_NLIT, GPZ_NDIST, sm.codes + GPZ_NLIT);
+        else if (warp == 2 && lane == 0) {
+            const uint8_t* ll = sm.lens;
+            const uint8_t* dl = sm.lens + GPZ_NLIT;
             int nlit = GPZ_NLIT;
             while (nlit > 257 && ll[nlit - 1] == 0) nlit--;
             int ndist = GPZ_NDIST;
@@ -836,25 +919,29 @@ __global__ void __launch_bounds__(kHuffThreads) k_huff(BatchParams bp) {
             sm.ndist = (uint32_t)ndist;
         }
         __syncthreads();
-        // meta code lengths, 7-bit limit (deflate.rs:896-903)
+        // meta code lengths, 7-bit limit (deflate.rs:896-903), and codes
         if (warp == 0) {
             const bool ok = warp_code_lengths(sm.meta_freq, 19, 7, sm.meta_lens, sm.tree[0]);
             if (!ok && lane == 0) sm.ok = 0;
+            __syncwarp();
+            warp_canonical(sm.meta_lens, 19, sm.meta_codes);
         }
         __syncthreads();
-        // header bits (deflate.rs:911-932), LSB first
+        // header bits (deflate.rs:911-932), LSB first, one 64-bit accumulator
         if (tid == 0) {
-            canonical_packed(sm.meta_lens, 19, sm.meta_codes);
             int hclen = 19;
             while (hclen > 4 && sm.meta_lens[c_meta_order[hclen - 1]] == 0) hclen--;
-            for (int q = 0; q < GPZ_MAX_HEADER_WORDS + 2; q++) sm.hdr[q] = 0;
-            uint32_t pos = 0;
-            auto put = [&](uint32_t v, uint32_t nb) {
-                if (!nb) return;
-                const uint32_t w = pos >> 5, s = pos & 31u;
-                sm.hdr[w] |= v << s;
-                if (s + nb > 32u) sm.hdr[w + 1] |= v >> (32u - s);
-                pos += nb;
+            unsigned long long acc = 0;
+            uint32_t nb = 0, wpos = 0, pos = 0;
+            auto put = [&](uint32_t v, uint32_t k) {
+                acc |= (unsigned long long)v << nb;
+                nb += k;
+                pos += k;
+                if (nb >= 32u) {
+                    sm.hdr[wpos++] = (uint32_t)acc;
+                    acc >>= 32;
+                    nb -= 32u;
+                }
             };
             put(5u, 3);
             put(sm.nlit - 257u, 5);
@@ -868,137 +955,149 @@ __global__ void __launch_bounds__(kHuffThreads) k_huff(BatchParams bp) {
                 else if (c == 17) put(sm.rle_extra[q], 3);
                 else if (c == 18) put(sm.rle_extra[q], 7);
             }
+            if (nb) sm.hdr[wpos++] = (uint32_t)acc;
             sm.hbits = pos;
         }
         __syncthreads();
 
         // bits per symbol occurrence (code + extra); total member bits
         uint32_t part = 0;
-        if (tid < GPZ_NSYM) {
-            const uint32_t cl = sm.codes[tid] >> 16;
+        for (int q = tid; q < GPZ_NSYM; q += kHuffThreads) {
+            const uint32_t cl = sm.codes[q] >> 16;
             uint32_t extra = 0;
-            if (tid >= 257 && tid < GPZ_NLIT) extra = len_extra_bits((uint32_t)tid - 257u);
-            else if (tid >= GPZ_NLIT) extra = dist_extra_bits((uint32_t)tid - GPZ_NLIT);
-            sm.blen[tid] = cl + extra;
-            part = sm.freq[tid] * (cl + extra);
+            if (q >= 257 && q < GPZ_NLIT) extra = len_extra_bits((uint32_t)q - 257u);
+            else if (q >= GPZ_NLIT) extra = dist_extra_bits((uint32_t)q - GPZ_NLIT);
+            sm.blen[q] = cl + extra;
+            part += sm.freq[q] * (cl + extra);
         }
-#pragma unroll
-        for (int o = 16; o; o >>= 1) part += __shfl_xor_sync(0xFFFFFFFFu, part, o);
+        part = __reduce_add_sync(0xFFFFFFFFu, part);
         if (lane == 0) sm.red[warp] = part;
+        // exact bit plan per tile from the tile histograms
+        __syncthreads();
+        for (uint32_t j = warp; j < md.ntiles; j += NW) {
+            const uint16_t* h = bp.tile_hist + (size_t)(md.tile_base + j) * GPZ_NSYM;
+            uint32_t sbits = 0;
+            for (int q = lane; q < GPZ_NSYM; q += 32) sbits += (uint32_t)h[q] * sm.blen[q];
+            sbits = __reduce_add_sync(0xFFFFFFFFu, sbits);
+            if (lane == 0) sm.tile_bits[j] = sbits;
+        }
         __syncthreads();
         if (tid == 0) {
             uint32_t tot = sm.hbits;
             for (int w = 0; w < NW; w++) tot += sm.red[w];
             sm.total = tot;
-        }
-        __syncthreads();
-        // place the member in the batch output: decoupled look-back over
-        // members on (18 + DEFLATE bytes), 32 predecessors per step
-        if (warp == 0) {
-            const unsigned long long agg = 18ull + ((sm.total + 7u) >> 3);
-            const unsigned long long vmask = (1ull << 62) - 1ull;
-            unsigned long long excl = 0;
-            if (lane == 0) atomicExch(&bp.member_status[m], ((m == 0 ? 2ull : 1ull) << 62) | agg);
-            long long j = (long long)m - 1;
-            uint32_t spins = 0;
-            while (j >= 0) {
-                const long long idx = j - lane;
-                const unsigned long long st = idx >= 0 ? ld_volatile64(&bp.member_status[idx]) : (2ull << 62);
-                const uint32_t f = (uint32_t)(st >> 62);
-                const uint32_t incl = __ballot_sync(0xFFFFFFFFu, f == 2u);
-                const uint32_t zero = __ballot_sync(0xFFFFFFFFu, f == 0u);
-                const int first = incl ? __ffs(incl) - 1 : 32;
-                const uint32_t before = first == 32 ? 0xFFFFFFFFu : ((1u << first) - 1u);
-                if (zero & before) {
-                    if (++spins > kSpinLimit) {
-                        if (lane == 0) atomicOr(bp.err, GPZ_ERRBIT_SPIN);
-                        break;
-                    }
-                    __nanosleep(64);
-                    continue;
-                }
-                unsigned long long v = (lane <= first) ? (st & vmask) : 0ull;
-#pragma unroll
-                for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
-                excl += v;
-                if (first < 32) break;
-                j -= 32;
-            }
-            if (lane == 0) {
-                if (m > 0) atomicExch(&bp.member_status[m], (2ull << 62) | (excl + agg));
-                sm.gz_off = bp.out_base + excl;
-            }
-        }
-        __syncthreads();
-
-        // exact bit plan per tile from the tile histograms
-        for (uint32_t j = warp; j < md.ntiles; j += NW) {
-            const uint16_t* h = bp.tile_hist + (size_t)(md.tile_base + j) * GPZ_NSYM;
-            uint32_t s = 0;
-            for (int q = lane; q < GPZ_NSYM; q += 32) s += (uint32_t)h[q] * sm.blen[q];
-#pragma unroll
-            for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xFFFFFFFFu, s, o);
-            if (lane == 0) sm.tile_bits[j] = s;
-        }
-        __syncthreads();
-        const uint32_t eob_len = sm.codes[256] >> 16;
-        const unsigned long long base = (sm.gz_off + 10ull) * 8ull;
-        uint32_t* outw = bp.out_words;
-        if (tid == 0) {
             uint32_t off = sm.hbits;
             for (uint32_t j = 0; j < md.ntiles; j++) {
                 bp.tile_bitoff[md.tile_base + j] = off;
                 off += sm.tile_bits[j];
             }
-            if (off + eob_len != sm.total) atomicOr(bp.err, GPZ_ERRBIT_BITS);
+            if (off + (sm.codes[256] >> 16) != tot) atomicOr(bp.err, GPZ_ERRBIT_BITS);
             if (!sm.ok) atomicOr(bp.err, GPZ_ERRBIT_HUFF);
-        }
-        __syncthreads();
-        // zero every word a tile boundary, the EOB or the last bit falls in
-        for (uint32_t j = tid; j < md.ntiles; j += kHuffThreads)
-            outw[(base + bp.tile_bitoff[md.tile_base + j]) >> 5] = 0u;
-        if (tid == 0) {
-            outw[(base + sm.total - eob_len) >> 5] = 0u;
-            outw[(base + sm.total - 1u) >> 5] = 0u;
-        }
-        __syncthreads();
-        // header words: whole words are stored, the word shared with the
-        // first token is OR-ed into its zeroed copy
-        {
-            const unsigned long long w0 = base >> 5, w1 = (base + sm.hbits - 1u) >> 5;
-            const unsigned long long shared = (base + sm.hbits) >> 5;
-            for (unsigned long long w = w0 + tid; w <= w1; w += kHuffThreads) {
-                const long long L = (long long)(w * 32ull) - (long long)base;  // header bit at word bit 0
-                uint32_t v;
-                if (L < 0) {
-                    v = sm.hdr[0] << (uint32_t)(-L);
-                } else {
-                    const uint32_t q = (uint32_t)L >> 5, s = (uint32_t)L & 31u;
-                    v = __funnelshift_r(sm.hdr[q], sm.hdr[q + 1], s);
-                }
-                const long long keep = (long long)sm.hbits - L;  // header bits in this word above L
-                if (keep < 32) v &= keep <= 0 ? 0u : ((1u << keep) - 1u);
-                if (w == shared) atomicOr(&outw[w], v);
-                else outw[w] = v;
-            }
-        }
-        if (tid == 0) {
-            const uint32_t eob = sm.codes[256] & 0xFFFFu;
-            const unsigned long long e0 = base + sm.total - eob_len;
-            const uint32_t s = (uint32_t)(e0 & 31u);
-            atomicOr(&outw[e0 >> 5], eob << s);
-            if (s + eob_len > 32u) atomicOr(&outw[(e0 >> 5) + 1], eob >> (32u - s));
             MemberOut mo;
-            mo.gz_off = sm.gz_off;
-            mo.deflate_bytes = (sm.total + 7u) >> 3;
+            mo.gz_off = 0;
+            mo.deflate_bytes = (tot + 7u) >> 3;
             mo.crc = sm.crc;
-            mo.total_bits = sm.total;
+            mo.total_bits = tot;
             mo.header_bits = sm.hbits;
             mo.len = md.len;
             mo.pad = 0;
             bp.member_out[m] = mo;
         }
-        for (int s = tid; s < GPZ_NSYM; s += kHuffThreads) bp.member_codes[(size_t)m * GPZ_NSYM + s] = sm.codes[s];
+        for (int q = tid; q < GPZ_NSYM; q += kHuffThreads) bp.member_codes[(size_t)m * GPZ_NSYM + q] = sm.codes[q];
+        for (int q = tid; q < GPZ_HDR_WORDS; q += kHuffThreads) bp.member_hdr[(size_t)m * GPZ_HDR_WORDS + q] = sm.hdr[q];
+    }
+}
+
+// ================================================================= k_place
+
+// Byte offset of every gzip member in the batch output: exclusive scan of
+// (18 + DEFLATE bytes) in member order, one CTA.
+constexpr int kPlaceThreads = 1024;
+
+__global__ void __launch_bounds__(kPlaceThreads) k_place(BatchParams bp) {
+    __shared__ unsigned long long wsum[32];
+    __shared__ unsigned long long carry;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) carry = bp.out_base;
+    __syncthreads();
+    for (uint32_t base = 0; base < bp.nmembers; base += kPlaceThreads) {
+        const uint32_t m = base + tid;
+        const unsigned long long v = m < bp.nmembers ? 18ull + bp.member_out[m].deflate_bytes : 0ull;
+        unsigned long long x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) wsum[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            unsigned long long s = wsum[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned long long y = __shfl_up_sync(0xFFFFFFFFu, s, o);
+                if (lane >= o) s += y;
+            }
+            wsum[lane] = s;
+        }
+        __syncthreads();
+        const unsigned long long excl = carry + (warp ? wsum[warp - 1] : 0ull) + x - v;
+        if (m < bp.nmembers) bp.member_out[m].gz_off = excl;
+        __syncthreads();
+        if (tid == 0) carry += wsum[31];
+        __syncthreads();
+    }
+}
+
+// ================================================================= k_frame
+
+// Per member: zero every output word that several writers share (a word a
+// tile boundary, the EOB or the last bit falls in), then store the header
+// words and OR in the EOB code.  k_emit then stores whole words and ORs the
+// shared ones.
+constexpr int kFrameThreads = 128;
+
+__global__ void __launch_bounds__(kFrameThreads) k_frame(BatchParams bp) {
+    const int tid = threadIdx.x;
+    for (uint32_t m = blockIdx.x; m < bp.nmembers; m += gridDim.x) {
+        const MemberDesc md = bp.members[m];
+        const MemberOut mo = bp.member_out[m];
+        const uint32_t eob = bp.member_codes[(size_t)m * GPZ_NSYM + 256];
+        const uint32_t eob_len = eob >> 16;
+        const unsigned long long base = (mo.gz_off + 10ull) * 8ull;
+        uint32_t* outw = bp.out_words;
+        for (uint32_t j = tid; j < md.ntiles; j += kFrameThreads)
+            outw[(base + bp.tile_bitoff[md.tile_base + j]) >> 5] = 0u;
+        if (tid == 0) {
+            outw[(base + mo.total_bits - eob_len) >> 5] = 0u;
+            outw[(base + mo.total_bits - 1u) >> 5] = 0u;
+        }
+        __syncthreads();
+        const uint32_t* hdr = bp.member_hdr + (size_t)m * GPZ_HDR_WORDS;
+        const unsigned long long w0 = base >> 5, w1 = (base + mo.header_bits - 1u) >> 5;
+        const unsigned long long shared = (base + mo.header_bits) >> 5;
+        for (unsigned long long w = w0 + tid; w <= w1; w += kFrameThreads) {
+            const long long L = (long long)(w * 32ull) - (long long)base;  // header bit at word bit 0
+            uint32_t v;
+            if (L < 0) {
+                v = hdr[0] << (uint32_t)(-L);
+            } else {
+                const uint32_t q = (uint32_t)L >> 5, s = (uint32_t)L & 31u;
+                v = __funnelshift_r(hdr[q], hdr[q + 1], s);
+            }
+            const long long keep = (long long)mo.header_bits - L;
+            if (keep < 32) v &= keep <= 0 ? 0u : ((1u << keep) - 1u);
+            if (w == shared) atomicOr(&outw[w], v);
+            else outw[w] = v;
+        }
+        if (tid == 0) {
+            const uint32_t code = eob & 0xFFFFu;
+            const unsigned long long e0 = base + mo.total_bits - eob_len;
+            const uint32_t s = (uint32_t)(e0 & 31u);
+            atomicOr(&outw[e0 >> 5], code << s);
+            if (s + eob_len > 32u) atomicOr(&outw[(e0 >> 5) + 1], code >> (32u - s));
+        }
+        __syncthreads();
     }
 }
 
@@ -1125,8 +1224,10 @@ int gpz_kernel_smem_setup() {
     tab[0] = x8;
     for (int k = 1; k < 32; k++) tab[k] = mul(tab[k - 1], tab[k - 1]);
     if (cudaMemcpyToSymbol(c_x8pow2, tab, sizeof tab) != cudaSuccess) return -1;
+    if (cudaFuncSetAttribute(k_segtab<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSegtabSmem) !=
+        cudaSuccess)
+        return -1;
     const int smem = (int)LookupSmem::kBytes;
-    if (cudaFuncSetAttribute(k_lookup<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) return -1;
     if (cudaFuncSetAttribute(k_lookup<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) return -1;
     if (cudaFuncSetAttribute(k_lookup<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
         return -1;
@@ -1135,6 +1236,7 @@ int gpz_kernel_smem_setup() {
 
 template <int T>
 static void launch_lookup(const BatchParams& bp, int grid, cudaStream_t s) {
+    k_segtab<512><<<grid, 512, kSegtabSmem, s>>>(bp);
     k_lookup<T><<<grid, T, LookupSmem::kBytes, s>>>(bp);
 }
 
@@ -1144,21 +1246,31 @@ int gpz_launch_batch(const BatchParams& bp, const LaunchShape& ls, void* stream,
         if (events) cudaEventRecord(static_cast<cudaEvent_t>(events[i]), s);
     };
     auto grid_of = [&](int g, uint32_t items) { return g > 0 ? g : (int)(items ? items : 1u); };
+    const int nm = bp.nmembers ? (int)bp.nmembers : 1;
     mark(0);
     const int gl = grid_of(ls.lookup_grid, bp.ntiles);
     switch (ls.lookup_threads) {
-        case 256: launch_lookup<256>(bp, gl, s); break;
-        case 1024: launch_lookup<1024>(bp, gl, s); break;
-        default: launch_lookup<512>(bp, gl, s); break;
+        case 512: launch_lookup<512>(bp, gl, s); break;
+        default: launch_lookup<1024>(bp, gl, s); break;
     }
     mark(1);
     const int gw = grid_of(ls.walk_grid, bp.ntiles);
     switch (ls.walk_threads) {
-        case 256: k_walk<256><<<gw, 256, 0, s>>>(bp); break;
-        default: k_walk<512><<<gw, 512, 0, s>>>(bp); break;
+        case 256:
+            k_walk_exit<256><<<gw, 256, 0, s>>>(bp);
+            k_chain<<<(nm + 127) / 128, 128, 0, s>>>(bp);
+            k_walk_mark<256><<<gw, 256, 0, s>>>(bp);
+            break;
+        default:
+            k_walk_exit<512><<<gw, 512, 0, s>>>(bp);
+            k_chain<<<(nm + 127) / 128, 128, 0, s>>>(bp);
+            k_walk_mark<512><<<gw, 512, 0, s>>>(bp);
+            break;
     }
     mark(2);
-    k_huff<<<bp.nmembers ? (int)bp.nmembers : 1, kHuffThreads, 0, s>>>(bp);
+    k_huff<<<nm, kHuffThreads, 0, s>>>(bp);
+    k_place<<<1, kPlaceThreads, 0, s>>>(bp);
+    k_frame<<<nm, kFrameThreads, 0, s>>>(bp);
     mark(3);
     const int ge = grid_of(ls.emit_grid, bp.ntiles);
     switch (ls.emit_threads) {

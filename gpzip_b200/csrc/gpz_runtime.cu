@@ -55,11 +55,11 @@ struct gpz_ctx {
     std::mutex mu;  // one device pass at a time per context
     std::string last_err;
     uint64_t launches = 0;
-    LaunchShape shape{512, 0, 512, 0, 512, 0};
+    LaunchShape shape{1024, 0, 512, 0, 512, 0};
 
     // device pool (one batch in flight)
-    DevArena d_in, d_pp, d_tok, d_out, d_tstat, d_texit, d_thist, d_tntok, d_tcrc, d_tbit, d_mcodes, d_mout,
-        d_mstat, d_cnt, d_members, d_tiles;
+    DevArena d_in, d_pp, d_tok, d_out, d_skeys, d_son, d_sposid, d_snkeys, d_tentry, d_texit, d_thist, d_tntok, d_tbit, d_mcodes, d_mhdr, d_mout,
+        d_cnt, d_members, d_tiles;
     size_t pool_used = 0;
     // pinned staging
     uint8_t* h_in = nullptr;
@@ -176,15 +176,18 @@ int reserve(gpz_ctx* c, size_t in_bytes, bool own_in, bool own_out, size_t out_b
     if ((rc = ensure_dev(c, c->d_pp, in_bytes * 4 + 64))) return rc;
     if ((rc = ensure_dev(c, c->d_tok, in_bytes * 4 + 64))) return rc;
     if (own_out && (rc = ensure_dev(c, c->d_out, out_bytes + 64))) return rc;
-    if ((rc = ensure_dev(c, c->d_tstat, nt * 4))) return rc;
+    if ((rc = ensure_dev(c, c->d_skeys, nt * GPZ_SEG * 2))) return rc;
+    if ((rc = ensure_dev(c, c->d_son, nt * GPZ_SEG * 4))) return rc;
+    if ((rc = ensure_dev(c, c->d_sposid, nt * GPZ_SEG * 2))) return rc;
+    if ((rc = ensure_dev(c, c->d_snkeys, nt * 4))) return rc;
+    if ((rc = ensure_dev(c, c->d_tentry, nt * 4))) return rc;
     if ((rc = ensure_dev(c, c->d_texit, nt * GPZ_EXITS * 2))) return rc;
     if ((rc = ensure_dev(c, c->d_thist, nt * GPZ_NSYM * 2))) return rc;
     if ((rc = ensure_dev(c, c->d_tntok, nt * 4))) return rc;
-    if ((rc = ensure_dev(c, c->d_tcrc, nt * 4))) return rc;
     if ((rc = ensure_dev(c, c->d_tbit, nt * 4))) return rc;
     if ((rc = ensure_dev(c, c->d_mcodes, nm * GPZ_NSYM * 4))) return rc;
     if ((rc = ensure_dev(c, c->d_mout, nm * sizeof(MemberOut)))) return rc;
-    if ((rc = ensure_dev(c, c->d_mstat, nm * 8))) return rc;
+    if ((rc = ensure_dev(c, c->d_mhdr, nm * GPZ_HDR_WORDS * 4))) return rc;
     if ((rc = ensure_dev(c, c->d_cnt, GPZ_NCOUNTERS * 4 + 64))) return rc;
     if ((rc = ensure_dev(c, c->d_members, nm * sizeof(MemberDesc)))) return rc;
     if ((rc = ensure_dev(c, c->d_tiles, nt * sizeof(TileDesc)))) return rc;
@@ -209,8 +212,6 @@ int run_device(gpz_ctx* c, const uint8_t* d_in, uint8_t* d_out, cudaStream_t s) 
     CU(c, cudaMemcpyAsync(c->d_members.p, c->h_members, nm * sizeof(MemberDesc), cudaMemcpyHostToDevice, s));
     if (nt) CU(c, cudaMemcpyAsync(c->d_tiles.p, c->h_tiles, nt * sizeof(TileDesc), cudaMemcpyHostToDevice, s));
     CU(c, cudaMemsetAsync(c->d_cnt.p, 0, GPZ_NCOUNTERS * 4 + 64, s));
-    if (nt) CU(c, cudaMemsetAsync(c->d_tstat.p, 0, nt * 4, s));
-    CU(c, cudaMemsetAsync(c->d_mstat.p, 0, nm * 8, s));
 
     BatchParams bp{};
     bp.in = d_in;
@@ -219,15 +220,18 @@ int run_device(gpz_ctx* c, const uint8_t* d_in, uint8_t* d_out, cudaStream_t s) 
     bp.pp = static_cast<uint32_t*>(c->d_pp.p);
     bp.tok = static_cast<uint32_t*>(c->d_tok.p);
     bp.out_words = reinterpret_cast<uint32_t*>(d_out);
-    bp.tile_status = static_cast<uint32_t*>(c->d_tstat.p);
+    bp.seg_keys = static_cast<uint16_t*>(c->d_skeys.p);
+    bp.seg_on = static_cast<uint32_t*>(c->d_son.p);
+    bp.seg_posid = static_cast<uint16_t*>(c->d_sposid.p);
+    bp.seg_nkeys = static_cast<uint32_t*>(c->d_snkeys.p);
+    bp.tile_entry = static_cast<uint32_t*>(c->d_tentry.p);
     bp.tile_exit = static_cast<uint16_t*>(c->d_texit.p);
     bp.tile_hist = static_cast<uint16_t*>(c->d_thist.p);
     bp.tile_ntok = static_cast<uint32_t*>(c->d_tntok.p);
-    bp.tile_crc = static_cast<uint32_t*>(c->d_tcrc.p);
     bp.tile_bitoff = static_cast<uint32_t*>(c->d_tbit.p);
     bp.member_codes = static_cast<uint32_t*>(c->d_mcodes.p);
     bp.member_out = static_cast<MemberOut*>(c->d_mout.p);
-    bp.member_status = static_cast<unsigned long long*>(c->d_mstat.p);
+    bp.member_hdr = static_cast<uint32_t*>(c->d_mhdr.p);
     bp.counters = static_cast<uint32_t*>(c->d_cnt.p);
     bp.err = bp.counters + GPZ_NCOUNTERS;
     bp.nmembers = (uint32_t)nm;
@@ -236,7 +240,7 @@ int run_device(gpz_ctx* c, const uint8_t* d_in, uint8_t* d_out, cudaStream_t s) 
     const bool timing = (c->flags & GPZ_FLAG_STAGE_TIMING) && c->ev[0];
     if (gpz_launch_batch(bp, c->shape, s, timing ? reinterpret_cast<void* const*>(c->ev) : nullptr) != 0)
         return fail(c, GPZ_E_CUDA, "kernel launch", cudaGetLastError());
-    c->launches = 4;
+    c->launches = 9;
     CU(c, cudaMemcpyAsync(c->h_mout, c->d_mout.p, nm * sizeof(MemberOut), cudaMemcpyDeviceToHost, s));
     CU(c, cudaMemcpyAsync(c->h_err, bp.err, 4, cudaMemcpyDeviceToHost, s));
     CU(c, cudaStreamSynchronize(s));
@@ -414,8 +418,9 @@ void gpz_destroy(gpz_ctx* c) {
     if (!c) return;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    for (DevArena* a : {&c->d_in, &c->d_pp, &c->d_tok, &c->d_out, &c->d_tstat, &c->d_texit, &c->d_thist, &c->d_tntok,
-                        &c->d_tcrc, &c->d_tbit, &c->d_mcodes, &c->d_mout, &c->d_mstat, &c->d_cnt, &c->d_members,
+    for (DevArena* a : {&c->d_in, &c->d_pp, &c->d_tok, &c->d_out, &c->d_skeys, &c->d_son, &c->d_sposid,
+                        &c->d_snkeys, &c->d_tentry, &c->d_texit, &c->d_thist,
+                        &c->d_tntok, &c->d_tbit, &c->d_mcodes, &c->d_mhdr, &c->d_mout, &c->d_cnt, &c->d_members,
                         &c->d_tiles})
         if (a->p) cudaFree(a->p);
     if (c->h_in) cudaFreeHost(c->h_in);
@@ -552,8 +557,8 @@ int gpz_get_shape(gpz_ctx* c, gpz_shape* s) {
 
 int gpz_set_shape(gpz_ctx* c, const gpz_shape* s) {
     if (!c || !s) return GPZ_E_ARG;
-    auto ok_t = [](int t, bool allow1024) { return t == 256 || t == 512 || (allow1024 && t == 1024); };
-    if (!ok_t(s->lookup_threads, true) || !ok_t(s->walk_threads, false) || !ok_t(s->emit_threads, false) ||
+    auto ok_t = [](int t) { return t == 256 || t == 512; };
+    if (!(s->lookup_threads == 512 || s->lookup_threads == 1024) || !ok_t(s->walk_threads) || !ok_t(s->emit_threads) ||
         s->lookup_grid < 0 || s->walk_grid < 0 || s->emit_grid < 0)
         return GPZ_E_ARG;
     std::lock_guard<std::mutex> lk(c->mu);

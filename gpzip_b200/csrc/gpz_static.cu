@@ -39,16 +39,19 @@ constexpr size_t kIn = 0;
 constexpr size_t kPp = kIn + al(kMax + 64);
 constexpr size_t kTok = kPp + al(kMax * 4 + 64);
 constexpr size_t kOut = kTok + al(kMax * 4 + 64);
-constexpr size_t kTstat = kOut + al(kOutCap + 64);
-constexpr size_t kTexit = kTstat + al(kTiles * 4);
+constexpr size_t kSkeys = kOut + al(kOutCap + 64);
+constexpr size_t kSon = kSkeys + al(kTiles * GPZ_SEG * 2);
+constexpr size_t kSposid = kSon + al(kTiles * GPZ_SEG * 4);
+constexpr size_t kSnkeys = kSposid + al(kTiles * GPZ_SEG * 2);
+constexpr size_t kTentry = kSnkeys + al(kTiles * 4);
+constexpr size_t kTexit = kTentry + al(kTiles * 4);
 constexpr size_t kThist = kTexit + al(kTiles * GPZ_EXITS * 2);
 constexpr size_t kTntok = kThist + al(kTiles * GPZ_NSYM * 2);
-constexpr size_t kTcrc = kTntok + al(kTiles * 4);
-constexpr size_t kTbit = kTcrc + al(kTiles * 4);
+constexpr size_t kTbit = kTntok + al(kTiles * 4);
 constexpr size_t kMcodes = kTbit + al(kTiles * 4);
-constexpr size_t kMout = kMcodes + al(GPZ_NSYM * 4);
-constexpr size_t kMstat = kMout + al(sizeof(MemberOut));
-constexpr size_t kCnt = kMstat + al(8);
+constexpr size_t kMhdr = kMcodes + al(GPZ_NSYM * 4);
+constexpr size_t kMout = kMhdr + al(GPZ_HDR_WORDS * 4);
+constexpr size_t kCnt = kMout + al(sizeof(MemberOut));
 constexpr size_t kMembers = kCnt + al(GPZ_NCOUNTERS * 4 + 64);
 constexpr size_t kTilesOff = kMembers + al(sizeof(MemberDesc));
 constexpr size_t kResult = kTilesOff + al(kTiles * sizeof(TileDesc));
@@ -67,18 +70,12 @@ namespace {
 // descriptors for one member of n bytes.
 __global__ void k_static_setup(uint8_t* base, uint32_t n) {
     uint32_t* cnt = reinterpret_cast<uint32_t*>(base + kCnt);
-    uint32_t* tstat = reinterpret_cast<uint32_t*>(base + kTstat);
-    unsigned long long* mstat = reinterpret_cast<unsigned long long*>(base + kMstat);
     MemberDesc* md = reinterpret_cast<MemberDesc*>(base + kMembers);
     TileDesc* td = reinterpret_cast<TileDesc*>(base + kTilesOff);
     const uint32_t nt = (n + GPZ_SEG - 1) / GPZ_SEG;
     for (uint32_t i = threadIdx.x; i < GPZ_NCOUNTERS + 16; i += blockDim.x) cnt[i] = 0u;
-    for (uint32_t i = threadIdx.x; i < kTiles; i += blockDim.x) {
-        tstat[i] = 0u;
-        td[i] = TileDesc{0u, i};
-    }
+    for (uint32_t i = threadIdx.x; i < kTiles; i += blockDim.x) td[i] = TileDesc{0u, i};
     if (threadIdx.x == 0) {
-        mstat[0] = 0ull;
         MemberDesc d{};
         d.in_off = 0;
         d.len = n;
@@ -167,21 +164,24 @@ extern "C" int gpz_compress_member_static(const uint8_t* d_in, size_t n, uint8_t
     bp.pp = reinterpret_cast<uint32_t*>(base + kPp);
     bp.tok = reinterpret_cast<uint32_t*>(base + kTok);
     bp.out_words = reinterpret_cast<uint32_t*>(base + kOut);
-    bp.tile_status = reinterpret_cast<uint32_t*>(base + kTstat);
+    bp.seg_keys = reinterpret_cast<uint16_t*>(base + kSkeys);
+    bp.seg_on = reinterpret_cast<uint32_t*>(base + kSon);
+    bp.seg_posid = reinterpret_cast<uint16_t*>(base + kSposid);
+    bp.seg_nkeys = reinterpret_cast<uint32_t*>(base + kSnkeys);
+    bp.tile_entry = reinterpret_cast<uint32_t*>(base + kTentry);
     bp.tile_exit = reinterpret_cast<uint16_t*>(base + kTexit);
     bp.tile_hist = reinterpret_cast<uint16_t*>(base + kThist);
     bp.tile_ntok = reinterpret_cast<uint32_t*>(base + kTntok);
-    bp.tile_crc = reinterpret_cast<uint32_t*>(base + kTcrc);
     bp.tile_bitoff = reinterpret_cast<uint32_t*>(base + kTbit);
     bp.member_codes = reinterpret_cast<uint32_t*>(base + kMcodes);
     bp.member_out = reinterpret_cast<MemberOut*>(base + kMout);
-    bp.member_status = reinterpret_cast<unsigned long long*>(base + kMstat);
+    bp.member_hdr = reinterpret_cast<uint32_t*>(base + kMhdr);
     bp.counters = reinterpret_cast<uint32_t*>(base + kCnt);
     bp.err = bp.counters + GPZ_NCOUNTERS;
     bp.nmembers = 1;
     bp.ntiles = (uint32_t)((n + GPZ_SEG - 1) / GPZ_SEG);
     bp.out_base = 0;
-    const LaunchShape shape{512, 0, 512, 0, 512, 0};
+    const LaunchShape shape{1024, 0, 512, 0, 512, 0};
     if (gpz_launch_batch(bp, shape, s, nullptr) != 0) return GPZ_E_CUDA;
     k_static_finish<<<8, 256, 0, s>>>(base, d_out, out_cap);
 

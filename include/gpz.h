@@ -170,7 +170,7 @@ GPZ_API uint64_t gpz_last_launches(gpz_ctx* ctx);
  * reference: it exists for callers that cannot allocate GPU memory when they
  * compress (their device memory is fully reserved by another allocator, or
  * the path must not take cudaMalloc / cudaFree, which can synchronise the
- * device).  All working memory is one fixed device array of about 1.5 MB
+ * device).  All working memory is one fixed device array of about 2.5 MB
  * inside this library, held by every GPU that loads it until process exit.
  * d_in (n <= GPZ_STATIC_MAX_BYTES bytes, any alignment) and d_out (out_cap
  * bytes; gpz_bound(n) always suffices) are device memory on the calling
