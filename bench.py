@@ -278,10 +278,12 @@ def main():
     max_ms = float(t.item())
     value = data.size * args.steps * world / (max_ms / 1e3) / 1e9
 
-    # end to end through the public host API (host buffers, copies inside)
+    # end to end through the public host API (host buffers, copies inside),
+    # on a context with the production settings (graphs, autotuned shapes)
+    ectx = native.Context(device=local, member_bytes=MEMBER)
     host_chunks = [np.ascontiguousarray(data[o:o + n]) for o, n in spans]
-    for _ in range(0 if args.device_only else min(args.warmup, 2)):
-        ctx.compress_batch(host_chunks)
+    for _ in range(0 if args.device_only else max(args.warmup, 2)):
+        ectx.compress_batch(host_chunks)
     barrier()
     e_times = []
     e2e_out = 0
@@ -289,7 +291,7 @@ def main():
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        outs = ctx.compress_batch(host_chunks)
+        outs = ectx.compress_batch(host_chunks)
         e1.record(stream)
         e1.synchronize()
         e_times.append(e0.elapsed_time(e1))
@@ -346,6 +348,7 @@ def main():
         }
         print(json.dumps(line), flush=True)
     ctx.close()
+    ectx.close()
     if world > 1:
         dist.destroy_process_group()
 

@@ -69,9 +69,10 @@ struct BatchParams {
     uint32_t* member_codes;   // [member][GPZ_NSYM] reversed code | len << 16
     uint32_t* member_hdr;     // [member][GPZ_HDR_WORDS] dynamic block header bits
     MemberOut* member_out;
-    uint32_t* counters;       // [0..3] tile claims per stage, [4] member claims
+    uint32_t* counters;       // work-claim counters per stage (zeroed per batch)
     uint32_t* err;
-    uint32_t nmembers;
+    const uint32_t* dims;     // device: [0] tiles, [1] members of this batch
+    uint32_t nmembers;        // host-side copies, used only to size exact grids
     uint32_t ntiles;
     uint64_t out_base;        // byte offset added to every member's gz_off
 };
@@ -86,18 +87,34 @@ enum {
     GPZ_NCOUNTERS = 8
 };
 
-// Per-stage launch geometry chosen by the autotuner (threads per CTA, CTAs).
+// Per-stage launch geometry chosen by the autotuner: threads per CTA, and
+// CTAs per grid (0 = one CTA per item of the batch; > 0 = a persistent grid
+// that claims items from the device counters).
 struct LaunchShape {
     int lookup_threads;
-    int lookup_grid;   // 0 = one CTA per tile
+    int lookup_grid;
     int walk_threads;
     int walk_grid;
     int emit_threads;
     int emit_grid;
+    int segtab_grid;
+    int huff_grid;
+};
+
+// Host-mapped pinned destinations of k_drain.
+struct DrainTarget {
+    uint8_t* h_out;
+    MemberOut* h_mout;
+    uint32_t* h_err;
+    int grid;
 };
 
 // Kernel launchers (gpz_kernels.cu).
 // events: NULL or 5 cudaEvent_t recorded before each stage and after the last.
-int gpz_launch_batch(const BatchParams& bp, const LaunchShape& ls, void* stream, void* const* events);
+// drain: NULL, or where k_drain streams the output, member table and error.
+int gpz_launch_batch(const BatchParams& bp, const LaunchShape& ls, void* stream, void* const* events,
+                     const DrainTarget* drain);
+// Persistent grid sizes (SMs x resident CTAs) for the shape's thread counts.
+int gpz_occupancy(LaunchShape* persistent);
 int gpz_kernel_smem_setup();
 size_t gpz_lookup_smem_bytes();

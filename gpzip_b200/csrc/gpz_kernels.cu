@@ -180,12 +180,13 @@ __global__ void __launch_bounds__(T, 2) k_segtab(BatchParams bp) {
     __shared__ uint32_t wsum[32];
     __shared__ uint32_t s_tile;
     const int tid = threadIdx.x, lane = tid & 31;
+    const uint32_t ntiles = bp.dims[0];
     for (;;) {
         __syncthreads();
         if (tid == 0) s_tile = atomicAdd(&bp.counters[GPZ_CNT_SEGSORT], 1u);
         __syncthreads();
         const uint32_t t = s_tile;
-        if (t >= bp.ntiles) break;
+        if (t >= ntiles) break;
         const TileDesc td = bp.tiles[t];
         const MemberDesc md = bp.members[td.member];
         const uint32_t n = md.len, start = td.seg << GPZ_SEG_LOG2;
@@ -284,12 +285,13 @@ __global__ void __launch_bounds__(T, 1) k_lookup(BatchParams bp) {
     __shared__ uint32_t s_tile;
     const int tid = threadIdx.x;
 
+    const uint32_t ntiles = bp.dims[0];
     for (;;) {
         __syncthreads();
         if (tid == 0) s_tile = atomicAdd(&bp.counters[GPZ_CNT_LOOKUP], 1u);
         __syncthreads();
         const uint32_t t = s_tile;
-        if (t >= bp.ntiles) break;
+        if (t >= ntiles) break;
         const TileDesc td = bp.tiles[t];
         const MemberDesc md = bp.members[td.member];
         const uint32_t n = md.len, S = td.seg, start = S << GPZ_SEG_LOG2;
@@ -431,12 +433,13 @@ __global__ void __launch_bounds__(T) k_walk_exit(BatchParams bp) {
     __shared__ WalkLinks w;
     __shared__ uint32_t s_tile;
     const int tid = threadIdx.x;
+    const uint32_t ntiles = bp.dims[0];
     for (;;) {
         __syncthreads();
         if (tid == 0) s_tile = atomicAdd(&bp.counters[GPZ_CNT_EXIT], 1u);
         __syncthreads();
         const uint32_t t = s_tile;
-        if (t >= bp.ntiles) break;
+        if (t >= ntiles) break;
         const TileDesc td = bp.tiles[t];
         const MemberDesc md = bp.members[td.member];
         if (td.seg + 1u == md.ntiles) continue;  // the member's last tile has no successor
@@ -461,14 +464,15 @@ __global__ void __launch_bounds__(T) k_walk_exit(BatchParams bp) {
 
 // Entry offset of every tile: one thread per member follows the exit tables.
 __global__ void k_chain(BatchParams bp) {
-    const uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
-    if (m >= bp.nmembers) return;
-    const MemberDesc md = bp.members[m];
-    uint32_t e = 0;
-    for (uint32_t b = 0; b < md.ntiles; b++) {
-        const uint32_t t = md.tile_base + b;
-        bp.tile_entry[t] = e;
-        if (b + 1u < md.ntiles) e = bp.tile_exit[(size_t)t * GPZ_EXITS + min(e, (uint32_t)GPZ_EXITS - 1u)];
+    const uint32_t nmembers = bp.dims[1];
+    for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < nmembers; m += gridDim.x * blockDim.x) {
+        const MemberDesc md = bp.members[m];
+        uint32_t e = 0;
+        for (uint32_t b = 0; b < md.ntiles; b++) {
+            const uint32_t t = md.tile_base + b;
+            bp.tile_entry[t] = e;
+            if (b + 1u < md.ntiles) e = bp.tile_exit[(size_t)t * GPZ_EXITS + min(e, (uint32_t)GPZ_EXITS - 1u)];
+        }
     }
 }
 
@@ -485,12 +489,13 @@ __global__ void __launch_bounds__(T) k_walk_mark(BatchParams bp) {
     constexpr int PER = GPZ_SEG / T;
     __shared__ MarkSmem sm;
     const int tid = threadIdx.x;
+    const uint32_t ntiles = bp.dims[0];
     for (;;) {
         __syncthreads();
         if (tid == 0) sm.tile = atomicAdd(&bp.counters[GPZ_CNT_MARK], 1u);
         __syncthreads();
         const uint32_t t = sm.tile;
-        if (t >= bp.ntiles) break;
+        if (t >= ntiles) break;
         const TileDesc td = bp.tiles[t];
         const MemberDesc md = bp.members[td.member];
         const uint32_t n = md.len, start = td.seg << GPZ_SEG_LOG2;
@@ -757,12 +762,13 @@ __global__ void __launch_bounds__(kHuffThreads) k_huff(BatchParams bp) {
         }
     }
 
+    const uint32_t nmembers = bp.dims[1];
     for (;;) {
         __syncthreads();
         if (tid == 0) sm.member = atomicAdd(&bp.counters[GPZ_CNT_HUFF], 1u);
         __syncthreads();
         const uint32_t m = sm.member;
-        if (m >= bp.nmembers) break;
+        if (m >= nmembers) break;
         const MemberDesc md = bp.members[m];
 
         // member symbol counts = sum of its tiles' histograms, + EOB
@@ -1018,11 +1024,12 @@ __global__ void __launch_bounds__(kPlaceThreads) k_place(BatchParams bp) {
     __shared__ unsigned long long wsum[32];
     __shared__ unsigned long long carry;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t nmembers = bp.dims[1];
     if (tid == 0) carry = bp.out_base;
     __syncthreads();
-    for (uint32_t base = 0; base < bp.nmembers; base += kPlaceThreads) {
+    for (uint32_t base = 0; base < nmembers; base += kPlaceThreads) {
         const uint32_t m = base + tid;
-        const unsigned long long v = m < bp.nmembers ? 18ull + bp.member_out[m].deflate_bytes : 0ull;
+        const unsigned long long v = m < nmembers ? 18ull + bp.member_out[m].deflate_bytes : 0ull;
         unsigned long long x = v;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -1042,7 +1049,7 @@ __global__ void __launch_bounds__(kPlaceThreads) k_place(BatchParams bp) {
         }
         __syncthreads();
         const unsigned long long excl = carry + (warp ? wsum[warp - 1] : 0ull) + x - v;
-        if (m < bp.nmembers) bp.member_out[m].gz_off = excl;
+        if (m < nmembers) bp.member_out[m].gz_off = excl;
         __syncthreads();
         if (tid == 0) carry += wsum[31];
         __syncthreads();
@@ -1059,7 +1066,8 @@ constexpr int kFrameThreads = 128;
 
 __global__ void __launch_bounds__(kFrameThreads) k_frame(BatchParams bp) {
     const int tid = threadIdx.x;
-    for (uint32_t m = blockIdx.x; m < bp.nmembers; m += gridDim.x) {
+    const uint32_t nmembers = bp.dims[1];
+    for (uint32_t m = blockIdx.x; m < nmembers; m += gridDim.x) {
         const MemberDesc md = bp.members[m];
         const MemberOut mo = bp.member_out[m];
         const uint32_t eob = bp.member_codes[(size_t)m * GPZ_NSYM + 256];
@@ -1116,12 +1124,13 @@ __global__ void __launch_bounds__(T) k_emit(BatchParams bp) {
     __shared__ EmitSmem sm;
     const int tid = threadIdx.x;
 
+    const uint32_t ntiles = bp.dims[0];
     for (;;) {
         __syncthreads();
         if (tid == 0) sm.tile = atomicAdd(&bp.counters[GPZ_CNT_EMIT], 1u);
         __syncthreads();
         const uint32_t t = sm.tile;
-        if (t >= bp.ntiles) break;
+        if (t >= ntiles) break;
         const TileDesc td = bp.tiles[t];
         const MemberDesc md = bp.members[td.member];
         const MemberOut mo = bp.member_out[td.member];
@@ -1198,6 +1207,27 @@ __global__ void __launch_bounds__(T) k_emit(BatchParams bp) {
     }
 }
 
+// ================================================================= k_drain
+
+// Streams the packed batch output, the member table and the error word into
+// host-mapped pinned memory, so the host needs no size round trip before its
+// copy: total = end of the last member.
+__global__ void k_drain(BatchParams bp, uint8_t* h_out, MemberOut* h_mout, uint32_t* h_err) {
+    const uint32_t nmembers = bp.dims[1];
+    const size_t gtid = (size_t)blockIdx.x * blockDim.x + threadIdx.x, gstride = (size_t)gridDim.x * blockDim.x;
+    unsigned long long total = 0;
+    if (nmembers) {
+        const MemberOut last = bp.member_out[nmembers - 1];
+        total = last.gz_off + 18ull + last.deflate_bytes - bp.out_base;
+    }
+    const uint4* src = reinterpret_cast<const uint4*>(bp.out_words);
+    uint4* dst = reinterpret_cast<uint4*>(h_out);
+    const size_t nvec = (size_t)((total + 15u) >> 4);
+    for (size_t i = gtid; i < nvec; i += gstride) dst[i] = src[i];
+    for (size_t m = gtid; m < nmembers; m += gstride) h_mout[m] = bp.member_out[m];
+    if (gtid == 0) *h_err = *bp.err;
+}
+
 }  // namespace
 
 // ================================================================ launchers
@@ -1234,43 +1264,44 @@ int gpz_kernel_smem_setup() {
     return 0;
 }
 
-template <int T>
-static void launch_lookup(const BatchParams& bp, int grid, cudaStream_t s) {
-    k_segtab<512><<<grid, 512, kSegtabSmem, s>>>(bp);
-    k_lookup<T><<<grid, T, LookupSmem::kBytes, s>>>(bp);
-}
-
-int gpz_launch_batch(const BatchParams& bp, const LaunchShape& ls, void* stream, void* const* events) {
+int gpz_launch_batch(const BatchParams& bp, const LaunchShape& ls, void* stream, void* const* events,
+                     const DrainTarget* drain) {
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     auto mark = [&](int i) {
         if (events) cudaEventRecord(static_cast<cudaEvent_t>(events[i]), s);
     };
+    // grid 0: one CTA per item of this batch (the host knows the counts);
+    // otherwise a persistent grid that claims items from the device counters
     auto grid_of = [&](int g, uint32_t items) { return g > 0 ? g : (int)(items ? items : 1u); };
-    const int nm = bp.nmembers ? (int)bp.nmembers : 1;
+    const int nm = grid_of(0, bp.nmembers);
     mark(0);
+    const int gs = grid_of(ls.segtab_grid, bp.ntiles);
     const int gl = grid_of(ls.lookup_grid, bp.ntiles);
+    k_segtab<512><<<gs, 512, kSegtabSmem, s>>>(bp);
     switch (ls.lookup_threads) {
-        case 512: launch_lookup<512>(bp, gl, s); break;
-        default: launch_lookup<1024>(bp, gl, s); break;
+        case 512: k_lookup<512><<<gl, 512, LookupSmem::kBytes, s>>>(bp); break;
+        default: k_lookup<1024><<<gl, 1024, LookupSmem::kBytes, s>>>(bp); break;
     }
     mark(1);
     const int gw = grid_of(ls.walk_grid, bp.ntiles);
+    const int gc = ls.huff_grid > 0 ? ls.huff_grid : (nm + 127) / 128;
     switch (ls.walk_threads) {
         case 256:
             k_walk_exit<256><<<gw, 256, 0, s>>>(bp);
-            k_chain<<<(nm + 127) / 128, 128, 0, s>>>(bp);
+            k_chain<<<gc, 128, 0, s>>>(bp);
             k_walk_mark<256><<<gw, 256, 0, s>>>(bp);
             break;
         default:
             k_walk_exit<512><<<gw, 512, 0, s>>>(bp);
-            k_chain<<<(nm + 127) / 128, 128, 0, s>>>(bp);
+            k_chain<<<gc, 128, 0, s>>>(bp);
             k_walk_mark<512><<<gw, 512, 0, s>>>(bp);
             break;
     }
     mark(2);
-    k_huff<<<nm, kHuffThreads, 0, s>>>(bp);
+    const int gh = grid_of(ls.huff_grid, bp.nmembers);
+    k_huff<<<gh, kHuffThreads, 0, s>>>(bp);
     k_place<<<1, kPlaceThreads, 0, s>>>(bp);
-    k_frame<<<nm, kFrameThreads, 0, s>>>(bp);
+    k_frame<<<gh, kFrameThreads, 0, s>>>(bp);
     mark(3);
     const int ge = grid_of(ls.emit_grid, bp.ntiles);
     switch (ls.emit_threads) {
@@ -1278,5 +1309,29 @@ int gpz_launch_batch(const BatchParams& bp, const LaunchShape& ls, void* stream,
         default: k_emit<512><<<ge, 512, 0, s>>>(bp); break;
     }
     mark(4);
+    if (drain) k_drain<<<drain->grid, 256, 0, s>>>(bp, drain->h_out, drain->h_mout, drain->h_err);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int gpz_occupancy(LaunchShape* persistent) {
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return -1;
+    auto occ = [&](const void* f, int threads, size_t smem) {
+        int n = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f, threads, smem) != cudaSuccess || n < 1) n = 1;
+        return n;
+    };
+    persistent->segtab_grid = sms * occ((const void*)k_segtab<512>, 512, kSegtabSmem);
+    persistent->lookup_grid = sms * occ(persistent->lookup_threads == 512 ? (const void*)k_lookup<512>
+                                                                           : (const void*)k_lookup<1024>,
+                                        persistent->lookup_threads, LookupSmem::kBytes);
+    persistent->walk_grid = sms * occ(persistent->walk_threads == 256 ? (const void*)k_walk_mark<256>
+                                                                       : (const void*)k_walk_mark<512>,
+                                      persistent->walk_threads, 0);
+    persistent->huff_grid = sms * occ((const void*)k_huff, kHuffThreads, 0);
+    persistent->emit_grid = sms * occ(persistent->emit_threads == 256 ? (const void*)k_emit<256>
+                                                                       : (const void*)k_emit<512>,
+                                      persistent->emit_threads, 0);
+    return sms;
 }

@@ -1,10 +1,20 @@
 // gpz_runtime.cu -- host runtime and C ABI of the gzip compression path.
 //
 // Replaces the reference's wgpu plumbing (GpuContext, Lz77HashPipeline's
-// BufferSet pool, BatchedLz77's submitter/completer threads; gpu.rs:125-167,
-// lz77_hash.rs:98-297, batch.rs:48-141) with one CUDA context per gpz_ctx:
-// a device pool sized for a batch, pinned staging, and a batch planner that
-// cuts every input into members and 4 KiB tiles for the persistent kernels.
+// BufferSet pool, BatchedLz77's submitter / completer threads; gpu.rs:125-167,
+// lz77_hash.rs:98-297, batch.rs:48-141) with:
+//
+//  * pipeline slots: each has a CUDA stream, device arenas sized for a batch,
+//    pinned input staging and host-mapped output, so one batch uploads while
+//    the previous one computes and drains;
+//  * a batch planner that cuts every input into members (member_bytes each,
+//    gpu.rs:193-208) and members into 4 KiB tiles, written as one descriptor
+//    block (batch dimensions, members, tiles) that the persistent kernels
+//    read on the device;
+//  * one CUDA graph per (slot, size bucket): the memset of the work counters,
+//    the stage kernels with the bucket's autotuned launch shape, and the
+//    drain into mapped host memory;
+//  * a continuous-batching serving engine (gpz_submit / gpz_poll).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -14,7 +24,7 @@
 #include <cstdio>
 #include <cstring>
 #include <deque>
-#include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <thread>
@@ -28,8 +38,10 @@ namespace {
 
 constexpr size_t kDefaultMember = 131072;
 constexpr size_t kMaxMember = 2u << 20;
-constexpr size_t kDefaultBatch = 256u << 20;
+constexpr size_t kDefaultBatch = 128u << 20;
 constexpr size_t kDefaultPool = 40ull << 30;
+constexpr int kBuckets = 5;
+constexpr size_t kDescHeader = 64;  // batch dimensions at the start of a descriptor block
 
 size_t round_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
@@ -38,12 +50,86 @@ size_t round_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 // at most 15 + 5 + 15 + 13 bits), the EOB, and word slack.
 size_t member_bound(size_t n) { return 18 + 600 + 2 * n + 8; }
 
+// Size bucket of a batch by its tile count.
+int bucket_of(size_t ntiles) {
+    if (ntiles <= 64) return 0;
+    if (ntiles <= 512) return 1;
+    if (ntiles <= 4096) return 2;
+    if (ntiles <= 32768) return 3;
+    return 4;
+}
+
 struct DevArena {
     void* p = nullptr;
     size_t cap = 0;
 };
 
+double now_ms() {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// memcpy over several threads for large copies.
+void par_memcpy(void* dst, const void* src, size_t n) {
+    constexpr size_t kPiece = 4u << 20;
+    if (n < 2 * kPiece) {
+        std::memcpy(dst, src, n);
+        return;
+    }
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t nth = std::min<size_t>(std::min<size_t>(hw, 16), n / kPiece);
+    const size_t per = round_up((n + nth - 1) / nth, 64);
+    std::vector<std::thread> th;
+    for (size_t t = 1; t < nth; t++) {
+        const size_t o = t * per;
+        if (o >= n) break;
+        th.emplace_back([=] {
+            std::memcpy(static_cast<char*>(dst) + o, static_cast<const char*>(src) + o, std::min(per, n - o));
+        });
+    }
+    std::memcpy(dst, src, std::min(per, n));
+    for (auto& x : th) x.join();
+}
+
+struct Span {
+    size_t n = 0;
+    uint64_t dev_off = 0;     // where the input sits in the batch input
+    size_t first_member = 0;  // index into the slot's member list
+    size_t nmembers = 0;
+};
+
+struct Slot {
+    DevArena d_in, d_pp, d_tok, d_out, d_skeys, d_son, d_sposid, d_snkeys, d_tentry, d_texit, d_thist, d_tntok,
+        d_tbit, d_mcodes, d_mhdr, d_mout, d_cnt, d_members, d_tiles, d_dims;
+    uint8_t* h_in = nullptr;
+    size_t h_in_cap = 0;
+    uint8_t* h_desc = nullptr;
+    size_t h_desc_cap = 0;
+    uint8_t* h_out = nullptr;  // mapped
+    size_t h_out_cap = 0;
+    MemberOut* h_mout = nullptr;  // mapped
+    size_t h_mout_cap = 0;
+    uint32_t* h_err = nullptr;  // mapped
+    size_t h_err_cap = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    uint64_t gen = 1;  // bumps whenever a buffer the graphs capture moves
+    struct Graph {
+        uint64_t gen = 0;
+        cudaGraphExec_t exec = nullptr;
+    } graphs[kBuckets];
+    // the batch in flight
+    std::vector<MemberDesc> members;
+    std::vector<TileDesc> tiles;
+    std::vector<Span> spans;
+    size_t in_bytes = 0;
+    bool busy = false;
+    int bucket = 0;
+};
+
 }  // namespace
+
+struct ServeEngine;
 
 struct gpz_ctx {
     int device = 0;
@@ -51,34 +137,21 @@ struct gpz_ctx {
     size_t pool_cap = kDefaultPool;
     size_t batch_bytes = kDefaultBatch;
     int flags = 0;
-    cudaStream_t stream = nullptr;
-    std::mutex mu;  // one device pass at a time per context
+    int sms = 0;
+    std::mutex mu;  // the synchronous entry points (and their slots)
     std::string last_err;
-    uint64_t launches = 0;
-    LaunchShape shape{1024, 0, 512, 0, 512, 0};
-
-    // device pool (one batch in flight)
-    DevArena d_in, d_pp, d_tok, d_out, d_skeys, d_son, d_sposid, d_snkeys, d_tentry, d_texit, d_thist, d_tntok, d_tbit, d_mcodes, d_mhdr, d_mout,
-        d_cnt, d_members, d_tiles;
-    size_t pool_used = 0;
-    // pinned staging
-    uint8_t* h_in = nullptr;
-    size_t h_in_cap = 0;
-    uint8_t* h_out = nullptr;
-    size_t h_out_cap = 0;
-    std::vector<MemberDesc> members;
-    std::vector<TileDesc> tiles;
-    std::vector<MemberOut> mout;
-    MemberDesc* h_members = nullptr;
-    size_t h_members_cap = 0;
-    TileDesc* h_tiles = nullptr;
-    size_t h_tiles_cap = 0;
-    MemberOut* h_mout = nullptr;
-    size_t h_mout_cap = 0;
-    uint32_t* h_err = nullptr;
-    // per-stage CUDA events of the last pass (GPZ_FLAG_STAGE_TIMING)
-    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    std::atomic<uint64_t> launches{0};
+    std::atomic<size_t> pool_used{0};
+    LaunchShape fixed{0, 0, 0, 0, 0, 0, 0, 0};  // set by gpz_set_shape (threads > 0 overrides)
+    LaunchShape shape[kBuckets];
+    bool tuned[kBuckets] = {false, false, false, false, false};
+    std::mutex tune_mu;
+    Slot slots[2];
+    int next_slot = 0;
     float stage_ms[4] = {0, 0, 0, 0};
+    std::vector<MemberOut> mout;  // member table of the last synchronous pass
+    std::unique_ptr<ServeEngine> serve;
+    std::mutex serve_mu;
 };
 
 namespace {
@@ -94,13 +167,13 @@ int fail(gpz_ctx* c, int code, const char* what, cudaError_t e = cudaSuccess) {
     return code;
 }
 
-#define CU(ctx, call)                                                       \
-    do {                                                                    \
-        cudaError_t _e = (call);                                            \
-        if (_e != cudaSuccess) return fail((ctx), GPZ_E_CUDA, #call, _e);   \
+#define CU(ctx, call)                                                     \
+    do {                                                                  \
+        cudaError_t _e = (call);                                          \
+        if (_e != cudaSuccess) return fail((ctx), GPZ_E_CUDA, #call, _e); \
     } while (0)
 
-int ensure_dev(gpz_ctx* c, DevArena& a, size_t bytes) {
+int ensure_dev(gpz_ctx* c, Slot& sl, DevArena& a, size_t bytes) {
     bytes = round_up(std::max<size_t>(bytes, 256), 256);
     if (a.cap >= bytes) return GPZ_OK;
     size_t grow = std::max(bytes, a.cap + a.cap / 2);
@@ -112,6 +185,7 @@ int ensure_dev(gpz_ctx* c, DevArena& a, size_t bytes) {
     c->pool_used -= a.cap;
     a.p = nullptr;
     a.cap = 0;
+    sl.gen++;
     cudaError_t e = cudaMalloc(&a.p, grow);
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -123,247 +197,642 @@ int ensure_dev(gpz_ctx* c, DevArena& a, size_t bytes) {
 }
 
 template <class T>
-int ensure_host(gpz_ctx* c, T*& p, size_t& cap, size_t count) {
+int ensure_host(gpz_ctx* c, Slot& sl, T*& p, size_t& cap, size_t count, bool mapped) {
     if (cap >= count) return GPZ_OK;
     size_t grow = std::max(count, cap + cap / 2);
     if (p) cudaFreeHost(p);
     p = nullptr;
     cap = 0;
-    cudaError_t e = cudaMallocHost(reinterpret_cast<void**>(&p), grow * sizeof(T));
+    if (mapped) sl.gen++;
+    cudaError_t e = cudaHostAlloc(reinterpret_cast<void**>(&p), grow * sizeof(T),
+                                  mapped ? cudaHostAllocMapped : cudaHostAllocDefault);
     if (e != cudaSuccess) {
         cudaGetLastError();
-        return fail(c, GPZ_E_NOMEM, "cudaMallocHost", e);
+        return fail(c, GPZ_E_NOMEM, "cudaHostAlloc", e);
     }
     cap = grow;
     return GPZ_OK;
 }
 
-struct Span {
-    size_t n;
-    uint64_t dev_off;      // where the input sits in the device input buffer
-    size_t first_member;   // index into ctx->members
-    size_t nmembers;
-};
+template <class T>
+T* mapped_dev(T* host) {
+    void* d = nullptr;
+    if (cudaHostGetDevicePointer(&d, host, 0) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return static_cast<T*>(d);
+}
 
-// Cut inputs into members (member_bytes each, gpu.rs:193-208: an input of at
-// most member_bytes, empty included, is one member) and members into tiles.
-void plan(gpz_ctx* c, std::vector<Span>& spans) {
-    c->members.clear();
-    c->tiles.clear();
-    for (auto& s : spans) {
-        s.first_member = c->members.size();
-        size_t nm = s.n == 0 ? 1 : (s.n + c->member_bytes - 1) / c->member_bytes;
+// Cut inputs into members (gpu.rs:193-208: an input of at most member_bytes,
+// empty included, is one member) and members into tiles.
+void plan(const gpz_ctx* c, Slot& sl) {
+    sl.members.clear();
+    sl.tiles.clear();
+    for (auto& s : sl.spans) {
+        s.first_member = sl.members.size();
+        const size_t nm = s.n == 0 ? 1 : (s.n + c->member_bytes - 1) / c->member_bytes;
         s.nmembers = nm;
         for (size_t j = 0; j < nm; j++) {
             MemberDesc md{};
             md.in_off = s.dev_off + j * c->member_bytes;
             md.len = (uint32_t)std::min(c->member_bytes, s.n - std::min(s.n, j * c->member_bytes));
-            md.tile_base = (uint32_t)c->tiles.size();
+            md.tile_base = (uint32_t)sl.tiles.size();
             md.ntiles = (md.len + GPZ_SEG - 1) / GPZ_SEG;
             md.level = 0;
-            md.out_slot = c->members.size();
-            for (uint32_t t = 0; t < md.ntiles; t++) c->tiles.push_back(TileDesc{(uint32_t)c->members.size(), t});
-            c->members.push_back(md);
+            md.out_slot = sl.members.size();
+            for (uint32_t t = 0; t < md.ntiles; t++) sl.tiles.push_back(TileDesc{(uint32_t)sl.members.size(), t});
+            sl.members.push_back(md);
         }
     }
 }
 
-// Sizes every device array for the planned batch.
-int reserve(gpz_ctx* c, size_t in_bytes, bool own_in, bool own_out, size_t out_bytes) {
-    const size_t nm = c->members.size(), nt = std::max<size_t>(c->tiles.size(), 1);
-    int rc;
-    if (own_in && (rc = ensure_dev(c, c->d_in, in_bytes + 64))) return rc;
-    if ((rc = ensure_dev(c, c->d_pp, in_bytes * 4 + 64))) return rc;
-    if ((rc = ensure_dev(c, c->d_tok, in_bytes * 4 + 64))) return rc;
-    if (own_out && (rc = ensure_dev(c, c->d_out, out_bytes + 64))) return rc;
-    if ((rc = ensure_dev(c, c->d_skeys, nt * GPZ_SEG * 2))) return rc;
-    if ((rc = ensure_dev(c, c->d_son, nt * GPZ_SEG * 4))) return rc;
-    if ((rc = ensure_dev(c, c->d_sposid, nt * GPZ_SEG * 2))) return rc;
-    if ((rc = ensure_dev(c, c->d_snkeys, nt * 4))) return rc;
-    if ((rc = ensure_dev(c, c->d_tentry, nt * 4))) return rc;
-    if ((rc = ensure_dev(c, c->d_texit, nt * GPZ_EXITS * 2))) return rc;
-    if ((rc = ensure_dev(c, c->d_thist, nt * GPZ_NSYM * 2))) return rc;
-    if ((rc = ensure_dev(c, c->d_tntok, nt * 4))) return rc;
-    if ((rc = ensure_dev(c, c->d_tbit, nt * 4))) return rc;
-    if ((rc = ensure_dev(c, c->d_mcodes, nm * GPZ_NSYM * 4))) return rc;
-    if ((rc = ensure_dev(c, c->d_mout, nm * sizeof(MemberOut)))) return rc;
-    if ((rc = ensure_dev(c, c->d_mhdr, nm * GPZ_HDR_WORDS * 4))) return rc;
-    if ((rc = ensure_dev(c, c->d_cnt, GPZ_NCOUNTERS * 4 + 64))) return rc;
-    if ((rc = ensure_dev(c, c->d_members, nm * sizeof(MemberDesc)))) return rc;
-    if ((rc = ensure_dev(c, c->d_tiles, nt * sizeof(TileDesc)))) return rc;
-    if ((rc = ensure_host(c, c->h_members, c->h_members_cap, nm))) return rc;
-    if ((rc = ensure_host(c, c->h_tiles, c->h_tiles_cap, nt))) return rc;
-    if ((rc = ensure_host(c, c->h_mout, c->h_mout_cap, nm))) return rc;
-    return GPZ_OK;
-}
-
-size_t out_bound_of_plan(const gpz_ctx* c) {
+size_t out_bound_of_plan(const Slot& sl) {
     size_t b = 0;
-    for (auto& m : c->members) b += member_bound(m.len);
+    for (auto& m : sl.members) b += member_bound(m.len);
     return b;
 }
 
-// Upload descriptors, clear the look-back state, launch the four stages and
-// read back the member table.  in/out are device pointers.
-int run_device(gpz_ctx* c, const uint8_t* d_in, uint8_t* d_out, cudaStream_t s) {
-    const size_t nm = c->members.size(), nt = c->tiles.size();
-    std::memcpy(c->h_members, c->members.data(), nm * sizeof(MemberDesc));
-    if (nt) std::memcpy(c->h_tiles, c->tiles.data(), nt * sizeof(TileDesc));
-    CU(c, cudaMemcpyAsync(c->d_members.p, c->h_members, nm * sizeof(MemberDesc), cudaMemcpyHostToDevice, s));
-    if (nt) CU(c, cudaMemcpyAsync(c->d_tiles.p, c->h_tiles, nt * sizeof(TileDesc), cudaMemcpyHostToDevice, s));
-    CU(c, cudaMemsetAsync(c->d_cnt.p, 0, GPZ_NCOUNTERS * 4 + 64, s));
+size_t desc_bytes(size_t nm, size_t nt) { return kDescHeader + nm * sizeof(MemberDesc) + nt * sizeof(TileDesc); }
 
+// The descriptor arenas have fixed addresses between reallocations (which
+// bump the slot's generation), so a captured graph stays valid for any batch
+// that fits them.
+
+// Sizes every device array (and the pinned staging) for the planned batch.
+int reserve(gpz_ctx* c, Slot& sl, size_t in_bytes, bool own_in, bool own_out, size_t out_bytes) {
+    const size_t nm = std::max<size_t>(sl.members.size(), 1), nt = std::max<size_t>(sl.tiles.size(), 1);
+    int rc;
+    if (own_in && (rc = ensure_dev(c, sl, sl.d_in, in_bytes + 64))) return rc;
+    if ((rc = ensure_dev(c, sl, sl.d_pp, in_bytes * 4 + 64))) return rc;
+    if ((rc = ensure_dev(c, sl, sl.d_tok, in_bytes * 4 + 64))) return rc;
+    if (own_out && (rc = ensure_dev(c, sl, sl.d_out, out_bytes + 64))) return rc;
+    if ((rc = ensure_dev(c, sl, sl.d_skeys, nt * GPZ_SEG * 2))) return rc;
+    if ((rc = ensure_dev(c, sl, sl.d_son, nt * GPZ_SEG * 4))) return rc;
+    if ((rc = ensure_dev(c, sl, sl.d_sposid, nt * GPZ_SEG * 2))) return rc;
+    if ((rc = ensure_dev(c, sl, sl.d_snkeys, nt * 4))) return rc;
+    if ((rc = ensure_dev(c, sl, sl.d_tentry, nt * 4))) return rc;
+    if ((rc = ensure_dev(c, sl, sl.d_texit, nt * GPZ_EXITS * 2))) return rc;
+    if ((rc = ensure_dev(c, sl, sl.d_thist, nt * GPZ_NSYM * 2))) return rc;
+    if ((rc = ensure_dev(c, sl, sl.d_tntok, nt * 4))) return rc;
+    if ((rc = ensure_dev(c, sl, sl.d_tbit, nt * 4))) return rc;
+    if ((rc = ensure_dev(c, sl, sl.d_mcodes, nm * GPZ_NSYM * 4))) return rc;
+    if ((rc = ensure_dev(c, sl, sl.d_mhdr, nm * GPZ_HDR_WORDS * 4))) return rc;
+    if ((rc = ensure_dev(c, sl, sl.d_mout, nm * sizeof(MemberOut)))) return rc;
+    if ((rc = ensure_dev(c, sl, sl.d_cnt, GPZ_NCOUNTERS * 4 + 64))) return rc;
+    if ((rc = ensure_dev(c, sl, sl.d_members, nm * sizeof(MemberDesc)))) return rc;
+    if ((rc = ensure_dev(c, sl, sl.d_tiles, nt * sizeof(TileDesc)))) return rc;
+    if ((rc = ensure_dev(c, sl, sl.d_dims, kDescHeader))) return rc;
+    if ((rc = ensure_host(c, sl, sl.h_desc, sl.h_desc_cap, desc_bytes(nm, nt), false))) return rc;
+    if ((rc = ensure_host(c, sl, sl.h_mout, sl.h_mout_cap, nm, true))) return rc;
+    if ((rc = ensure_host(c, sl, sl.h_err, sl.h_err_cap, 16, true))) return rc;
+    return GPZ_OK;
+}
+
+BatchParams params_of(Slot& sl, const uint8_t* d_in, uint8_t* d_out) {
     BatchParams bp{};
     bp.in = d_in;
-    bp.members = static_cast<const MemberDesc*>(c->d_members.p);
-    bp.tiles = static_cast<const TileDesc*>(c->d_tiles.p);
-    bp.pp = static_cast<uint32_t*>(c->d_pp.p);
-    bp.tok = static_cast<uint32_t*>(c->d_tok.p);
+    bp.dims = static_cast<const uint32_t*>(sl.d_dims.p);
+    bp.members = static_cast<const MemberDesc*>(sl.d_members.p);
+    bp.tiles = static_cast<const TileDesc*>(sl.d_tiles.p);
+    bp.pp = static_cast<uint32_t*>(sl.d_pp.p);
+    bp.seg_keys = static_cast<uint16_t*>(sl.d_skeys.p);
+    bp.seg_on = static_cast<uint32_t*>(sl.d_son.p);
+    bp.seg_posid = static_cast<uint16_t*>(sl.d_sposid.p);
+    bp.seg_nkeys = static_cast<uint32_t*>(sl.d_snkeys.p);
+    bp.tok = static_cast<uint32_t*>(sl.d_tok.p);
     bp.out_words = reinterpret_cast<uint32_t*>(d_out);
-    bp.seg_keys = static_cast<uint16_t*>(c->d_skeys.p);
-    bp.seg_on = static_cast<uint32_t*>(c->d_son.p);
-    bp.seg_posid = static_cast<uint16_t*>(c->d_sposid.p);
-    bp.seg_nkeys = static_cast<uint32_t*>(c->d_snkeys.p);
-    bp.tile_entry = static_cast<uint32_t*>(c->d_tentry.p);
-    bp.tile_exit = static_cast<uint16_t*>(c->d_texit.p);
-    bp.tile_hist = static_cast<uint16_t*>(c->d_thist.p);
-    bp.tile_ntok = static_cast<uint32_t*>(c->d_tntok.p);
-    bp.tile_bitoff = static_cast<uint32_t*>(c->d_tbit.p);
-    bp.member_codes = static_cast<uint32_t*>(c->d_mcodes.p);
-    bp.member_out = static_cast<MemberOut*>(c->d_mout.p);
-    bp.member_hdr = static_cast<uint32_t*>(c->d_mhdr.p);
-    bp.counters = static_cast<uint32_t*>(c->d_cnt.p);
+    bp.tile_entry = static_cast<uint32_t*>(sl.d_tentry.p);
+    bp.tile_exit = static_cast<uint16_t*>(sl.d_texit.p);
+    bp.tile_hist = static_cast<uint16_t*>(sl.d_thist.p);
+    bp.tile_ntok = static_cast<uint32_t*>(sl.d_tntok.p);
+    bp.tile_bitoff = static_cast<uint32_t*>(sl.d_tbit.p);
+    bp.member_codes = static_cast<uint32_t*>(sl.d_mcodes.p);
+    bp.member_hdr = static_cast<uint32_t*>(sl.d_mhdr.p);
+    bp.member_out = static_cast<MemberOut*>(sl.d_mout.p);
+    bp.counters = static_cast<uint32_t*>(sl.d_cnt.p);
     bp.err = bp.counters + GPZ_NCOUNTERS;
-    bp.nmembers = (uint32_t)nm;
-    bp.ntiles = (uint32_t)nt;
+    bp.nmembers = (uint32_t)sl.members.size();
+    bp.ntiles = (uint32_t)sl.tiles.size();
     bp.out_base = 0;
-    const bool timing = (c->flags & GPZ_FLAG_STAGE_TIMING) && c->ev[0];
-    if (gpz_launch_batch(bp, c->shape, s, timing ? reinterpret_cast<void* const*>(c->ev) : nullptr) != 0)
-        return fail(c, GPZ_E_CUDA, "kernel launch", cudaGetLastError());
-    c->launches = 9;
-    CU(c, cudaMemcpyAsync(c->h_mout, c->d_mout.p, nm * sizeof(MemberOut), cudaMemcpyDeviceToHost, s));
-    CU(c, cudaMemcpyAsync(c->h_err, bp.err, 4, cudaMemcpyDeviceToHost, s));
-    CU(c, cudaStreamSynchronize(s));
-    c->mout.assign(c->h_mout, c->h_mout + nm);
-    if (timing)
-        for (int i = 0; i < 4; i++) cudaEventElapsedTime(&c->stage_ms[i], c->ev[i], c->ev[i + 1]);
-    const uint32_t err = *c->h_err;
+    return bp;
+}
+
+// Descriptors staged as [dims][members][tiles] in pinned memory, uploaded
+// into their three arenas.
+int upload_desc(gpz_ctx* c, Slot& sl, cudaStream_t s) {
+    const size_t nm = sl.members.size(), nt = sl.tiles.size();
+    uint32_t* dims = reinterpret_cast<uint32_t*>(sl.h_desc);
+    std::memset(dims, 0, kDescHeader);
+    dims[0] = (uint32_t)nt;
+    dims[1] = (uint32_t)nm;
+    uint8_t* hm = sl.h_desc + kDescHeader;
+    uint8_t* ht = hm + nm * sizeof(MemberDesc);
+    std::memcpy(hm, sl.members.data(), nm * sizeof(MemberDesc));
+    if (nt) std::memcpy(ht, sl.tiles.data(), nt * sizeof(TileDesc));
+    CU(c, cudaMemcpyAsync(sl.d_dims.p, sl.h_desc, kDescHeader, cudaMemcpyHostToDevice, s));
+    CU(c, cudaMemcpyAsync(sl.d_members.p, hm, nm * sizeof(MemberDesc), cudaMemcpyHostToDevice, s));
+    if (nt) CU(c, cudaMemcpyAsync(sl.d_tiles.p, ht, nt * sizeof(TileDesc), cudaMemcpyHostToDevice, s));
+    return GPZ_OK;
+}
+
+LaunchShape shape_for(gpz_ctx* c, int bucket) {
+    LaunchShape s;
+    {
+        std::lock_guard<std::mutex> lk(c->tune_mu);
+        s = c->shape[bucket];
+    }
+    if (c->fixed.lookup_threads) {
+        LaunchShape f{c->fixed.lookup_threads, 0, c->fixed.walk_threads, 0, c->fixed.emit_threads, 0, 0, 0};
+        gpz_occupancy(&f);
+        if (c->fixed.lookup_grid) f.lookup_grid = c->fixed.lookup_grid;
+        if (c->fixed.walk_grid) f.walk_grid = c->fixed.walk_grid;
+        if (c->fixed.emit_grid) f.emit_grid = c->fixed.emit_grid;
+        s = f;
+    }
+    return s;
+}
+
+// Stage kernels (+ drain) for the slot's planned batch, as a CUDA graph per
+// (slot, bucket) or as direct launches on stream s.
+int launch(gpz_ctx* c, Slot& sl, const BatchParams& bp, const LaunchShape& shape, bool use_graph,
+           const DrainTarget* drain, bool timing, cudaStream_t s) {
+    if (!use_graph) {
+        CU(c, cudaMemsetAsync(sl.d_cnt.p, 0, GPZ_NCOUNTERS * 4 + 64, s));
+        if (gpz_launch_batch(bp, shape, s, timing ? reinterpret_cast<void* const*>(sl.ev) : nullptr, drain) != 0)
+            return fail(c, GPZ_E_CUDA, "kernel launch", cudaGetLastError());
+        c->launches = 10 + (drain ? 1 : 0);
+        return GPZ_OK;
+    }
+    Slot::Graph& g = sl.graphs[sl.bucket];
+    if (g.exec && g.gen != sl.gen) {
+        cudaGraphExecDestroy(g.exec);
+        g.exec = nullptr;
+    }
+    if (!g.exec) {
+        cudaGraph_t graph = nullptr;
+        CU(c, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        cudaMemsetAsync(sl.d_cnt.p, 0, GPZ_NCOUNTERS * 4 + 64, s);
+        gpz_launch_batch(bp, shape, s, nullptr, drain);
+        cudaError_t e = cudaStreamEndCapture(s, &graph);
+        if (e != cudaSuccess) return fail(c, GPZ_E_CUDA, "graph capture", e);
+        e = cudaGraphInstantiate(&g.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+            g.exec = nullptr;
+            return fail(c, GPZ_E_CUDA, "graph instantiate", e);
+        }
+        g.gen = sl.gen;
+    }
+    CU(c, cudaGraphLaunch(g.exec, s));
+    c->launches = 10 + (drain ? 1 : 0);
+    return GPZ_OK;
+}
+
+// Persistent default shape for every bucket; tuned lazily on first use.
+void default_shapes(gpz_ctx* c) {
+    for (int b = 0; b < kBuckets; b++) {
+        LaunchShape s{1024, 0, 512, 0, 512, 0, 0, 0};
+        gpz_occupancy(&s);
+        c->shape[b] = s;
+    }
+}
+
+// Autotuner: each candidate (threads per lookup CTA, per walk CTA, per emit
+// CTA, with persistent grids from occupancy) runs the batch once -- every
+// shape gives the same output -- and the fastest becomes the bucket's shape.
+int autotune(gpz_ctx* c, Slot& sl, const BatchParams& bp, const DrainTarget* dt, cudaStream_t s) {
+    const int lt[2] = {1024, 512}, wt[2] = {512, 256}, et[2] = {512, 256};
+    float best = 1e30f;
+    LaunchShape best_s = c->shape[sl.bucket];
+    cudaEvent_t a, b;
+    CU(c, cudaEventCreate(&a));
+    CU(c, cudaEventCreate(&b));
+    int rc = GPZ_OK;
+    for (int i = 0; i < 8 && rc == GPZ_OK; i++) {
+        LaunchShape cand{lt[i & 1], 0, wt[(i >> 1) & 1], 0, et[(i >> 2) & 1], 0, 0, 0};
+        gpz_occupancy(&cand);
+        cudaEventRecord(a, s);
+        rc = launch(c, sl, bp, cand, false, dt, false, s);
+        cudaEventRecord(b, s);
+        if (cudaEventSynchronize(b) != cudaSuccess) rc = fail(c, GPZ_E_CUDA, "autotune", cudaGetLastError());
+        float ms = 0;
+        cudaEventElapsedTime(&ms, a, b);
+        if (rc == GPZ_OK && ms < best) {
+            best = ms;
+            best_s = cand;
+        }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(c->tune_mu);
+    c->shape[sl.bucket] = best_s;
+    c->tuned[sl.bucket] = true;
+    return GPZ_OK;
+}
+
+// Plans, uploads and launches one batch of host items on a slot (no wait).
+int submit_slot(gpz_ctx* c, Slot& sl, const gpz_desc* d, size_t count, bool plain) {
+    sl.spans.assign(count, Span{});
+    size_t in_bytes = 0;
+    for (size_t i = 0; i < count; i++) {
+        sl.spans[i].n = d[i].n;
+        sl.spans[i].dev_off = in_bytes;
+        in_bytes += round_up(std::max<size_t>(d[i].n, 1), 16);
+    }
+    sl.in_bytes = in_bytes;
+    plan(c, sl);
+    const size_t obound = out_bound_of_plan(sl);
+    int rc;
+    if ((rc = reserve(c, sl, in_bytes, true, true, obound))) return rc;
+    if ((rc = ensure_host(c, sl, sl.h_in, sl.h_in_cap, in_bytes + 64, false))) return rc;
+    if ((rc = ensure_host(c, sl, sl.h_out, sl.h_out_cap, obound + 64, true))) return rc;
+    for (size_t i = 0; i < count; i++)
+        if (d[i].n) par_memcpy(sl.h_in + sl.spans[i].dev_off, d[i].in, d[i].n);
+    cudaStream_t s = sl.stream;
+    CU(c, cudaMemcpyAsync(sl.d_in.p, sl.h_in, in_bytes, cudaMemcpyHostToDevice, s));
+    if ((rc = upload_desc(c, sl, s))) return rc;
+    BatchParams bp = params_of(sl, static_cast<const uint8_t*>(sl.d_in.p), static_cast<uint8_t*>(sl.d_out.p));
+    DrainTarget dt{mapped_dev(sl.h_out), mapped_dev(sl.h_mout), mapped_dev(sl.h_err), c->sms * 4};
+    if (!dt.h_out || !dt.h_mout || !dt.h_err) return fail(c, GPZ_E_CUDA, "mapped host memory");
+    sl.bucket = bucket_of(sl.tiles.size());
+    const bool timing = (c->flags & GPZ_FLAG_STAGE_TIMING) != 0;
+    if (plain) {
+        // one launch per kernel, grids sized to this batch, no graph
+        const LaunchShape exact{1024, 0, 512, 0, 512, 0, 0, 0};
+        rc = launch(c, sl, bp, exact, false, &dt, timing, s);
+    } else {
+        bool tuned;
+        {
+            std::lock_guard<std::mutex> lk(c->tune_mu);
+            tuned = c->tuned[sl.bucket];
+        }
+        if (!tuned && !(c->flags & GPZ_FLAG_NO_AUTOTUNE) && !c->fixed.lookup_threads &&
+            (rc = autotune(c, sl, bp, &dt, s)))
+            return rc;
+        const bool graphs = !(c->flags & GPZ_FLAG_NO_GRAPHS) && !timing;
+        rc = launch(c, sl, bp, shape_for(c, sl.bucket), graphs, &dt, timing, s);
+    }
+    if (rc) return rc;
+    CU(c, cudaEventRecord(sl.done, s));
+    sl.busy = true;
+    return GPZ_OK;
+}
+
+// 10-byte header and 8-byte trailer of every member (deflate.rs:962-980),
+// written into a host copy of the batch output that starts at `base`.
+void frame_members(const MemberOut* mo, size_t first, size_t count, uint8_t* dst, uint64_t base) {
+    static const uint8_t hdr[10] = {0x1f, 0x8b, 0x08, 0x00, 0x00, 0x00, 0x00, 0x00, 0x00, 0xff};
+    for (size_t m = first; m < first + count; m++) {
+        uint8_t* p = dst + (mo[m].gz_off - base);
+        std::memcpy(p, hdr, 10);
+        uint8_t* t = p + 10 + mo[m].deflate_bytes;
+        for (int i = 0; i < 4; i++) t[i] = (uint8_t)(mo[m].crc >> (8 * i));
+        for (int i = 0; i < 4; i++) t[4 + i] = (uint8_t)(mo[m].len >> (8 * i));
+    }
+}
+
+// Waits for the slot's batch; returns the device status.
+int wait_slot(gpz_ctx* c, Slot& sl) {
+    sl.busy = false;
+    CU(c, cudaEventSynchronize(sl.done));
+    if (c->flags & GPZ_FLAG_STAGE_TIMING)
+        for (int i = 0; i < 4; i++) cudaEventElapsedTime(&c->stage_ms[i], sl.ev[i], sl.ev[i + 1]);
+    const uint32_t err = *sl.h_err;
     if (err & GPZ_ERRBIT_SPIN) return fail(c, GPZ_E_TIMEOUT, "bounded device wait expired");
     if (err) return fail(c, GPZ_E_INTERNAL, "device self-check failed");
     return GPZ_OK;
 }
 
-uint64_t batch_out_bytes(const gpz_ctx* c) {
-    if (c->mout.empty()) return 0;
-    const MemberOut& l = c->mout.back();
-    return l.gz_off + 18 + l.deflate_bytes;
-}
-
-// 10-byte header and 8-byte trailer of every member (deflate.rs:962-980),
-// written into a host copy of the batch output that starts at `base`.
-void frame_members(const gpz_ctx* c, size_t first, size_t count, uint8_t* dst, uint64_t base) {
-    static const uint8_t hdr[10] = {0x1f, 0x8b, 0x08, 0x00, 0x00, 0x00, 0x00, 0x00, 0x00, 0xff};
-    for (size_t m = first; m < first + count; m++) {
-        const MemberOut& mo = c->mout[m];
-        uint8_t* p = dst + (mo.gz_off - base);
-        std::memcpy(p, hdr, 10);
-        uint8_t* t = p + 10 + mo.deflate_bytes;
-        for (int i = 0; i < 4; i++) t[i] = (uint8_t)(mo.crc >> (8 * i));
-        for (int i = 0; i < 4; i++) t[4 + i] = (uint8_t)(mo.len >> (8 * i));
-    }
-}
-
-// Host inputs -> one device pass -> host outputs.  Items must fit one batch.
-int run_host_batch(gpz_ctx* c, const gpz_desc* d, size_t count, gpz_out* outs, uint32_t* pp_out = nullptr,
-                   uint32_t* tok_out = nullptr, size_t* ntok = nullptr) {
-    std::vector<Span> spans(count);
-    size_t in_bytes = 0;
-    for (size_t i = 0; i < count; i++) {
-        spans[i].n = d[i].n;
-        spans[i].dev_off = in_bytes;
-        in_bytes += round_up(std::max<size_t>(d[i].n, 1), 16);
-    }
-    plan(c, spans);
-    const size_t obound = out_bound_of_plan(c);
-    int rc;
-    if ((rc = reserve(c, in_bytes, true, true, obound))) return rc;
-    if ((rc = ensure_host(c, c->h_in, c->h_in_cap, in_bytes + 64))) return rc;
-    for (size_t i = 0; i < count; i++)
-        if (d[i].n) std::memcpy(c->h_in + spans[i].dev_off, d[i].in, d[i].n);
-    cudaStream_t s = c->stream;
-    CU(c, cudaMemcpyAsync(c->d_in.p, c->h_in, in_bytes, cudaMemcpyHostToDevice, s));
-    if ((rc = run_device(c, static_cast<const uint8_t*>(c->d_in.p), static_cast<uint8_t*>(c->d_out.p), s)))
-        return rc;
-    const uint64_t total = batch_out_bytes(c);
-    if ((rc = ensure_host(c, c->h_out, c->h_out_cap, total + 64))) return rc;
-    CU(c, cudaMemcpyAsync(c->h_out, c->d_out.p, total, cudaMemcpyDeviceToHost, s));
-    if (pp_out && in_bytes) {
-        // per-position tokens of input 0 (debug path: one input)
-        CU(c, cudaMemcpyAsync(pp_out, c->d_pp.p, d[0].n * 4, cudaMemcpyDeviceToHost, s));
-    }
-    std::vector<uint32_t> tok_all, tntok;
-    if (tok_out && ntok) {
-        tok_all.resize(std::max<size_t>(d[0].n, 1));
-        tntok.resize(std::max<size_t>(c->tiles.size(), 1));
-        if (d[0].n) CU(c, cudaMemcpyAsync(tok_all.data(), c->d_tok.p, d[0].n * 4, cudaMemcpyDeviceToHost, s));
-        if (!c->tiles.empty())
-            CU(c, cudaMemcpyAsync(tntok.data(), c->d_tntok.p, c->tiles.size() * 4, cudaMemcpyDeviceToHost, s));
-    }
-    CU(c, cudaStreamSynchronize(s));
-    frame_members(c, 0, c->members.size(), c->h_out, 0);
+// Waits for the slot's batch, frames it and copies each item's gzip stream
+// into its caller buffer.
+int finish_slot(gpz_ctx* c, Slot& sl, gpz_out* outs, size_t first_item) {
+    int rc = wait_slot(c, sl);
+    const size_t nm = sl.members.size();
+    c->mout.assign(sl.h_mout, sl.h_mout + nm);
+    if (rc) return rc;
+    frame_members(sl.h_mout, 0, nm, sl.h_out, 0);
     int first_bad = GPZ_OK;
-    for (size_t i = 0; i < count; i++) {
-        const Span& sp = spans[i];
-        const MemberOut& a = c->mout[sp.first_member];
-        const MemberOut& z = c->mout[sp.first_member + sp.nmembers - 1];
+    for (size_t i = 0; i < sl.spans.size(); i++) {
+        const Span& sp = sl.spans[i];
+        const MemberOut& a = sl.h_mout[sp.first_member];
+        const MemberOut& z = sl.h_mout[sp.first_member + sp.nmembers - 1];
         const uint64_t beg = a.gz_off, end = z.gz_off + 18 + z.deflate_bytes;
-        outs[i].out_len = end - beg;
-        if (!outs[i].out || outs[i].out_cap < end - beg) {
-            outs[i].status = GPZ_E_SPACE;
+        gpz_out& o = outs[first_item + i];
+        o.out_len = end - beg;
+        if (!o.out || o.out_cap < end - beg) {
+            o.status = GPZ_E_SPACE;
             if (first_bad == GPZ_OK) first_bad = GPZ_E_SPACE;
             continue;
         }
-        std::memcpy(outs[i].out, c->h_out + beg, end - beg);
-        outs[i].status = GPZ_OK;
-    }
-    if (tok_out && ntok) {
-        size_t k = 0;
-        for (size_t t = 0; t < c->tiles.size(); t++) {
-            const TileDesc& td = c->tiles[t];
-            const MemberDesc& md = c->members[td.member];
-            const uint32_t* src = tok_all.data() + md.in_off + ((size_t)td.seg << GPZ_SEG_LOG2);
-            std::memcpy(tok_out + k, src, tntok[t] * 4);
-            k += tntok[t];
-        }
-        *ntok = k;
+        par_memcpy(o.out, sl.h_out + beg, end - beg);
+        o.status = GPZ_OK;
     }
     if (first_bad != GPZ_OK) fail(c, first_bad, "output buffer too small");
     return first_bad;
 }
 
-// Split a list of items into device passes of at most batch_bytes input.
+// Items -> device passes of at most batch_bytes, pipelined over both slots
+// (plain: one item per pass, waited for before the next).
 int run_host_items(gpz_ctx* c, const gpz_desc* d, size_t count, gpz_out* outs, bool plain) {
-    int first_bad = GPZ_OK;
+    int first_bad = GPZ_OK, fatal = GPZ_OK;
+    size_t pending_first[2] = {0, 0};
+    auto settle = [&](int k) {
+        Slot& sl = c->slots[k];
+        if (!sl.busy) return;
+        int rc = finish_slot(c, sl, outs, pending_first[k]);
+        if (rc != GPZ_OK && rc != GPZ_E_SPACE) {
+            for (size_t q = 0; q < sl.spans.size(); q++) outs[pending_first[k] + q].status = rc;
+            if (fatal == GPZ_OK) fatal = rc;
+        } else if (rc != GPZ_OK && first_bad == GPZ_OK) {
+            first_bad = rc;
+        }
+    };
     size_t i = 0;
-    while (i < count) {
+    while (i < count && fatal == GPZ_OK) {
         size_t j = i, bytes = 0;
         if (plain) {
             j = i + 1;
         } else {
             while (j < count && (j == i || bytes + d[j].n <= c->batch_bytes)) bytes += d[j++].n;
         }
-        int rc = run_host_batch(c, d + i, j - i, outs + i);
-        if (rc != GPZ_OK && rc != GPZ_E_SPACE) {
-            for (size_t k = i; k < j; k++) outs[k].status = rc;
-            return rc;
+        const int k = plain ? 0 : c->next_slot;
+        settle(k);
+        if (fatal) break;
+        int rc = submit_slot(c, c->slots[k], d + i, j - i, plain);
+        if (rc) {
+            for (size_t q = i; q < j; q++) outs[q].status = rc;
+            fatal = rc;
+            break;
         }
-        if (rc != GPZ_OK && first_bad == GPZ_OK) first_bad = rc;
+        pending_first[k] = i;
+        if (plain) settle(0);
+        else c->next_slot ^= 1;
         i = j;
     }
-    return first_bad;
+    for (int q = 0; q < 2; q++) settle((c->next_slot + q) & 1);
+    return fatal != GPZ_OK ? fatal : first_bad;
+}
+
+int init_slot(gpz_ctx* c, Slot& sl) {
+    CU(c, cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking));
+    CU(c, cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
+    if (c->flags & GPZ_FLAG_STAGE_TIMING)
+        for (auto& e : sl.ev) CU(c, cudaEventCreate(&e));
+    return ensure_host(c, sl, sl.h_err, sl.h_err_cap, 16, true);
+}
+
+void free_slot(gpz_ctx* c, Slot& sl) {
+    if (sl.stream) cudaStreamSynchronize(sl.stream);
+    for (auto& g : sl.graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    for (DevArena* a : {&sl.d_in, &sl.d_pp, &sl.d_tok, &sl.d_out, &sl.d_skeys, &sl.d_son, &sl.d_sposid, &sl.d_snkeys,
+                        &sl.d_tentry, &sl.d_texit, &sl.d_thist, &sl.d_tntok, &sl.d_tbit, &sl.d_mcodes, &sl.d_mhdr,
+                        &sl.d_mout, &sl.d_cnt, &sl.d_members, &sl.d_tiles, &sl.d_dims})
+        if (a->p) {
+            cudaFree(a->p);
+            c->pool_used -= a->cap;
+            a->p = nullptr;
+            a->cap = 0;
+        }
+    for (void* h : {(void*)sl.h_in, (void*)sl.h_desc, (void*)sl.h_out, (void*)sl.h_mout, (void*)sl.h_err})
+        if (h) cudaFreeHost(h);
+    for (auto& e : sl.ev)
+        if (e) cudaEventDestroy(e);
+    if (sl.done) cudaEventDestroy(sl.done);
+    if (sl.stream) cudaStreamDestroy(sl.stream);
 }
 
 }  // namespace
+
+// ================================================================ serving
+
+namespace {
+
+struct Request {
+    uint64_t id = 0;
+    std::vector<uint8_t> in;
+    size_t units = 0, units_done = 0;
+    std::vector<std::vector<uint8_t>> pieces;  // gzip members of each unit
+    double t_arrive = 0, t_done = 0;
+    int status = GPZ_OK;
+    bool done = false;
+    bool small = false;
+};
+
+struct Unit {
+    std::shared_ptr<Request> req;
+    size_t index = 0, off = 0, n = 0;
+};
+
+}  // namespace
+
+// Continuous batching: requests are cut into 2 MiB units (whole members);
+// whenever a pipeline slot is free, the engine forms a batch from the waiting
+// units -- those of requests of at most 1 MiB first, then the rest in arrival
+// order, up to the batch cap -- and launches it while the other slot's batch
+// is still on the device.  A request completes when its last unit does, and
+// its gzip stream is its units' members in order, byte for byte what
+// gpz_compress_chunk returns for it alone.  Admission: a request is rejected
+// (GPZ_E_BUSY) while the bytes queued or on the device would exceed the pool
+// cap.
+struct ServeEngine {
+    gpz_ctx* c = nullptr;
+    Slot slots[2];
+    std::thread th;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<Unit> small_q, large_q;
+    std::unordered_map<uint64_t, std::shared_ptr<Request>> reqs;
+    uint64_t next_id = 1;
+    bool stop = false;
+    size_t queued_bytes = 0;
+    size_t batch_cap = 16u << 20;
+    std::vector<double> lat_all, lat_small;
+    uint64_t rejected = 0, batches = 0, bytes_in = 0, bytes_out = 0;
+    double max_queue_ms = 0;
+    std::vector<Unit> inflight[2];
+
+    static constexpr size_t kUnit = 2u << 20;
+    static constexpr size_t kSmall = 1u << 20;
+
+    int start(gpz_ctx* ctx) {
+        c = ctx;
+        cudaSetDevice(c->device);
+        for (auto& s : slots) {
+            int rc = init_slot(c, s);
+            if (rc) return rc;
+        }
+        th = std::thread([this] { loop(); });
+        return GPZ_OK;
+    }
+
+    void shutdown() {
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            stop = true;
+        }
+        cv_work.notify_all();
+        if (th.joinable()) th.join();
+        for (auto& s : slots) free_slot(c, s);
+    }
+
+    int submit(const gpz_desc* d, uint64_t* ticket) {
+        auto r = std::make_shared<Request>();
+        r->t_arrive = now_ms();
+        r->small = d->n <= kSmall;
+        r->units = d->n == 0 ? 1 : (d->n + kUnit - 1) / kUnit;
+        r->pieces.resize(r->units);
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            if (queued_bytes + d->n > c->pool_cap) {
+                rejected++;
+                return GPZ_E_BUSY;
+            }
+            queued_bytes += d->n;
+        }
+        r->in.assign(d->in, d->in + d->n);
+        std::lock_guard<std::mutex> lk(mu);
+        r->id = next_id++;
+        for (size_t u = 0; u < r->units; u++) {
+            Unit un{r, u, u * kUnit, std::min(kUnit, d->n - std::min(d->n, u * kUnit))};
+            (r->small ? small_q : large_q).push_back(un);
+        }
+        reqs[r->id] = r;
+        *ticket = r->id;
+        cv_work.notify_one();
+        return GPZ_OK;
+    }
+
+    int poll(uint64_t ticket, gpz_out* o, int wait_ms) {
+        std::unique_lock<std::mutex> lk(mu);
+        auto it = reqs.find(ticket);
+        if (it == reqs.end()) return GPZ_E_ARG;
+        auto r = it->second;
+        if (!r->done && wait_ms > 0)
+            cv_done.wait_for(lk, std::chrono::milliseconds(wait_ms), [&] { return r->done; });
+        if (!r->done) return GPZ_E_PENDING;
+        size_t total = 0;
+        for (auto& p : r->pieces) total += p.size();
+        o->out_len = total;
+        if (r->status != GPZ_OK) {
+            o->status = r->status;
+            reqs.erase(it);
+            return o->status;
+        }
+        if (!o->out || o->out_cap < total) {
+            o->status = GPZ_E_SPACE;
+            return GPZ_E_SPACE;  // the result stays available for a larger buffer
+        }
+        size_t k = 0;
+        for (auto& p : r->pieces) {
+            std::memcpy(o->out + k, p.data(), p.size());
+            k += p.size();
+        }
+        o->status = GPZ_OK;
+        reqs.erase(it);
+        return GPZ_OK;
+    }
+
+    // The next batch of units, small requests first (caller holds mu).
+    std::vector<Unit> take_batch() {
+        std::vector<Unit> b;
+        size_t bytes = 0;
+        for (auto* q : {&small_q, &large_q}) {
+            while (!q->empty() && (b.empty() || bytes + q->front().n <= batch_cap)) {
+                bytes += q->front().n;
+                b.push_back(q->front());
+                q->pop_front();
+            }
+        }
+        return b;
+    }
+
+    void complete(int k, int rc) {
+        Slot& sl = slots[k];
+        std::vector<Unit>& units = inflight[k];
+        const double t = now_ms();
+        std::vector<std::vector<uint8_t>> outs(units.size());
+        if (rc == GPZ_OK) {
+            frame_members(sl.h_mout, 0, sl.members.size(), sl.h_out, 0);
+            for (size_t i = 0; i < units.size(); i++) {
+                const Span& sp = sl.spans[i];
+                const MemberOut& a = sl.h_mout[sp.first_member];
+                const MemberOut& z = sl.h_mout[sp.first_member + sp.nmembers - 1];
+                outs[i].assign(sl.h_out + a.gz_off, sl.h_out + z.gz_off + 18 + z.deflate_bytes);
+            }
+        }
+        std::lock_guard<std::mutex> lk(mu);
+        for (size_t i = 0; i < units.size(); i++) {
+            auto& r = units[i].req;
+            queued_bytes -= units[i].n;
+            if (rc != GPZ_OK) r->status = rc;
+            else {
+                bytes_out += outs[i].size();
+                r->pieces[units[i].index] = std::move(outs[i]);
+            }
+            if (++r->units_done == r->units) {
+                r->done = true;
+                r->t_done = t;
+                const double lat = t - r->t_arrive;
+                lat_all.push_back(lat);
+                if (r->small) lat_small.push_back(lat);
+                bytes_in += r->in.size();
+                std::vector<uint8_t>().swap(r->in);
+            }
+        }
+        units.clear();
+        cv_done.notify_all();
+    }
+
+    void loop() {
+        cudaSetDevice(c->device);
+        int turn = 0;
+        for (;;) {
+            std::vector<Unit> batch;
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                if (!slots[0].busy && !slots[1].busy)
+                    cv_work.wait(lk, [&] { return stop || !small_q.empty() || !large_q.empty(); });
+                if (stop && small_q.empty() && large_q.empty() && !slots[0].busy && !slots[1].busy) return;
+                if (!slots[turn].busy) batch = take_batch();
+                if (!batch.empty()) max_queue_ms = std::max(max_queue_ms, now_ms() - batch.front().req->t_arrive);
+            }
+            if (!batch.empty()) {
+                Slot& sl = slots[turn];
+                std::vector<gpz_desc> ds(batch.size());
+                for (size_t i = 0; i < batch.size(); i++)
+                    ds[i] = gpz_desc{batch[i].req->in.data() + batch[i].off, batch[i].n, 0};
+                inflight[turn] = std::move(batch);
+                const int rc = submit_slot(c, sl, ds.data(), ds.size(), false);
+                if (rc) {
+                    sl.busy = false;
+                    complete(turn, rc);
+                } else {
+                    std::lock_guard<std::mutex> lk(mu);
+                    batches++;
+                }
+                turn ^= 1;
+                continue;
+            }
+            // nothing new to launch on this slot: retire the oldest batch
+            const int k = slots[turn].busy ? turn : (turn ^ 1);
+            if (slots[k].busy) {
+                const int rc = wait_slot(c, slots[k]);
+                complete(k, rc);
+                turn = k;
+            }
+        }
+    }
+
+    static double pct(std::vector<double> v, double q) {
+        if (v.empty()) return 0;
+        std::sort(v.begin(), v.end());
+        const size_t i = (size_t)std::min<double>((double)(v.size() - 1), q * (double)(v.size() - 1) + 0.5);
+        return v[i];
+    }
+};
 
 // ====================================================================== ABI
 
@@ -382,7 +851,7 @@ int gpz_create(const gpz_config* cfg, gpz_ctx** out) {
     gpz_config def;
     gpz_config_default(&def);
     if (!cfg) cfg = &def;
-    size_t mb = cfg->member_bytes ? cfg->member_bytes : kDefaultMember;
+    const size_t mb = cfg->member_bytes ? cfg->member_bytes : kDefaultMember;
     if (mb % GPZ_SEG != 0 || mb > kMaxMember) return GPZ_E_ARG;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
@@ -397,19 +866,18 @@ int gpz_create(const gpz_config* cfg, gpz_ctx** out) {
     c->pool_cap = cfg->pool_bytes ? cfg->pool_bytes : kDefaultPool;
     c->batch_bytes = cfg->batch_bytes ? cfg->batch_bytes : kDefaultBatch;
     c->flags = cfg->flags;
-    if (cudaSetDevice(c->device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        gpz_kernel_smem_setup() != 0 || cudaMallocHost(reinterpret_cast<void**>(&c->h_err), 64) != cudaSuccess) {
+    if (cudaSetDevice(c->device) != cudaSuccess || gpz_kernel_smem_setup() != 0) {
         cudaGetLastError();
-        gpz_destroy(c);
+        delete c;
         return GPZ_E_CUDA;
     }
-    if (c->flags & GPZ_FLAG_STAGE_TIMING)
-        for (auto& e : c->ev)
-            if (cudaEventCreate(&e) != cudaSuccess) {
-                cudaGetLastError();
-                gpz_destroy(c);
-                return GPZ_E_CUDA;
-            }
+    cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->device);
+    default_shapes(c);
+    for (auto& s : c->slots)
+        if (init_slot(c, s) != GPZ_OK) {
+            gpz_destroy(c);
+            return GPZ_E_CUDA;
+        }
     *out = c;
     return GPZ_OK;
 }
@@ -417,32 +885,22 @@ int gpz_create(const gpz_config* cfg, gpz_ctx** out) {
 void gpz_destroy(gpz_ctx* c) {
     if (!c) return;
     cudaSetDevice(c->device);
-    if (c->stream) cudaStreamSynchronize(c->stream);
-    for (DevArena* a : {&c->d_in, &c->d_pp, &c->d_tok, &c->d_out, &c->d_skeys, &c->d_son, &c->d_sposid,
-                        &c->d_snkeys, &c->d_tentry, &c->d_texit, &c->d_thist,
-                        &c->d_tntok, &c->d_tbit, &c->d_mcodes, &c->d_mhdr, &c->d_mout, &c->d_cnt, &c->d_members,
-                        &c->d_tiles})
-        if (a->p) cudaFree(a->p);
-    if (c->h_in) cudaFreeHost(c->h_in);
-    if (c->h_out) cudaFreeHost(c->h_out);
-    if (c->h_members) cudaFreeHost(c->h_members);
-    if (c->h_tiles) cudaFreeHost(c->h_tiles);
-    if (c->h_mout) cudaFreeHost(c->h_mout);
-    if (c->h_err) cudaFreeHost(c->h_err);
-    for (auto& e : c->ev)
-        if (e) cudaEventDestroy(e);
-    if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->serve) {
+        c->serve->shutdown();
+        c->serve.reset();
+    }
+    for (auto& s : c->slots) free_slot(c, s);
     delete c;
 }
 
 size_t gpz_bound(size_t n) {
-    size_t nm = n == 0 ? 1 : (n + kDefaultMember - 1) / kDefaultMember;
+    const size_t nm = n == 0 ? 1 : (n + kDefaultMember - 1) / kDefaultMember;
     return nm * member_bound(kDefaultMember);
 }
 
 size_t gpz_bound_ctx(const gpz_ctx* c, size_t n) {
     if (!c) return gpz_bound(n);
-    size_t nm = n == 0 ? 1 : (n + c->member_bytes - 1) / c->member_bytes;
+    const size_t nm = n == 0 ? 1 : (n + c->member_bytes - 1) / c->member_bytes;
     return nm * member_bound(c->member_bytes);
 }
 
@@ -453,9 +911,9 @@ int gpz_compress_chunk(gpz_ctx* c, const uint8_t* in, size_t n, int level, uint8
     cudaSetDevice(c->device);
     gpz_desc d{in, n, level};
     gpz_out o{out, out_cap, 0, 0};
-    int rc = run_host_batch(c, &d, 1, &o);
+    const int rc = run_host_items(c, &d, 1, &o, false);
     *out_len = o.out_len;
-    return rc;
+    return rc != GPZ_OK ? rc : o.status;
 }
 
 int gpz_compress_batch(gpz_ctx* c, const gpz_desc* d, size_t count, gpz_out* outs) {
@@ -481,30 +939,45 @@ int gpz_compress_device(gpz_ctx* c, const void* d_in, const uint64_t* in_off, co
     if (!c || !d_in || !d_out || !in_off || !in_len || !out_off || !count) return GPZ_E_ARG;
     std::lock_guard<std::mutex> lk(c->mu);
     cudaSetDevice(c->device);
-    std::vector<Span> spans(count);
+    Slot& sl = c->slots[0];
+    sl.spans.assign(count, Span{});
     size_t in_end = 0;
     for (size_t i = 0; i < count; i++) {
         if (in_off[i] % 16) return fail(c, GPZ_E_ARG, "device inputs must start 16-byte aligned");
-        spans[i].n = in_len[i];
-        spans[i].dev_off = in_off[i];
+        sl.spans[i].n = in_len[i];
+        sl.spans[i].dev_off = in_off[i];
         in_end = std::max<size_t>(in_end, in_off[i] + round_up(std::max<uint64_t>(in_len[i], 1), 16));
     }
-    plan(c, spans);
-    if (out_bound_of_plan(c) > out_cap) return fail(c, GPZ_E_SPACE, "device output buffer below bound");
+    plan(c, sl);
+    if (out_bound_of_plan(sl) > out_cap) return fail(c, GPZ_E_SPACE, "device output buffer below bound");
     int rc;
-    if ((rc = reserve(c, in_end, false, false, 0))) return rc;
-    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : c->stream;
-    if ((rc = run_device(c, static_cast<const uint8_t*>(d_in), static_cast<uint8_t*>(d_out), s))) return rc;
-    for (size_t i = 0; i < count; i++) out_off[i] = c->mout[spans[i].first_member].gz_off;
-    out_off[count] = batch_out_bytes(c);
+    if ((rc = reserve(c, sl, in_end, false, false, 0))) return rc;
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : sl.stream;
+    if ((rc = upload_desc(c, sl, s))) return rc;
+    BatchParams bp = params_of(sl, static_cast<const uint8_t*>(d_in), static_cast<uint8_t*>(d_out));
+    sl.bucket = bucket_of(sl.tiles.size());
+    const bool timing = (c->flags & GPZ_FLAG_STAGE_TIMING) != 0;
+    if ((rc = launch(c, sl, bp, shape_for(c, sl.bucket), false, nullptr, timing, s))) return rc;
+    CU(c, cudaMemcpyAsync(sl.h_mout, sl.d_mout.p, sl.members.size() * sizeof(MemberOut), cudaMemcpyDeviceToHost, s));
+    CU(c, cudaMemcpyAsync(sl.h_err, static_cast<uint32_t*>(sl.d_cnt.p) + GPZ_NCOUNTERS, 4, cudaMemcpyDeviceToHost, s));
+    CU(c, cudaStreamSynchronize(s));
+    if (timing)
+        for (int i = 0; i < 4; i++) cudaEventElapsedTime(&c->stage_ms[i], sl.ev[i], sl.ev[i + 1]);
+    c->mout.assign(sl.h_mout, sl.h_mout + sl.members.size());
+    if (*sl.h_err) return fail(c, (*sl.h_err & GPZ_ERRBIT_SPIN) ? GPZ_E_TIMEOUT : GPZ_E_INTERNAL, "device self-check");
+    for (size_t i = 0; i < count; i++) out_off[i] = c->mout[sl.spans[i].first_member].gz_off;
+    const MemberOut& l = c->mout.back();
+    out_off[count] = l.gz_off + 18 + l.deflate_bytes;
     return GPZ_OK;
 }
 
 int gpz_frame_host(gpz_ctx* c, uint8_t* host_out, size_t cap) {
     if (!c || !host_out) return GPZ_E_ARG;
     std::lock_guard<std::mutex> lk(c->mu);
-    if (batch_out_bytes(c) > cap) return GPZ_E_SPACE;
-    frame_members(c, 0, c->mout.size(), host_out, 0);
+    if (c->mout.empty()) return GPZ_E_ARG;
+    const MemberOut& l = c->mout.back();
+    if (l.gz_off + 18 + l.deflate_bytes > cap) return GPZ_E_SPACE;
+    frame_members(c->mout.data(), 0, c->mout.size(), host_out, 0);
     return GPZ_OK;
 }
 
@@ -521,9 +994,79 @@ int gpz_debug_chunk(gpz_ctx* c, const uint8_t* in, size_t n, uint32_t* pp, uint3
         o.out = tmp.data();
         o.out_cap = tmp.size();
     }
-    int rc = run_host_batch(c, &d, 1, &o, pp, tokens, ntok);
+    const int rc = run_host_items(c, &d, 1, &o, true);
     if (out_len) *out_len = o.out_len;
-    return rc;
+    if (rc) return rc;
+    Slot& sl = c->slots[0];
+    if (pp && n) CU(c, cudaMemcpy(pp, sl.d_pp.p, n * 4, cudaMemcpyDeviceToHost));
+    if (tokens && ntok) {
+        std::vector<uint32_t> tok_all(std::max<size_t>(n, 1)), tntok(std::max<size_t>(sl.tiles.size(), 1));
+        if (n) CU(c, cudaMemcpy(tok_all.data(), sl.d_tok.p, n * 4, cudaMemcpyDeviceToHost));
+        if (!sl.tiles.empty())
+            CU(c, cudaMemcpy(tntok.data(), sl.d_tntok.p, sl.tiles.size() * 4, cudaMemcpyDeviceToHost));
+        size_t k = 0;
+        for (size_t t = 0; t < sl.tiles.size(); t++) {
+            const TileDesc& td = sl.tiles[t];
+            const MemberDesc& md = sl.members[td.member];
+            std::memcpy(tokens + k, tok_all.data() + md.in_off + ((size_t)td.seg << GPZ_SEG_LOG2), tntok[t] * 4);
+            k += tntok[t];
+        }
+        *ntok = k;
+    }
+    return o.status;
+}
+
+int gpz_submit(gpz_ctx* c, const gpz_desc* d, uint64_t* ticket) {
+    if (!c || !d || !ticket || (!d->in && d->n)) return GPZ_E_ARG;
+    {
+        std::lock_guard<std::mutex> lk(c->serve_mu);
+        if (!c->serve) {
+            auto e = std::make_unique<ServeEngine>();
+            const int rc = e->start(c);
+            if (rc) return rc;
+            c->serve = std::move(e);
+        }
+    }
+    return c->serve->submit(d, ticket);
+}
+
+int gpz_poll(gpz_ctx* c, uint64_t ticket, gpz_out* o, int wait_ms) {
+    if (!c || !o || !c->serve) return GPZ_E_ARG;
+    return c->serve->poll(ticket, o, wait_ms);
+}
+
+int gpz_serve_stats_get(gpz_ctx* c, gpz_serve_stats* st) {
+    if (!c || !st) return GPZ_E_ARG;
+    std::memset(st, 0, sizeof *st);
+    if (!c->serve) return GPZ_OK;
+    ServeEngine& e = *c->serve;
+    std::lock_guard<std::mutex> lk(e.mu);
+    st->completed = e.lat_all.size();
+    st->rejected = e.rejected;
+    st->batches = e.batches;
+    st->p50_ms = ServeEngine::pct(e.lat_all, 0.50);
+    st->p99_ms = ServeEngine::pct(e.lat_all, 0.99);
+    st->p999_ms = ServeEngine::pct(e.lat_all, 0.999);
+    st->max_queue_ms = e.max_queue_ms;
+    st->bytes_in = e.bytes_in;
+    st->bytes_out = e.bytes_out;
+    st->completed_small = e.lat_small.size();
+    st->p50_small_ms = ServeEngine::pct(e.lat_small, 0.50);
+    st->p99_small_ms = ServeEngine::pct(e.lat_small, 0.99);
+    st->p999_small_ms = ServeEngine::pct(e.lat_small, 0.999);
+    st->queued_bytes = e.queued_bytes;
+    return GPZ_OK;
+}
+
+int gpz_serve_reset_stats(gpz_ctx* c) {
+    if (!c) return GPZ_E_ARG;
+    if (!c->serve) return GPZ_OK;
+    std::lock_guard<std::mutex> lk(c->serve->mu);
+    c->serve->lat_all.clear();
+    c->serve->lat_small.clear();
+    c->serve->rejected = c->serve->batches = c->serve->bytes_in = c->serve->bytes_out = 0;
+    c->serve->max_queue_ms = 0;
+    return GPZ_OK;
 }
 
 const char* gpz_strerror(int s) {
@@ -546,28 +1089,30 @@ const char* gpz_last_error(gpz_ctx* c) { return c ? c->last_err.c_str() : "no co
 
 int gpz_get_shape(gpz_ctx* c, gpz_shape* s) {
     if (!c || !s) return GPZ_E_ARG;
-    s->lookup_threads = c->shape.lookup_threads;
-    s->lookup_grid = c->shape.lookup_grid;
-    s->walk_threads = c->shape.walk_threads;
-    s->walk_grid = c->shape.walk_grid;
-    s->emit_threads = c->shape.emit_threads;
-    s->emit_grid = c->shape.emit_grid;
+    const LaunchShape x = shape_for(c, bucket_of(64 * 1024));
+    s->lookup_threads = x.lookup_threads;
+    s->lookup_grid = x.lookup_grid;
+    s->walk_threads = x.walk_threads;
+    s->walk_grid = x.walk_grid;
+    s->emit_threads = x.emit_threads;
+    s->emit_grid = x.emit_grid;
     return GPZ_OK;
 }
 
 int gpz_set_shape(gpz_ctx* c, const gpz_shape* s) {
     if (!c || !s) return GPZ_E_ARG;
     auto ok_t = [](int t) { return t == 256 || t == 512; };
-    if (!(s->lookup_threads == 512 || s->lookup_threads == 1024) || !ok_t(s->walk_threads) || !ok_t(s->emit_threads) ||
-        s->lookup_grid < 0 || s->walk_grid < 0 || s->emit_grid < 0)
+    if (!(s->lookup_threads == 512 || s->lookup_threads == 1024) || !ok_t(s->walk_threads) ||
+        !ok_t(s->emit_threads) || s->lookup_grid < 0 || s->walk_grid < 0 || s->emit_grid < 0)
         return GPZ_E_ARG;
     std::lock_guard<std::mutex> lk(c->mu);
-    c->shape = LaunchShape{s->lookup_threads, s->lookup_grid, s->walk_threads, s->walk_grid, s->emit_threads,
-                           s->emit_grid};
+    c->fixed = LaunchShape{s->lookup_threads, s->lookup_grid, s->walk_threads, s->walk_grid, s->emit_threads,
+                           s->emit_grid, 0, 0};
+    for (auto& sl : c->slots) sl.gen++;
     return GPZ_OK;
 }
 
-uint64_t gpz_last_launches(gpz_ctx* c) { return c ? c->launches : 0; }
+uint64_t gpz_last_launches(gpz_ctx* c) { return c ? c->launches.load() : 0; }
 
 int gpz_stage_times(gpz_ctx* c, float* ms4) {
     if (!c || !ms4 || !(c->flags & GPZ_FLAG_STAGE_TIMING)) return GPZ_E_ARG;
@@ -575,9 +1120,5 @@ int gpz_stage_times(gpz_ctx* c, float* ms4) {
     for (int i = 0; i < 4; i++) ms4[i] = c->stage_ms[i];
     return GPZ_OK;
 }
-
-int gpz_submit(gpz_ctx*, const gpz_desc*, uint64_t*) { return GPZ_E_ARG; }
-int gpz_poll(gpz_ctx*, uint64_t, gpz_out*, int) { return GPZ_E_ARG; }
-int gpz_serve_stats_get(gpz_ctx*, gpz_serve_stats*) { return GPZ_E_ARG; }
 
 }  // extern "C"

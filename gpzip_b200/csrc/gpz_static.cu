@@ -54,7 +54,8 @@ constexpr size_t kMout = kMhdr + al(GPZ_HDR_WORDS * 4);
 constexpr size_t kCnt = kMout + al(sizeof(MemberOut));
 constexpr size_t kMembers = kCnt + al(GPZ_NCOUNTERS * 4 + 64);
 constexpr size_t kTilesOff = kMembers + al(sizeof(MemberDesc));
-constexpr size_t kResult = kTilesOff + al(kTiles * sizeof(TileDesc));
+constexpr size_t kDims = kTilesOff + al(kTiles * sizeof(TileDesc));
+constexpr size_t kResult = kDims + al(64);
 constexpr size_t kTotal = kResult + al(16);
 
 }  // namespace
@@ -72,7 +73,12 @@ __global__ void k_static_setup(uint8_t* base, uint32_t n) {
     uint32_t* cnt = reinterpret_cast<uint32_t*>(base + kCnt);
     MemberDesc* md = reinterpret_cast<MemberDesc*>(base + kMembers);
     TileDesc* td = reinterpret_cast<TileDesc*>(base + kTilesOff);
+    uint32_t* dims = reinterpret_cast<uint32_t*>(base + kDims);
     const uint32_t nt = (n + GPZ_SEG - 1) / GPZ_SEG;
+    if (threadIdx.x == 0) {
+        dims[0] = nt;
+        dims[1] = 1u;
+    }
     for (uint32_t i = threadIdx.x; i < GPZ_NCOUNTERS + 16; i += blockDim.x) cnt[i] = 0u;
     for (uint32_t i = threadIdx.x; i < kTiles; i += blockDim.x) td[i] = TileDesc{0u, i};
     if (threadIdx.x == 0) {
@@ -178,11 +184,12 @@ extern "C" int gpz_compress_member_static(const uint8_t* d_in, size_t n, uint8_t
     bp.member_hdr = reinterpret_cast<uint32_t*>(base + kMhdr);
     bp.counters = reinterpret_cast<uint32_t*>(base + kCnt);
     bp.err = bp.counters + GPZ_NCOUNTERS;
+    bp.dims = reinterpret_cast<const uint32_t*>(base + kDims);
     bp.nmembers = 1;
     bp.ntiles = (uint32_t)((n + GPZ_SEG - 1) / GPZ_SEG);
     bp.out_base = 0;
-    const LaunchShape shape{1024, 0, 512, 0, 512, 0};
-    if (gpz_launch_batch(bp, shape, s, nullptr) != 0) return GPZ_E_CUDA;
+    const LaunchShape shape{1024, 0, 512, 0, 512, 0, 0, 0};
+    if (gpz_launch_batch(bp, shape, s, nullptr, nullptr) != 0) return GPZ_E_CUDA;
     k_static_finish<<<8, 256, 0, s>>>(base, d_out, out_cap);
 
     unsigned long long result[2] = {0, 0};

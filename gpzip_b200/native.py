@@ -28,6 +28,7 @@ EXPORTS = [
     "gpz_compress_batch", "gpz_compress_batch_plain", "gpz_compress_device", "gpz_frame_host",
     "gpz_debug_chunk", "gpz_submit", "gpz_poll", "gpz_serve_stats_get", "gpz_strerror", "gpz_last_error",
     "gpz_get_shape", "gpz_set_shape", "gpz_last_launches", "gpz_stage_times", "gpz_compress_member_static",
+    "gpz_serve_reset_stats",
 ]
 
 
@@ -59,7 +60,10 @@ class Shape(ctypes.Structure):
 class ServeStats(ctypes.Structure):
     _fields_ = [("completed", ctypes.c_uint64), ("rejected", ctypes.c_uint64), ("batches", ctypes.c_uint64),
                 ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double), ("p999_ms", ctypes.c_double),
-                ("max_queue_ms", ctypes.c_double), ("bytes_in", ctypes.c_uint64), ("bytes_out", ctypes.c_uint64)]
+                ("max_queue_ms", ctypes.c_double), ("bytes_in", ctypes.c_uint64), ("bytes_out", ctypes.c_uint64),
+                ("completed_small", ctypes.c_uint64), ("p50_small_ms", ctypes.c_double),
+                ("p99_small_ms", ctypes.c_double), ("p999_small_ms", ctypes.c_double),
+                ("queued_bytes", ctypes.c_uint64)]
 
 
 _lib = None
@@ -102,6 +106,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.gpz_poll.restype = ctypes.c_int
     L.gpz_serve_stats_get.argtypes = [vp, ctypes.POINTER(ServeStats)]
     L.gpz_serve_stats_get.restype = ctypes.c_int
+    L.gpz_serve_reset_stats.argtypes = [vp]
+    L.gpz_serve_reset_stats.restype = ctypes.c_int
     L.gpz_strerror.argtypes = [ctypes.c_int]
     L.gpz_strerror.restype = ctypes.c_char_p
     L.gpz_last_error.argtypes = [vp]
@@ -257,13 +263,21 @@ class Context:
         return t.value
 
     def poll(self, ticket: int, cap: int, wait_ms: int = 0):
-        buf = np.empty(cap, dtype=np.uint8)
+        """The gzip stream of a submitted request, or None while pending."""
+        buf = np.empty(max(cap, 1), dtype=np.uint8)
         o = Out(buf.ctypes.data, cap, 0, 0)
         rc = self.L.gpz_poll(self._h, ticket, ctypes.byref(o), wait_ms)
         if rc == GPZ_E_PENDING:
             return None
+        if rc == 6:  # GPZ_E_SPACE: the result is kept; retry with the size needed
+            buf = np.empty(o.out_len, dtype=np.uint8)
+            o = Out(buf.ctypes.data, o.out_len, 0, 0)
+            rc = self.L.gpz_poll(self._h, ticket, ctypes.byref(o), wait_ms)
         self._check(rc, "gpz_poll")
         return buf[:o.out_len].tobytes()
+
+    def serve_reset_stats(self):
+        self._check(self.L.gpz_serve_reset_stats(self._h), "gpz_serve_reset_stats")
 
     def serve_stats(self) -> dict:
         s = ServeStats()

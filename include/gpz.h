@@ -127,13 +127,20 @@ GPZ_API int gpz_frame_host(gpz_ctx* ctx, uint8_t* host_out, size_t cap);
 GPZ_API int gpz_debug_chunk(gpz_ctx* ctx, const uint8_t* in, size_t n, uint32_t* pp, uint32_t* tokens,
                     size_t* ntok, uint8_t* out, size_t out_cap, size_t* out_len);
 
-/* Serving: submit a request (the input is copied before return), poll for
- * its result.  gpz_poll returns GPZ_E_PENDING until the gzip stream is ready;
- * wait_ms > 0 blocks up to that long.  The result is copied into o->out. */
+/* Serving (continuous batching): submit a request -- one gzip stream, the
+ * input is copied before return -- and poll for its result.  Requests that
+ * arrive while others are on the device join the next batch as soon as a
+ * pipeline slot frees; requests of at most 1 MiB go first.  A request whose
+ * bytes would push the queued and in-flight total past the pool cap is
+ * rejected with GPZ_E_BUSY.  gpz_poll returns GPZ_E_PENDING until the stream
+ * is ready (wait_ms > 0 blocks up to that long), GPZ_E_SPACE (result kept)
+ * if o->out_cap is short; the result is copied into o->out. */
 GPZ_API int gpz_submit(gpz_ctx* ctx, const gpz_desc* d, uint64_t* ticket);
 GPZ_API int gpz_poll(gpz_ctx* ctx, uint64_t ticket, gpz_out* o, int wait_ms);
 
-/* Serving statistics since the context started (latencies in ms). */
+/* Serving statistics since the engine started or was last reset (latencies
+ * in ms, arrival at gpz_submit to result ready; "small" = requests of at most
+ * 1 MiB). */
 typedef struct gpz_serve_stats {
     uint64_t completed;
     uint64_t rejected;
@@ -141,8 +148,12 @@ typedef struct gpz_serve_stats {
     double p50_ms, p99_ms, p999_ms;
     double max_queue_ms;
     uint64_t bytes_in, bytes_out;
+    uint64_t completed_small;
+    double p50_small_ms, p99_small_ms, p999_small_ms;
+    uint64_t queued_bytes;
 } gpz_serve_stats;
 GPZ_API int gpz_serve_stats_get(gpz_ctx* ctx, gpz_serve_stats* st);
+GPZ_API int gpz_serve_reset_stats(gpz_ctx* ctx);
 
 GPZ_API const char* gpz_strerror(int status);
 

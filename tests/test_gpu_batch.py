@@ -1,0 +1,140 @@
+"""Batched, plain, device-resident and serving paths against each other and the oracle (GPU).
+
+All comparisons are byte-exact: the path is integer work end to end.
+"""
+import ctypes
+import threading
+import zlib
+
+import numpy as np
+import pytest
+
+from gpzip_b200 import native
+from gpzip_b200 import workloads as W
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def uneven_items(count=24, seed=5):
+    rng = np.random.default_rng(seed)
+    items = []
+    for i in range(count):
+        n = int(np.exp(rng.uniform(np.log(1), np.log(3 << 20))))
+        kind = ["text", "logs", "binary"][i % 3]
+        items.append(W.GENERATORS[kind](n, seed=100 + i).tobytes())
+    items[3] = b""
+    items[7] = b"x"
+    return items
+
+
+def test_batch_plain_oracle_uneven(ctx):
+    items = uneven_items()
+    got = ctx.compress_batch(items)
+    plain = ctx.compress_batch_plain(items)
+    for it, g, p in zip(items, got, plain):
+        assert g == p
+        assert g == O.gzip_chunk(it, 131072, threads=8)
+
+
+def test_graph_reuse_across_batch_sizes(ctx):
+    # same size bucket, different member/tile counts: the captured graph reads
+    # the batch dimensions from device memory
+    a = [W.text(300_000, seed=1).tobytes(), W.logs(200_000, seed=2).tobytes()]
+    b = [W.binary(150_001, seed=3).tobytes()]
+    c = [W.text(40_000, seed=4).tobytes()] * 5
+    for items in (a, b, c, a):
+        for it, g in zip(items, ctx.compress_batch(items)):
+            assert g == O.gzip_chunk(it, 131072)
+
+
+def test_every_launch_shape_gives_the_same_bytes(ctx):
+    data = W.logs(700_000, seed=9).tobytes()
+    want = O.gzip_chunk(data, 131072)
+    keep = ctx.get_shape()
+    for lt in (1024, 512):
+        for wt in (512, 256):
+            for et in (512, 256):
+                ctx.set_shape(native.Shape(lt, 0, wt, 0, et, 0))
+                assert ctx.compress_chunk(data) == want, (lt, wt, et)
+    ctx.set_shape(keep)
+
+
+def test_device_api_matches_host_api(ctx):
+    import torch
+    items = [W.text(500_000, seed=11).tobytes(), W.binary(123_457, seed=12).tobytes(), b"", b"ab"]
+    offs, lens, pos = [], [], 0
+    for it in items:
+        offs.append(pos)
+        lens.append(len(it))
+        pos += (max(len(it), 1) + 15) // 16 * 16
+    packed = np.zeros(pos + 64, dtype=np.uint8)
+    for it, o in zip(items, offs):
+        packed[o:o + len(it)] = np.frombuffer(it, dtype=np.uint8)
+    d_in = torch.from_numpy(packed).cuda()
+    cap = sum(ctx.bound(len(it)) for it in items) + 1024
+    d_out = torch.zeros(cap, dtype=torch.uint8, device="cuda")
+    oo = ctx.compress_device(d_in.data_ptr(), offs, lens, d_out.data_ptr(), cap)
+    host = d_out[:oo[-1]].cpu().numpy().copy()
+    ctx.frame_host(host)
+    want = ctx.compress_batch(items)
+    for i, w in enumerate(want):
+        assert host[oo[i]:oo[i + 1]].tobytes() == w
+
+
+def test_short_output_buffer_is_reported(ctx):
+    L = native.load()
+    data = np.frombuffer(W.text(10_000, seed=3).tobytes(), dtype=np.uint8)
+    out = np.zeros(16, dtype=np.uint8)
+    n = ctypes.c_size_t()
+    rc = L.gpz_compress_chunk(ctx._h, data.ctypes.data, data.size, 5, out.ctypes.data, out.size, ctypes.byref(n))
+    assert rc == 6 and n.value > 16  # GPZ_E_SPACE, with the needed size
+    assert ctx.compress_chunk(data) == O.gzip_chunk(data.tobytes(), 131072)  # context still usable
+
+
+def test_whole_chunk_member_mode():
+    data = W.logs(3 << 20, seed=21).tobytes()
+    with native.Context(member_bytes=2 << 20) as c2:
+        got = c2.compress_chunk(data)
+    assert got == O.gzip_chunk(data, 2 << 20)
+    assert zlib.decompress(got[:len(got)], 31) is not None
+
+
+def test_serving_alone_equals_mix(ctx):
+    rng = np.random.default_rng(4)
+    reqs = []
+    for i in range(40):
+        n = int(np.exp(rng.uniform(np.log(4096), np.log(6 << 20))))
+        reqs.append(W.GENERATORS[["text", "logs", "binary"][i % 3]](n, seed=300 + i).tobytes())
+    tickets = [None] * len(reqs)
+
+    def submitter(lo, hi):
+        for i in range(lo, hi):
+            tickets[i] = ctx.submit(reqs[i])
+
+    ths = [threading.Thread(target=submitter, args=(k * 10, (k + 1) * 10)) for k in range(4)]
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join()
+    mixed = [ctx.poll(t, ctx.bound(len(r)), wait_ms=60_000) for t, r in zip(tickets, reqs)]
+    for r, m in zip(reqs, mixed):
+        assert m is not None
+        assert m == ctx.compress_chunk(r)  # alone, same bytes
+    st = ctx.serve_stats()
+    assert st["completed"] >= len(reqs) and st["batches"] >= 1
+
+
+def test_serving_pending_space_and_admission():
+    with native.Context(pool_bytes=64 << 20) as c:
+        data = W.text(3 << 20, seed=8).tobytes()
+        t = c.submit(data)
+        r = c.poll(t, 16, wait_ms=60_000)  # too small at first: the result is kept, then fetched whole
+        assert r == O.gzip_chunk(data, 131072)
+    # a fresh context with a tiny cap rejects what it cannot queue
+    with native.Context(pool_bytes=1 << 20) as c:
+        with pytest.raises(native.GpzError) as e:
+            c.submit(b"z" * (2 << 20))
+        assert e.value.status == native.GPZ_E_BUSY
+        st = c.serve_stats()
+        assert st["rejected"] == 1
