@@ -51,7 +51,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="logs", choices=["logs", "text", "binary"])
+    ap.add_argument("--workload", default="logs", choices=["logs", "text", "binary", "uneven"])
+    ap.add_argument("--serve-seconds", type=float, default=1.5,
+                    help="seconds per arrival rate of the serving measurement (0: skip)")
+    ap.add_argument("--serve-rates", default="1000,10000,50000")
     ap.add_argument("--cpu-sample-mib", type=int, default=8)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baselines (quick runs)")
     ap.add_argument("--device-only", action="store_true",
@@ -163,6 +166,128 @@ def cpu_zlib_rate(data: np.ndarray, threads: int):
     return data.size / dt / 1e9, len(gz) / data.size
 
 
+def uneven_items(scale: float = 1.0):
+    """The 1,000-file mix (seed 3) cut into 2 MiB chunks + short remainders."""
+    files = W.uneven_files(1000, seed=3, scale=scale)
+    items = []
+    for _, _, data in files:
+        for o, n in W.chunk_spans(data.size, CHUNK):
+            items.append(np.ascontiguousarray(data[o:o + n]))
+    return items
+
+
+def run_uneven(ctx, args, stream):
+    """Batched persistent path vs the plain one-launch-per-chunk path, host API."""
+    import torch
+    items = uneven_items()
+    total = sum(x.size for x in items)
+    for _ in range(max(1, args.warmup)):
+        ctx.compress_batch(items)
+    times = []
+    for _ in range(max(1, args.steps)):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        outs = ctx.compress_batch(items)
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+    batched = total / (min(times) / 1e3) / 1e9
+    ctx.compress_batch_plain(items[:8])
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    plain_outs = ctx.compress_batch_plain(items)
+    e1.record(stream)
+    e1.synchronize()
+    plain = total / (e0.elapsed_time(e1) / 1e3) / 1e9
+    same = all(a == b for a, b in zip(outs, plain_outs))
+    return {"files": 1000, "chunks": len(items), "bytes": int(total), "batched_gbs": round(batched, 4),
+            "plain_gbs": round(plain, 4), "batched_over_plain": round(batched / plain, 3),
+            "batched_ms": round(min(times), 3), "outputs_identical": same,
+            "ratio": round(sum(len(o) for o in outs) / total, 5)}
+
+
+def run_serving(device: int, seconds: float, rates):
+    """Open-loop Poisson arrivals (seed 4), sizes log-uniform 4 KiB-16 MiB,
+    content sliced from the three generators; continuous batching engine."""
+    import ctypes
+    import threading
+
+    from gpzip_b200 import native
+    pools = [W.text(48 << 20, seed=40), W.logs(48 << 20, seed=41), W.binary(48 << 20, seed=42)]
+    results = []
+    for rate in rates:
+        ctx = native.Context(device=device, pool_bytes=40 << 30)
+        L = ctx.L
+        t, sizes, kinds, offs = W.serving_arrivals(rate, seconds, seed=4)
+        sizes = np.minimum(sizes, (48 << 20) - 1)
+        tickets = []
+        lock = threading.Lock()
+        done = threading.Event()
+        rejected = [0]
+
+        def poller():
+            buf = np.empty(ctx.bound(16 << 20), dtype=np.uint8)
+            i = 0
+            while True:
+                with lock:
+                    have = len(tickets)
+                if i >= have:
+                    if done.is_set():
+                        with lock:
+                            if i >= len(tickets):
+                                return
+                    threading.Event().wait(0.0005)
+                    continue
+                tk = tickets[i]
+                o = native.Out(buf.ctypes.data, buf.size, 0, 0)
+                while L.gpz_poll(ctx._h, tk, ctypes.byref(o), 1000) == native.GPZ_E_PENDING:
+                    pass
+                i += 1
+
+        # warm the engine (graphs, autotune) before the clock starts
+        for w in range(3):
+            tk = ctx.submit(pools[w][: 1 << 20])
+            ctx.poll(tk, ctx.bound(1 << 20), wait_ms=30000)
+        ctx.serve_reset_stats()
+        th = threading.Thread(target=poller)
+        th.start()
+        import time as _t
+        t0 = _t.perf_counter()
+        d = native.Desc()
+        tk = ctypes.c_uint64()
+        for i in range(t.size):
+            while _t.perf_counter() - t0 < t[i]:
+                pass
+            pool = pools[int(kinds[i])]
+            n = int(sizes[i])
+            off = int(offs[i] * (pool.size - n))
+            d.in_, d.n, d.level = pool.ctypes.data + off, n, 5
+            rc = L.gpz_submit(ctx._h, ctypes.byref(d), ctypes.byref(tk))
+            if rc == native.GPZ_OK:
+                with lock:
+                    tickets.append(tk.value)
+            else:
+                rejected[0] += 1
+        offered_s = _t.perf_counter() - t0
+        done.set()
+        th.join()
+        wall = _t.perf_counter() - t0
+        st = ctx.serve_stats()
+        small = int(np.sum(sizes <= (1 << 20)))
+        results.append({
+            "rate_per_s": rate, "seconds": seconds, "requests": int(t.size), "requests_le_1MiB": small,
+            "completed": st["completed"], "rejected": rejected[0],
+            "rejected_frac": round(rejected[0] / max(1, t.size), 4),
+            "p50_ms": round(st["p50_ms"], 3), "p99_ms": round(st["p99_ms"], 3), "p999_ms": round(st["p999_ms"], 3),
+            "p50_le_1MiB_ms": round(st["p50_small_ms"], 3), "p99_le_1MiB_ms": round(st["p99_small_ms"], 3),
+            "p999_le_1MiB_ms": round(st["p999_small_ms"], 3),
+            "offered_gbs": round(float(np.sum(sizes)) / seconds / 1e9, 3),
+            "throughput_gbs": round(st["bytes_in"] / wall / 1e9, 3), "batches": st["batches"],
+            "submit_lag_s": round(offered_s - seconds, 3)})
+        ctx.close()
+    return results
+
+
 def run_reference(args, rank: int):
     """--impl reference: the CPU port of the path on all host threads."""
     if rank != 0:
@@ -215,6 +340,23 @@ def main():
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
+
+    if args.workload == "uneven":
+        uctx = native.Context(device=local, member_bytes=MEMBER)
+        res = run_uneven(uctx, args, torch.cuda.current_stream())
+        uctx.close()
+        if rank == 0:
+            line = {"metric": METRIC, "value": res["batched_gbs"], "unit": "GB/s", "n_gpus": world,
+                    "steps": args.steps, "warmup": args.warmup, "ms_per_step": res["batched_ms"],
+                    "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+                    "data": "synthetic (seeded generators standing in for the reference's corpora)",
+                    "config": {"workload": "uneven-1000-files (seed 3): 2 MiB chunks + remainders, host API",
+                               "member_bytes": MEMBER},
+                    "uneven": res}
+            print(json.dumps(line), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
+        return
 
     data, desc = workload(args.workload)
     spans = W.chunk_spans(data.size, CHUNK)
@@ -322,6 +464,11 @@ def main():
         zl = {"value": round(zr, 4), "unit": "GB/s", "cores": threads, "ratio": round(zratio, 5),
               "what": "gpzip-cpu equivalent: zlib 1.3 level 5, one gzip member per 2 MiB chunk"}
 
+    serving = None
+    if rank == 0 and args.serve_seconds > 0 and not args.device_only:
+        rates = [int(x) for x in args.serve_rates.split(",") if x]
+        serving = run_serving(local, args.serve_seconds, rates)
+
     if world > 1:
         dist.barrier()
     if rank == 0:
@@ -345,6 +492,7 @@ def main():
             "clocks": clk,
             "ratio": round(ratio, 5),
             "parity": parity,
+            "serving": serving,
         }
         print(json.dumps(line), flush=True)
     ctx.close()

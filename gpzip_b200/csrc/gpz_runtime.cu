@@ -38,7 +38,7 @@ namespace {
 
 constexpr size_t kDefaultMember = 131072;
 constexpr size_t kMaxMember = 2u << 20;
-constexpr size_t kDefaultBatch = 128u << 20;
+constexpr size_t kDefaultBatch = 32u << 20;
 constexpr size_t kDefaultPool = 40ull << 30;
 constexpr int kBuckets = 5;
 constexpr size_t kDescHeader = 64;  // batch dimensions at the start of a descriptor block
@@ -68,26 +68,100 @@ double now_ms() {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
-// memcpy over several threads for large copies.
-void par_memcpy(void* dst, const void* src, size_t n) {
-    constexpr size_t kPiece = 4u << 20;
-    if (n < 2 * kPiece) {
-        std::memcpy(dst, src, n);
-        return;
+// A small pool of host threads for the staging copies (inputs into pinned
+// memory, gzip streams out of it): a batch's copies are cut into pieces and
+// spread over the workers and the calling thread.  Each run publishes an
+// immutable job; a worker that wakes late only finds it drained.
+class CopyPool {
+  public:
+    struct Copy {
+        void* dst;
+        const void* src;
+        size_t n;
+    };
+
+    CopyPool() {
+        const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+        const unsigned nw = std::min(hw, 16u) - 1;
+        for (unsigned i = 0; i < nw; i++) th_.emplace_back([this] { work(); });
     }
-    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    const size_t nth = std::min<size_t>(std::min<size_t>(hw, 16), n / kPiece);
-    const size_t per = round_up((n + nth - 1) / nth, 64);
-    std::vector<std::thread> th;
-    for (size_t t = 1; t < nth; t++) {
-        const size_t o = t * per;
-        if (o >= n) break;
-        th.emplace_back([=] {
-            std::memcpy(static_cast<char*>(dst) + o, static_cast<const char*>(src) + o, std::min(per, n - o));
-        });
+    ~CopyPool() {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        for (auto& t : th_) t.join();
     }
-    std::memcpy(dst, src, std::min(per, n));
-    for (auto& x : th) x.join();
+
+    void run(const std::vector<Copy>& copies) {
+        constexpr size_t kPiece = 1u << 20;
+        size_t total = 0;
+        for (auto& c : copies) total += c.n;
+        if (total < 2 * kPiece || th_.empty()) {
+            for (auto& c : copies) std::memcpy(c.dst, c.src, c.n);
+            return;
+        }
+        auto job = std::make_shared<Job>();
+        for (auto& c : copies)
+            for (size_t o = 0; o < c.n; o += kPiece)
+                job->pieces.push_back(Copy{static_cast<char*>(c.dst) + o, static_cast<const char*>(c.src) + o,
+                                           std::min(kPiece, c.n - o)});
+        job->left = job->pieces.size();
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            job_ = job;
+            gen_++;
+        }
+        cv_.notify_all();
+        drain(*job);
+        std::unique_lock<std::mutex> lk(job->mu);
+        job->cv.wait(lk, [&] { return job->left.load() == 0; });
+    }
+
+  private:
+    struct Job {
+        std::vector<Copy> pieces;
+        std::atomic<size_t> next{0}, left{0};
+        std::mutex mu;
+        std::condition_variable cv;
+    };
+    static void drain(Job& j) {
+        for (;;) {
+            const size_t i = j.next.fetch_add(1);
+            if (i >= j.pieces.size()) return;
+            std::memcpy(j.pieces[i].dst, j.pieces[i].src, j.pieces[i].n);
+            if (j.left.fetch_sub(1) == 1) {
+                std::lock_guard<std::mutex> lk(j.mu);
+                j.cv.notify_all();
+            }
+        }
+    }
+    void work() {
+        uint64_t seen = 0;
+        for (;;) {
+            std::shared_ptr<Job> job;
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_.wait(lk, [&] { return stop_ || gen_ != seen; });
+                if (stop_) return;
+                seen = gen_;
+                job = job_;
+            }
+            if (job) drain(*job);
+        }
+    }
+    std::vector<std::thread> th_;
+    std::mutex mu_;
+    std::condition_variable cv_;
+    std::shared_ptr<Job> job_;
+    uint64_t gen_ = 0;
+    bool stop_ = false;
+};
+
+CopyPool& copy_pool() {
+    static CopyPool pool;
+    return pool;
 }
 
 struct Span {
@@ -448,8 +522,12 @@ int submit_slot(gpz_ctx* c, Slot& sl, const gpz_desc* d, size_t count, bool plai
     if ((rc = reserve(c, sl, in_bytes, true, true, obound))) return rc;
     if ((rc = ensure_host(c, sl, sl.h_in, sl.h_in_cap, in_bytes + 64, false))) return rc;
     if ((rc = ensure_host(c, sl, sl.h_out, sl.h_out_cap, obound + 64, true))) return rc;
-    for (size_t i = 0; i < count; i++)
-        if (d[i].n) par_memcpy(sl.h_in + sl.spans[i].dev_off, d[i].in, d[i].n);
+    {
+        std::vector<CopyPool::Copy> copies;
+        for (size_t i = 0; i < count; i++)
+            if (d[i].n) copies.push_back(CopyPool::Copy{sl.h_in + sl.spans[i].dev_off, d[i].in, d[i].n});
+        copy_pool().run(copies);
+    }
     cudaStream_t s = sl.stream;
     CU(c, cudaMemcpyAsync(sl.d_in.p, sl.h_in, in_bytes, cudaMemcpyHostToDevice, s));
     if ((rc = upload_desc(c, sl, s))) return rc;
@@ -514,6 +592,7 @@ int finish_slot(gpz_ctx* c, Slot& sl, gpz_out* outs, size_t first_item) {
     if (rc) return rc;
     frame_members(sl.h_mout, 0, nm, sl.h_out, 0);
     int first_bad = GPZ_OK;
+    std::vector<CopyPool::Copy> copies;
     for (size_t i = 0; i < sl.spans.size(); i++) {
         const Span& sp = sl.spans[i];
         const MemberOut& a = sl.h_mout[sp.first_member];
@@ -526,9 +605,10 @@ int finish_slot(gpz_ctx* c, Slot& sl, gpz_out* outs, size_t first_item) {
             if (first_bad == GPZ_OK) first_bad = GPZ_E_SPACE;
             continue;
         }
-        par_memcpy(o.out, sl.h_out + beg, end - beg);
+        copies.push_back(CopyPool::Copy{o.out, sl.h_out + beg, end - beg});
         o.status = GPZ_OK;
     }
+    copy_pool().run(copies);
     if (first_bad != GPZ_OK) fail(c, first_bad, "output buffer too small");
     return first_bad;
 }
