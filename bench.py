@@ -184,6 +184,7 @@ def run_uneven(ctx, args, stream):
     for _ in range(max(1, args.warmup)):
         ctx.compress_batch(items)
     times = []
+    ctx.host_times(reset=True)
     for _ in range(max(1, args.steps)):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -192,6 +193,7 @@ def run_uneven(ctx, args, stream):
         e1.synchronize()
         times.append(e0.elapsed_time(e1))
     batched = total / (min(times) / 1e3) / 1e9
+    host = {k: round(v / max(1, args.steps), 3) for k, v in ctx.host_times(reset=True).items()}
     ctx.compress_batch_plain(items[:8])
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
@@ -202,7 +204,7 @@ def run_uneven(ctx, args, stream):
     same = all(a == b for a, b in zip(outs, plain_outs))
     return {"files": 1000, "chunks": len(items), "bytes": int(total), "batched_gbs": round(batched, 4),
             "plain_gbs": round(plain, 4), "batched_over_plain": round(batched / plain, 3),
-            "batched_ms": round(min(times), 3), "outputs_identical": same,
+            "batched_ms": round(min(times), 3), "outputs_identical": same, "host_ms_per_step": host,
             "ratio": round(sum(len(o) for o in outs) / total, 5)}
 
 
@@ -249,6 +251,7 @@ def run_serving(device: int, seconds: float, rates):
             tk = ctx.submit(pools[w][: 1 << 20])
             ctx.poll(tk, ctx.bound(1 << 20), wait_ms=30000)
         ctx.serve_reset_stats()
+        ctx.host_times(reset=True)
         th = threading.Thread(target=poller)
         th.start()
         import time as _t
@@ -262,7 +265,7 @@ def run_serving(device: int, seconds: float, rates):
             n = int(sizes[i])
             off = int(offs[i] * (pool.size - n))
             d.in_, d.n, d.level = pool.ctypes.data + off, n, 5
-            rc = L.gpz_submit(ctx._h, ctypes.byref(d), ctypes.byref(tk))
+            rc = L.gpz_submit_ref(ctx._h, ctypes.byref(d), ctypes.byref(tk))
             if rc == native.GPZ_OK:
                 with lock:
                     tickets.append(tk.value)
@@ -273,6 +276,7 @@ def run_serving(device: int, seconds: float, rates):
         th.join()
         wall = _t.perf_counter() - t0
         st = ctx.serve_stats()
+        host = {k: round(v, 1) for k, v in ctx.host_times().items()}
         small = int(np.sum(sizes <= (1 << 20)))
         results.append({
             "rate_per_s": rate, "seconds": seconds, "requests": int(t.size), "requests_le_1MiB": small,
@@ -283,7 +287,7 @@ def run_serving(device: int, seconds: float, rates):
             "p999_le_1MiB_ms": round(st["p999_small_ms"], 3),
             "offered_gbs": round(float(np.sum(sizes)) / seconds / 1e9, 3),
             "throughput_gbs": round(st["bytes_in"] / wall / 1e9, 3), "batches": st["batches"],
-            "submit_lag_s": round(offered_s - seconds, 3)})
+            "submit_lag_s": round(offered_s - seconds, 3), "host_ms_total": host, "wall_s": round(wall, 3)})
         ctx.close()
     return results
 
@@ -429,6 +433,7 @@ def main():
     barrier()
     e_times = []
     e2e_out = 0
+    ectx.host_times(reset=True)
     for _ in range(1 if args.device_only else max(2, args.steps // 2)):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
@@ -442,6 +447,7 @@ def main():
     if world > 1:
         dist.all_reduce(et, op=dist.ReduceOp.MAX)
     e2e_value = data.size * len(e_times) * world / (float(et.item()) / 1e3) / 1e9
+    e2e_host = {k: round(v / max(1, len(e_times)), 3) for k, v in ectx.host_times().items()}
 
     stage_ms = stages / args.steps
     names = ["k_lookup", "k_walk", "k_huff", "k_emit"]
@@ -487,7 +493,8 @@ def main():
             "cpu_baseline": cpu,
             "gpzip_cpu_equiv": zl,
             "e2e": {"value": round(e2e_value, 4), "unit": "GB/s", "h2d_bytes_per_step": int(data.size),
-                    "d2h_bytes_per_step": int(e2e_out), "api": "gpz_compress_batch (host buffers)"},
+                    "d2h_bytes_per_step": int(e2e_out), "api": "gpz_compress_batch (host buffers)",
+                    "host_ms_per_step": e2e_host},
             "gpu_launches": int(launches),
             "clocks": clk,
             "ratio": round(ratio, 5),

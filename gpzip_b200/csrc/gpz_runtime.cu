@@ -223,6 +223,9 @@ struct gpz_ctx {
     Slot slots[2];
     int next_slot = 0;
     float stage_ms[4] = {0, 0, 0, 0};
+    // host-side time per pipeline step, ms, accumulated (gpz_host_times)
+    std::mutex times_mu;
+    double host_ms[6] = {0, 0, 0, 0, 0, 0};  // plan, copy in, enqueue, wait, frame + copy out, batches
     std::vector<MemberOut> mout;  // member table of the last synchronous pass
     std::unique_ptr<ServeEngine> serve;
     std::mutex serve_mu;
@@ -506,8 +509,14 @@ int autotune(gpz_ctx* c, Slot& sl, const BatchParams& bp, const DrainTarget* dt,
     return GPZ_OK;
 }
 
+void add_time(gpz_ctx* c, int k, double ms) {
+    std::lock_guard<std::mutex> lk(c->times_mu);
+    c->host_ms[k] += ms;
+}
+
 // Plans, uploads and launches one batch of host items on a slot (no wait).
 int submit_slot(gpz_ctx* c, Slot& sl, const gpz_desc* d, size_t count, bool plain) {
+    double t0 = now_ms();
     sl.spans.assign(count, Span{});
     size_t in_bytes = 0;
     for (size_t i = 0; i < count; i++) {
@@ -522,12 +531,16 @@ int submit_slot(gpz_ctx* c, Slot& sl, const gpz_desc* d, size_t count, bool plai
     if ((rc = reserve(c, sl, in_bytes, true, true, obound))) return rc;
     if ((rc = ensure_host(c, sl, sl.h_in, sl.h_in_cap, in_bytes + 64, false))) return rc;
     if ((rc = ensure_host(c, sl, sl.h_out, sl.h_out_cap, obound + 64, true))) return rc;
+    double t1 = now_ms();
+    add_time(c, 0, t1 - t0);
     {
         std::vector<CopyPool::Copy> copies;
         for (size_t i = 0; i < count; i++)
             if (d[i].n) copies.push_back(CopyPool::Copy{sl.h_in + sl.spans[i].dev_off, d[i].in, d[i].n});
         copy_pool().run(copies);
     }
+    t0 = now_ms();
+    add_time(c, 1, t0 - t1);
     cudaStream_t s = sl.stream;
     CU(c, cudaMemcpyAsync(sl.d_in.p, sl.h_in, in_bytes, cudaMemcpyHostToDevice, s));
     if ((rc = upload_desc(c, sl, s))) return rc;
@@ -555,6 +568,11 @@ int submit_slot(gpz_ctx* c, Slot& sl, const gpz_desc* d, size_t count, bool plai
     if (rc) return rc;
     CU(c, cudaEventRecord(sl.done, s));
     sl.busy = true;
+    add_time(c, 2, now_ms() - t0);
+    {
+        std::lock_guard<std::mutex> lk(c->times_mu);
+        c->host_ms[5] += 1;
+    }
     return GPZ_OK;
 }
 
@@ -574,7 +592,9 @@ void frame_members(const MemberOut* mo, size_t first, size_t count, uint8_t* dst
 // Waits for the slot's batch; returns the device status.
 int wait_slot(gpz_ctx* c, Slot& sl) {
     sl.busy = false;
+    const double t0 = now_ms();
     CU(c, cudaEventSynchronize(sl.done));
+    add_time(c, 3, now_ms() - t0);
     if (c->flags & GPZ_FLAG_STAGE_TIMING)
         for (int i = 0; i < 4; i++) cudaEventElapsedTime(&c->stage_ms[i], sl.ev[i], sl.ev[i + 1]);
     const uint32_t err = *sl.h_err;
@@ -587,6 +607,7 @@ int wait_slot(gpz_ctx* c, Slot& sl) {
 // into its caller buffer.
 int finish_slot(gpz_ctx* c, Slot& sl, gpz_out* outs, size_t first_item) {
     int rc = wait_slot(c, sl);
+    const double t0 = now_ms();
     const size_t nm = sl.members.size();
     c->mout.assign(sl.h_mout, sl.h_mout + nm);
     if (rc) return rc;
@@ -609,6 +630,7 @@ int finish_slot(gpz_ctx* c, Slot& sl, gpz_out* outs, size_t first_item) {
         o.status = GPZ_OK;
     }
     copy_pool().run(copies);
+    add_time(c, 4, now_ms() - t0);
     if (first_bad != GPZ_OK) fail(c, first_bad, "output buffer too small");
     return first_bad;
 }
@@ -692,7 +714,9 @@ namespace {
 
 struct Request {
     uint64_t id = 0;
-    std::vector<uint8_t> in;
+    std::vector<uint8_t> in;  // owned copy (gpz_submit), or empty (gpz_submit_ref)
+    const uint8_t* src = nullptr;
+    size_t n = 0;
     size_t units = 0, units_done = 0;
     std::vector<std::vector<uint8_t>> pieces;  // gzip members of each unit
     double t_arrive = 0, t_done = 0;
@@ -708,22 +732,29 @@ struct Unit {
 
 }  // namespace
 
-// Continuous batching: requests are cut into 2 MiB units (whole members);
-// whenever a pipeline slot is free, the engine forms a batch from the waiting
-// units -- those of requests of at most 1 MiB first, then the rest in arrival
-// order, up to the batch cap -- and launches it while the other slot's batch
-// is still on the device.  A request completes when its last unit does, and
-// its gzip stream is its units' members in order, byte for byte what
-// gpz_compress_chunk returns for it alone.  Admission: a request is rejected
-// (GPZ_E_BUSY) while the bytes queued or on the device would exceed the pool
-// cap.
+// Continuous batching: requests are cut into 2 MiB units (whole members).
+// A launcher thread forms a batch whenever a pipeline slot is free -- units
+// of requests of at most 1 MiB first, then the rest in arrival order, up to
+// the batch cap -- and launches it while the other slots' batches are still
+// on the device; a completer thread retires finished batches in launch order
+// (framing, copies into the requests).  A request completes when its last
+// unit does, and its gzip stream is its units' members in order: byte for
+// byte what gpz_compress_chunk returns for it alone.  Admission: a request is
+// rejected (GPZ_E_BUSY) while the bytes queued or on the device would exceed
+// the pool cap.
 struct ServeEngine {
+    static constexpr int kSlots = 3;
+    static constexpr size_t kUnit = 2u << 20;
+    static constexpr size_t kSmall = 1u << 20;
+
     gpz_ctx* c = nullptr;
-    Slot slots[2];
-    std::thread th;
+    Slot slots[kSlots];
+    std::thread launcher, completer;
     std::mutex mu;
-    std::condition_variable cv_work, cv_done;
+    std::condition_variable cv_work, cv_done, cv_inflight, cv_free;
     std::deque<Unit> small_q, large_q;
+    std::deque<int> inflight_q;  // slots in launch order
+    bool slot_free[kSlots] = {true, true, true};
     std::unordered_map<uint64_t, std::shared_ptr<Request>> reqs;
     uint64_t next_id = 1;
     bool stop = false;
@@ -732,19 +763,17 @@ struct ServeEngine {
     std::vector<double> lat_all, lat_small;
     uint64_t rejected = 0, batches = 0, bytes_in = 0, bytes_out = 0;
     double max_queue_ms = 0;
-    std::vector<Unit> inflight[2];
-
-    static constexpr size_t kUnit = 2u << 20;
-    static constexpr size_t kSmall = 1u << 20;
+    std::vector<Unit> inflight[kSlots];
 
     int start(gpz_ctx* ctx) {
         c = ctx;
         cudaSetDevice(c->device);
         for (auto& s : slots) {
-            int rc = init_slot(c, s);
+            const int rc = init_slot(c, s);
             if (rc) return rc;
         }
-        th = std::thread([this] { loop(); });
+        launcher = std::thread([this] { launch_loop(); });
+        completer = std::thread([this] { complete_loop(); });
         return GPZ_OK;
     }
 
@@ -754,11 +783,14 @@ struct ServeEngine {
             stop = true;
         }
         cv_work.notify_all();
-        if (th.joinable()) th.join();
+        cv_inflight.notify_all();
+        cv_free.notify_all();
+        if (launcher.joinable()) launcher.join();
+        if (completer.joinable()) completer.join();
         for (auto& s : slots) free_slot(c, s);
     }
 
-    int submit(const gpz_desc* d, uint64_t* ticket) {
+    int submit(const gpz_desc* d, uint64_t* ticket, bool copy) {
         auto r = std::make_shared<Request>();
         r->t_arrive = now_ms();
         r->small = d->n <= kSmall;
@@ -772,11 +804,17 @@ struct ServeEngine {
             }
             queued_bytes += d->n;
         }
-        r->in.assign(d->in, d->in + d->n);
+        if (copy) {
+            r->in.assign(d->in, d->in + d->n);
+            r->src = r->in.data();
+        } else {
+            r->src = d->in;  // the caller keeps it alive until the result is polled
+        }
+        r->n = d->n;
         std::lock_guard<std::mutex> lk(mu);
         r->id = next_id++;
         for (size_t u = 0; u < r->units; u++) {
-            Unit un{r, u, u * kUnit, std::min(kUnit, d->n - std::min(d->n, u * kUnit))};
+            const Unit un{r, u, u * kUnit, std::min(kUnit, d->n - std::min(d->n, u * kUnit))};
             (r->small ? small_q : large_q).push_back(un);
         }
         reqs[r->id] = r;
@@ -805,13 +843,15 @@ struct ServeEngine {
             o->status = GPZ_E_SPACE;
             return GPZ_E_SPACE;  // the result stays available for a larger buffer
         }
+        lk.unlock();
         size_t k = 0;
         for (auto& p : r->pieces) {
             std::memcpy(o->out + k, p.data(), p.size());
             k += p.size();
         }
         o->status = GPZ_OK;
-        reqs.erase(it);
+        lk.lock();
+        reqs.erase(ticket);
         return GPZ_OK;
     }
 
@@ -829,10 +869,70 @@ struct ServeEngine {
         return b;
     }
 
+    void launch_loop() {
+        cudaSetDevice(c->device);
+        for (;;) {
+            int k = -1;
+            std::vector<Unit> batch;
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                cv_free.wait(lk, [&] {
+                    if (stop) return true;
+                    for (int i = 0; i < kSlots; i++)
+                        if (slot_free[i]) return true;
+                    return false;
+                });
+                cv_work.wait(lk, [&] { return stop || !small_q.empty() || !large_q.empty(); });
+                if (stop) return;
+                for (int i = 0; i < kSlots; i++)
+                    if (slot_free[i]) {
+                        k = i;
+                        break;
+                    }
+                if (k < 0) continue;
+                batch = take_batch();
+                if (batch.empty()) continue;
+                slot_free[k] = false;
+                max_queue_ms = std::max(max_queue_ms, now_ms() - batch.front().req->t_arrive);
+            }
+            std::vector<gpz_desc> ds(batch.size());
+            for (size_t i = 0; i < batch.size(); i++)
+                ds[i] = gpz_desc{batch[i].req->src + batch[i].off, batch[i].n, 0};
+            inflight[k] = std::move(batch);
+            const int rc = submit_slot(c, slots[k], ds.data(), ds.size(), false);
+            std::lock_guard<std::mutex> lk(mu);
+            if (rc == GPZ_OK) batches++;
+            else slots[k].busy = false;
+            launch_rc[k] = rc;
+            inflight_q.push_back(k);
+            cv_inflight.notify_one();
+        }
+    }
+
+    void complete_loop() {
+        cudaSetDevice(c->device);
+        for (;;) {
+            int k;
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                cv_inflight.wait(lk, [&] { return (stop && inflight_q.empty()) || !inflight_q.empty(); });
+                if (inflight_q.empty()) return;
+                k = inflight_q.front();
+                inflight_q.pop_front();
+            }
+            int rc = launch_rc[k];
+            if (rc == GPZ_OK) rc = wait_slot(c, slots[k]);
+            complete(k, rc);
+            std::lock_guard<std::mutex> lk(mu);
+            slot_free[k] = true;
+            cv_free.notify_one();
+        }
+    }
+
     void complete(int k, int rc) {
         Slot& sl = slots[k];
         std::vector<Unit>& units = inflight[k];
-        const double t = now_ms();
+        const double t0 = now_ms();
         std::vector<std::vector<uint8_t>> outs(units.size());
         if (rc == GPZ_OK) {
             frame_members(sl.h_mout, 0, sl.members.size(), sl.h_out, 0);
@@ -843,6 +943,8 @@ struct ServeEngine {
                 outs[i].assign(sl.h_out + a.gz_off, sl.h_out + z.gz_off + 18 + z.deflate_bytes);
             }
         }
+        const double t = now_ms();
+        add_time(c, 4, t - t0);
         std::lock_guard<std::mutex> lk(mu);
         for (size_t i = 0; i < units.size(); i++) {
             auto& r = units[i].req;
@@ -858,53 +960,16 @@ struct ServeEngine {
                 const double lat = t - r->t_arrive;
                 lat_all.push_back(lat);
                 if (r->small) lat_small.push_back(lat);
-                bytes_in += r->in.size();
+                bytes_in += r->n;
                 std::vector<uint8_t>().swap(r->in);
+                r->src = nullptr;
             }
         }
         units.clear();
         cv_done.notify_all();
     }
 
-    void loop() {
-        cudaSetDevice(c->device);
-        int turn = 0;
-        for (;;) {
-            std::vector<Unit> batch;
-            {
-                std::unique_lock<std::mutex> lk(mu);
-                if (!slots[0].busy && !slots[1].busy)
-                    cv_work.wait(lk, [&] { return stop || !small_q.empty() || !large_q.empty(); });
-                if (stop && small_q.empty() && large_q.empty() && !slots[0].busy && !slots[1].busy) return;
-                if (!slots[turn].busy) batch = take_batch();
-                if (!batch.empty()) max_queue_ms = std::max(max_queue_ms, now_ms() - batch.front().req->t_arrive);
-            }
-            if (!batch.empty()) {
-                Slot& sl = slots[turn];
-                std::vector<gpz_desc> ds(batch.size());
-                for (size_t i = 0; i < batch.size(); i++)
-                    ds[i] = gpz_desc{batch[i].req->in.data() + batch[i].off, batch[i].n, 0};
-                inflight[turn] = std::move(batch);
-                const int rc = submit_slot(c, sl, ds.data(), ds.size(), false);
-                if (rc) {
-                    sl.busy = false;
-                    complete(turn, rc);
-                } else {
-                    std::lock_guard<std::mutex> lk(mu);
-                    batches++;
-                }
-                turn ^= 1;
-                continue;
-            }
-            // nothing new to launch on this slot: retire the oldest batch
-            const int k = slots[turn].busy ? turn : (turn ^ 1);
-            if (slots[k].busy) {
-                const int rc = wait_slot(c, slots[k]);
-                complete(k, rc);
-                turn = k;
-            }
-        }
-    }
+    int launch_rc[kSlots] = {0, 0, 0};
 
     static double pct(std::vector<double> v, double q) {
         if (v.empty()) return 0;
@@ -1107,7 +1172,30 @@ int gpz_submit(gpz_ctx* c, const gpz_desc* d, uint64_t* ticket) {
             c->serve = std::move(e);
         }
     }
-    return c->serve->submit(d, ticket);
+    return c->serve->submit(d, ticket, true);
+}
+
+int gpz_submit_ref(gpz_ctx* c, const gpz_desc* d, uint64_t* ticket) {
+    if (!c || !d || !ticket || (!d->in && d->n)) return GPZ_E_ARG;
+    {
+        std::lock_guard<std::mutex> lk(c->serve_mu);
+        if (!c->serve) {
+            auto e = std::make_unique<ServeEngine>();
+            const int rc = e->start(c);
+            if (rc) return rc;
+            c->serve = std::move(e);
+        }
+    }
+    return c->serve->submit(d, ticket, false);
+}
+
+int gpz_host_times(gpz_ctx* c, double* ms6, int reset) {
+    if (!c || !ms6) return GPZ_E_ARG;
+    std::lock_guard<std::mutex> lk(c->times_mu);
+    for (int i = 0; i < 6; i++) ms6[i] = c->host_ms[i];
+    if (reset)
+        for (double& x : c->host_ms) x = 0;
+    return GPZ_OK;
 }
 
 int gpz_poll(gpz_ctx* c, uint64_t ticket, gpz_out* o, int wait_ms) {

@@ -28,7 +28,7 @@ EXPORTS = [
     "gpz_compress_batch", "gpz_compress_batch_plain", "gpz_compress_device", "gpz_frame_host",
     "gpz_debug_chunk", "gpz_submit", "gpz_poll", "gpz_serve_stats_get", "gpz_strerror", "gpz_last_error",
     "gpz_get_shape", "gpz_set_shape", "gpz_last_launches", "gpz_stage_times", "gpz_compress_member_static",
-    "gpz_serve_reset_stats",
+    "gpz_serve_reset_stats", "gpz_submit_ref", "gpz_host_times",
 ]
 
 
@@ -108,6 +108,10 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.gpz_serve_stats_get.restype = ctypes.c_int
     L.gpz_serve_reset_stats.argtypes = [vp]
     L.gpz_serve_reset_stats.restype = ctypes.c_int
+    L.gpz_submit_ref.argtypes = [vp, ctypes.POINTER(Desc), ctypes.POINTER(ctypes.c_uint64)]
+    L.gpz_submit_ref.restype = ctypes.c_int
+    L.gpz_host_times.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.c_int]
+    L.gpz_host_times.restype = ctypes.c_int
     L.gpz_strerror.argtypes = [ctypes.c_int]
     L.gpz_strerror.restype = ctypes.c_char_p
     L.gpz_last_error.argtypes = [vp]
@@ -188,21 +192,29 @@ class Context:
         return out[:n.value].tobytes()
 
     def _batch(self, fn, items, level: int = 5):
+        """One output allocation for all items; results are zero-copy views."""
         arrs = [_u8(x) for x in items]
         k = len(arrs)
         descs = (Desc * max(k, 1))()
         outs = (Out * max(k, 1))()
-        bufs = []
+        bounds = [self.bound(a.size) for a in arrs]
+        out = np.empty(max(1, sum(bounds)), dtype=np.uint8)
+        base = out.ctypes.data
+        off = 0
         for i, a in enumerate(arrs):
             descs[i].in_ = a.ctypes.data if a.size else None
             descs[i].n = a.size
             descs[i].level = level
-            b = np.empty(self.bound(a.size), dtype=np.uint8)
-            bufs.append(b)
-            outs[i].out = b.ctypes.data
-            outs[i].out_cap = b.size
+            outs[i].out = base + off
+            outs[i].out_cap = bounds[i]
+            off += bounds[i]
         self._check(fn(self._h, descs, k, outs), fn.__name__)
-        return [bufs[i][:outs[i].out_len].tobytes() for i in range(k)]
+        mv = memoryview(out)
+        res, off = [], 0
+        for i in range(k):
+            res.append(mv[off:off + outs[i].out_len])
+            off += bounds[i]
+        return res
 
     def compress_batch(self, items, level: int = 5):
         return self._batch(self.L.gpz_compress_batch, items, level)
@@ -275,6 +287,11 @@ class Context:
             rc = self.L.gpz_poll(self._h, ticket, ctypes.byref(o), wait_ms)
         self._check(rc, "gpz_poll")
         return buf[:o.out_len].tobytes()
+
+    def host_times(self, reset: bool = False) -> dict:
+        a = (ctypes.c_double * 6)()
+        self._check(self.L.gpz_host_times(self._h, a, int(reset)), "gpz_host_times")
+        return dict(zip(["plan_ms", "copy_in_ms", "enqueue_ms", "wait_ms", "copy_out_ms", "passes"], list(a)))
 
     def serve_reset_stats(self):
         self._check(self.L.gpz_serve_reset_stats(self._h), "gpz_serve_reset_stats")

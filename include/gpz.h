@@ -137,6 +137,9 @@ GPZ_API int gpz_debug_chunk(gpz_ctx* ctx, const uint8_t* in, size_t n, uint32_t*
  * is ready (wait_ms > 0 blocks up to that long), GPZ_E_SPACE (result kept)
  * if o->out_cap is short; the result is copied into o->out. */
 GPZ_API int gpz_submit(gpz_ctx* ctx, const gpz_desc* d, uint64_t* ticket);
+/* As gpz_submit, without the copy: the caller keeps d->in unchanged and
+ * alive until gpz_poll has returned the result. */
+GPZ_API int gpz_submit_ref(gpz_ctx* ctx, const gpz_desc* d, uint64_t* ticket);
 GPZ_API int gpz_poll(gpz_ctx* ctx, uint64_t ticket, gpz_out* o, int wait_ms);
 
 /* Serving statistics since the engine started or was last reset (latencies
@@ -198,6 +201,12 @@ GPZ_API uint64_t gpz_last_launches(gpz_ctx* ctx);
  * reuse of d_out. */
 GPZ_API int gpz_compress_member_static(const uint8_t* d_in, size_t n, uint8_t* d_out, size_t out_cap,
                                        size_t* out_len, void* stream);
+
+/* Host time spent in each pipeline step since the last reset, in ms: batch
+ * planning and buffer sizing, copying inputs into pinned staging, enqueueing
+ * uploads and kernels, waiting for the device, framing and copying results
+ * out; ms6[5] counts the device passes.  reset != 0 clears the counters. */
+GPZ_API int gpz_host_times(gpz_ctx* ctx, double* ms6, int reset);
 
 /* Device time of each stage of the last device pass, in ms: lookup, walk,
  * Huffman plan, emit.  Needs GPZ_FLAG_STAGE_TIMING at gpz_create. */
