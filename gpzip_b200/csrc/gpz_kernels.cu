@@ -1,20 +1,29 @@
 // gpz_kernels.cu -- sm_100a kernels of the gzip compression path.
 //
-// Four stages per batch, each a persistent kernel that claims work items
-// (4 KiB tiles, or members) from a device counter:
+// Kernels of one batch, in launch order.  The persistent ones claim work
+// items (4 KiB tiles, or members) from a device counter and read the batch's
+// member / tile counts from device memory, so one captured launch sequence
+// serves every batch of a size bucket:
 //
-//   k_lookup  per tile: segmented-hash build + window-bounded lookup
-//             (lz77_hash_build.wgsl:45-54 + lz77_hash_lookup.wgsl:99-173),
-//             plus the tile's zero-init CRC-32 (slice-by-8).
-//   k_walk    per tile: lazy-rule walk (lz77.rs:260-284) by pointer jumping,
-//             chained across tiles with a decoupled look-back; emits the
-//             walked tokens and the tile's symbol histogram.
-//   k_huff    per member: length-limited Huffman code construction
-//             (huffman.rs:26-152), dynamic block header (deflate.rs:830-932),
-//             exact bit plan per tile, gzip member placement by a decoupled
-//             look-back over members, CRC-32 combine.
-//   k_emit    per tile: per-token codes, block scan of bit lengths, bit
-//             packing into the batch's gzip stream (deflate.rs:934-958).
+//   k_segtab     per tile: the 4 KiB segment's distinct hashes with their
+//                oldest / newest offsets (what lz77_hash_build.wgsl:45-54
+//                leaves in table[h][seg]) and a per-position hash id.
+//   k_lookup     per tile: window-bounded candidate walk over the tile and
+//                the 8 segments before it (lz77_hash_lookup.wgsl:45-119),
+//                one packed token per position (pp).
+//   k_walk_exit  per tile: exit offset for each of the 258 entry offsets of
+//                the lazy walk (lz77.rs:260-284), by pointer jumping.
+//   k_chain      per member: the entry offset of every tile.
+//   k_walk_mark  per tile: walked tokens in order and the tile's symbol
+//                histogram.
+//   k_huff       per member: CRC-32, length-limited codes (huffman.rs:26-152),
+//                dynamic block header (deflate.rs:830-932), exact bit plan
+//                per tile.
+//   k_place      one CTA: byte offset of every gzip member (scan).
+//   k_frame      per member: gzip header words, shared boundary words, EOB.
+//   k_emit       per tile: per-token codes and bit packing
+//                (deflate.rs:934-958) into the batch's gzip stream.
+//   k_drain      optional: output and member table into mapped host memory.
 //
 // All arithmetic is integer and bit-exact with the reference.
 #include <cuda_runtime.h>
