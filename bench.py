@@ -403,7 +403,7 @@ def main():
     barrier()
     clocks = Clocks(local)
     clocks.start()
-    times, stages = [], np.zeros(4)
+    times, stages = [], np.zeros(len(native.STAGE_NAMES))
     for _ in range(args.steps):
         flush.zero_()
         e0 = torch.cuda.Event(enable_timing=True)
@@ -450,12 +450,14 @@ def main():
     e2e_host = {k: round(v / max(1, len(e_times)), 3) for k, v in ectx.host_times().items()}
 
     stage_ms = stages / args.steps
-    names = ["k_lookup", "k_walk", "k_huff", "k_emit"]
+    names = native.STAGE_NAMES
     dom = int(np.argmax(stage_ms))
     peak, peak_kind = measured_peaks()
     algo_bytes = data.size * (1.0 + ratio)
     achieved = algo_bytes / (stage_ms[dom] / 1e3) / 1e9
     tr = committed_traffic().get(names[dom])
+    # ncu DRAM bytes of that kernel per input byte on this workload, scaled
+    # to this launch's input (traffic grows with the input it processes)
     traffic = round(tr["dram_bytes_per_input_byte"] * data.size) if tr else None
 
     cpu = None

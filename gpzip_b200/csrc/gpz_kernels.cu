@@ -1287,11 +1287,12 @@ int gpz_launch_batch(const BatchParams& bp, const LaunchShape& ls, void* stream,
     const int gs = grid_of(ls.segtab_grid, bp.ntiles);
     const int gl = grid_of(ls.lookup_grid, bp.ntiles);
     k_segtab<512><<<gs, 512, kSegtabSmem, s>>>(bp);
+    mark(1);
     switch (ls.lookup_threads) {
         case 512: k_lookup<512><<<gl, 512, LookupSmem::kBytes, s>>>(bp); break;
         default: k_lookup<1024><<<gl, 1024, LookupSmem::kBytes, s>>>(bp); break;
     }
-    mark(1);
+    mark(2);
     const int gw = grid_of(ls.walk_grid, bp.ntiles);
     const int gc = ls.huff_grid > 0 ? ls.huff_grid : (nm + 127) / 128;
     switch (ls.walk_threads) {
@@ -1306,18 +1307,18 @@ int gpz_launch_batch(const BatchParams& bp, const LaunchShape& ls, void* stream,
             k_walk_mark<512><<<gw, 512, 0, s>>>(bp);
             break;
     }
-    mark(2);
+    mark(3);
     const int gh = grid_of(ls.huff_grid, bp.nmembers);
     k_huff<<<gh, kHuffThreads, 0, s>>>(bp);
     k_place<<<1, kPlaceThreads, 0, s>>>(bp);
     k_frame<<<gh, kFrameThreads, 0, s>>>(bp);
-    mark(3);
+    mark(4);
     const int ge = grid_of(ls.emit_grid, bp.ntiles);
     switch (ls.emit_threads) {
         case 256: k_emit<256><<<ge, 256, 0, s>>>(bp); break;
         default: k_emit<512><<<ge, 512, 0, s>>>(bp); break;
     }
-    mark(4);
+    mark(5);
     if (drain) k_drain<<<drain->grid, 256, 0, s>>>(bp, drain->h_out, drain->h_mout, drain->h_err);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }

@@ -186,7 +186,7 @@ struct Slot {
     size_t h_err_cap = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t done = nullptr;
-    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t ev[GPZ_STAGES + 1] = {};
     uint64_t gen = 1;  // bumps whenever a buffer the graphs capture moves
     struct Graph {
         uint64_t gen = 0;
@@ -222,7 +222,7 @@ struct gpz_ctx {
     std::mutex tune_mu;
     Slot slots[2];
     int next_slot = 0;
-    float stage_ms[4] = {0, 0, 0, 0};
+    float stage_ms[GPZ_STAGES] = {};
     // host-side time per pipeline step, ms, accumulated (gpz_host_times)
     std::mutex times_mu;
     double host_ms[6] = {0, 0, 0, 0, 0, 0};  // plan, copy in, enqueue, wait, frame + copy out, batches
@@ -596,7 +596,7 @@ int wait_slot(gpz_ctx* c, Slot& sl) {
     CU(c, cudaEventSynchronize(sl.done));
     add_time(c, 3, now_ms() - t0);
     if (c->flags & GPZ_FLAG_STAGE_TIMING)
-        for (int i = 0; i < 4; i++) cudaEventElapsedTime(&c->stage_ms[i], sl.ev[i], sl.ev[i + 1]);
+        for (int i = 0; i < GPZ_STAGES; i++) cudaEventElapsedTime(&c->stage_ms[i], sl.ev[i], sl.ev[i + 1]);
     const uint32_t err = *sl.h_err;
     if (err & GPZ_ERRBIT_SPIN) return fail(c, GPZ_E_TIMEOUT, "bounded device wait expired");
     if (err) return fail(c, GPZ_E_INTERNAL, "device self-check failed");
@@ -1107,7 +1107,7 @@ int gpz_compress_device(gpz_ctx* c, const void* d_in, const uint64_t* in_off, co
     CU(c, cudaMemcpyAsync(sl.h_err, static_cast<uint32_t*>(sl.d_cnt.p) + GPZ_NCOUNTERS, 4, cudaMemcpyDeviceToHost, s));
     CU(c, cudaStreamSynchronize(s));
     if (timing)
-        for (int i = 0; i < 4; i++) cudaEventElapsedTime(&c->stage_ms[i], sl.ev[i], sl.ev[i + 1]);
+        for (int i = 0; i < GPZ_STAGES; i++) cudaEventElapsedTime(&c->stage_ms[i], sl.ev[i], sl.ev[i + 1]);
     c->mout.assign(sl.h_mout, sl.h_mout + sl.members.size());
     if (*sl.h_err) return fail(c, (*sl.h_err & GPZ_ERRBIT_SPIN) ? GPZ_E_TIMEOUT : GPZ_E_INTERNAL, "device self-check");
     for (size_t i = 0; i < count; i++) out_off[i] = c->mout[sl.spans[i].first_member].gz_off;
@@ -1282,10 +1282,10 @@ int gpz_set_shape(gpz_ctx* c, const gpz_shape* s) {
 
 uint64_t gpz_last_launches(gpz_ctx* c) { return c ? c->launches.load() : 0; }
 
-int gpz_stage_times(gpz_ctx* c, float* ms4) {
-    if (!c || !ms4 || !(c->flags & GPZ_FLAG_STAGE_TIMING)) return GPZ_E_ARG;
+int gpz_stage_times(gpz_ctx* c, float* ms) {
+    if (!c || !ms || !(c->flags & GPZ_FLAG_STAGE_TIMING)) return GPZ_E_ARG;
     std::lock_guard<std::mutex> lk(c->mu);
-    for (int i = 0; i < 4; i++) ms4[i] = c->stage_ms[i];
+    for (int i = 0; i < GPZ_STAGES; i++) ms[i] = c->stage_ms[i];
     return GPZ_OK;
 }
 

@@ -21,6 +21,8 @@ GPZ_E_BUSY = 8
 GPZ_FLAG_NO_GRAPHS = 1
 GPZ_FLAG_NO_AUTOTUNE = 2
 GPZ_FLAG_STAGE_TIMING = 4
+# gpz_stage_times order (GPZ_STAGES values): the kernels each stage covers
+STAGE_NAMES = ["k_segtab", "k_lookup", "k_walk", "k_huff", "k_emit"]
 
 # Every symbol include/gpz.h declares.
 EXPORTS = [
@@ -260,8 +262,8 @@ class Context:
         return self.L.gpz_last_launches(self._h)
 
     def stage_times(self):
-        """Device ms of lookup, walk, Huffman plan, emit in the last pass."""
-        a = (ctypes.c_float * 4)()
+        """Device ms of each stage of the last pass (STAGE_NAMES order)."""
+        a = (ctypes.c_float * len(STAGE_NAMES))()
         self._check(self.L.gpz_stage_times(self._h, a), "gpz_stage_times")
         return list(a)
 

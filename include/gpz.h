@@ -208,9 +208,12 @@ GPZ_API int gpz_compress_member_static(const uint8_t* d_in, size_t n, uint8_t* d
  * out; ms6[5] counts the device passes.  reset != 0 clears the counters. */
 GPZ_API int gpz_host_times(gpz_ctx* ctx, double* ms6, int reset);
 
-/* Device time of each stage of the last device pass, in ms: lookup, walk,
- * Huffman plan, emit.  Needs GPZ_FLAG_STAGE_TIMING at gpz_create. */
-GPZ_API int gpz_stage_times(gpz_ctx* ctx, float* ms4);
+/* Device time of each stage of the last device pass, in ms, GPZ_STAGES
+ * values: segment summaries (k_segtab), lookup (k_lookup), walk (k_walk_exit,
+ * k_chain, k_walk_mark), Huffman plan and placement (k_huff, k_place,
+ * k_frame), emit (k_emit).  Needs GPZ_FLAG_STAGE_TIMING at gpz_create. */
+#define GPZ_STAGES 5
+GPZ_API int gpz_stage_times(gpz_ctx* ctx, float* ms);
 
 #ifdef __cplusplus
 }
