@@ -55,6 +55,7 @@ def parse():
     ap.add_argument("--serve-seconds", type=float, default=1.5,
                     help="seconds per arrival rate of the serving measurement (0: skip)")
     ap.add_argument("--serve-rates", default="1000,10000,50000")
+    ap.add_argument("--serve-only", action="store_true", help="run only the serving measurement")
     ap.add_argument("--cpu-sample-mib", type=int, default=8)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baselines (quick runs)")
     ap.add_argument("--device-only", action="store_true",
@@ -208,24 +209,29 @@ def run_uneven(ctx, args, stream):
             "ratio": round(sum(len(o) for o in outs) / total, 5)}
 
 
-def run_serving(device: int, seconds: float, rates):
+def run_serving(device: int, seconds: float, rates, warm_seconds: float = 0.3):
     """Open-loop Poisson arrivals (seed 4), sizes log-uniform 4 KiB-16 MiB,
-    content sliced from the three generators; continuous batching engine."""
+    content sliced from the three generators; continuous batching engine.
+    Each rate first runs warm_seconds of the same arrival process (seed 5:
+    graphs captured, pipelines primed), then the statistics are reset and
+    the measured run starts."""
     import ctypes
     import threading
+    import time as _t
 
     from gpzip_b200 import native
     pools = [W.text(48 << 20, seed=40), W.logs(48 << 20, seed=41), W.binary(48 << 20, seed=42)]
     results = []
-    for rate in rates:
-        ctx = native.Context(device=device, pool_bytes=40 << 30)
+
+    def drive(ctx, rate, secs, seed):
+        """Submits one arrival process open loop while a poller collects the
+        results; returns (requests, sizes, rejected, offered seconds, wall)."""
         L = ctx.L
-        t, sizes, kinds, offs = W.serving_arrivals(rate, seconds, seed=4)
+        t, sizes, kinds, offs = W.serving_arrivals(rate, secs, seed=seed)
         sizes = np.minimum(sizes, (48 << 20) - 1)
         tickets = []
         lock = threading.Lock()
         done = threading.Event()
-        rejected = [0]
 
         def poller():
             buf = np.empty(ctx.bound(16 << 20), dtype=np.uint8)
@@ -238,26 +244,19 @@ def run_serving(device: int, seconds: float, rates):
                         with lock:
                             if i >= len(tickets):
                                 return
-                    threading.Event().wait(0.0005)
+                    _t.sleep(0.0005)
                     continue
-                tk = tickets[i]
                 o = native.Out(buf.ctypes.data, buf.size, 0, 0)
-                while L.gpz_poll(ctx._h, tk, ctypes.byref(o), 1000) == native.GPZ_E_PENDING:
+                while L.gpz_poll(ctx._h, tickets[i], ctypes.byref(o), 1000) == native.GPZ_E_PENDING:
                     pass
                 i += 1
 
-        # warm the engine (graphs, autotune) before the clock starts
-        for w in range(3):
-            tk = ctx.submit(pools[w][: 1 << 20])
-            ctx.poll(tk, ctx.bound(1 << 20), wait_ms=30000)
-        ctx.serve_reset_stats()
-        ctx.host_times(reset=True)
         th = threading.Thread(target=poller)
         th.start()
-        import time as _t
-        t0 = _t.perf_counter()
+        rejected = 0
         d = native.Desc()
         tk = ctypes.c_uint64()
+        t0 = _t.perf_counter()
         for i in range(t.size):
             while _t.perf_counter() - t0 < t[i]:
                 pass
@@ -265,29 +264,37 @@ def run_serving(device: int, seconds: float, rates):
             n = int(sizes[i])
             off = int(offs[i] * (pool.size - n))
             d.in_, d.n, d.level = pool.ctypes.data + off, n, 5
-            rc = L.gpz_submit_ref(ctx._h, ctypes.byref(d), ctypes.byref(tk))
-            if rc == native.GPZ_OK:
+            if L.gpz_submit_ref(ctx._h, ctypes.byref(d), ctypes.byref(tk)) == native.GPZ_OK:
                 with lock:
                     tickets.append(tk.value)
             else:
-                rejected[0] += 1
-        offered_s = _t.perf_counter() - t0
+                rejected += 1
+        offered = _t.perf_counter() - t0
         done.set()
         th.join()
-        wall = _t.perf_counter() - t0
+        return t.size, sizes, rejected, offered, _t.perf_counter() - t0
+
+    for rate in rates:
+        ctx = native.Context(device=device, pool_bytes=40 << 30)
+        drive(ctx, rate, warm_seconds, seed=5)
+        ctx.serve_reset_stats()
+        ctx.host_times(reset=True)
+        nreq, sizes, rejected, offered_s, wall = drive(ctx, rate, seconds, seed=4)
         st = ctx.serve_stats()
         host = {k: round(v, 1) for k, v in ctx.host_times().items()}
+        lanes = [{k: (round(v, 3) if isinstance(v, float) else v) for k, v in ctx.lane_stats(i).items()}
+                 for i in range(2)]
         small = int(np.sum(sizes <= (1 << 20)))
         results.append({
-            "rate_per_s": rate, "seconds": seconds, "requests": int(t.size), "requests_le_1MiB": small,
-            "completed": st["completed"], "rejected": rejected[0],
-            "rejected_frac": round(rejected[0] / max(1, t.size), 4),
+            "rate_per_s": rate, "seconds": seconds, "requests": int(nreq), "requests_le_1MiB": small,
+            "completed": st["completed"], "rejected": rejected,
+            "rejected_frac": round(rejected / max(1, nreq), 4),
             "p50_ms": round(st["p50_ms"], 3), "p99_ms": round(st["p99_ms"], 3), "p999_ms": round(st["p999_ms"], 3),
             "p50_le_1MiB_ms": round(st["p50_small_ms"], 3), "p99_le_1MiB_ms": round(st["p99_small_ms"], 3),
             "p999_le_1MiB_ms": round(st["p999_small_ms"], 3),
             "offered_gbs": round(float(np.sum(sizes)) / seconds / 1e9, 3),
             "throughput_gbs": round(st["bytes_in"] / wall / 1e9, 3), "batches": st["batches"],
-            "submit_lag_s": round(offered_s - seconds, 3), "host_ms_total": host, "wall_s": round(wall, 3)})
+            "submit_lag_s": round(offered_s - seconds, 3), "host_ms_total": host, "lanes": lanes, "wall_s": round(wall, 3)})
         ctx.close()
     return results
 
@@ -337,6 +344,11 @@ def main():
     from gpzip_b200 import native
 
     torch.cuda.set_device(local)
+    if args.serve_only:
+        if rank == 0:
+            rates = [int(x) for x in args.serve_rates.split(",") if x]
+            print(json.dumps({"serving": run_serving(local, args.serve_seconds, rates)}), flush=True)
+        return
     if world > 1:
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
 

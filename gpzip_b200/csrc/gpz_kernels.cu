@@ -116,22 +116,50 @@ __device__ __forceinline__ uint32_t match_len(const uint32_t* w, uint32_t a, uin
     return limit;
 }
 
+// The first 16 bytes at window offset b as little-endian words: a
+// position loads them once and compares every candidate's first 16 bytes
+// against registers.
+struct Head {
+    uint32_t x0, x1, x2, x3;
+};
+
+__device__ __forceinline__ Head load_head(const uint32_t* w, uint32_t b) {
+    const uint32_t sb = (b & 3u) * 8u, ib = b >> 2;
+    const uint32_t b0 = w[ib], b1 = w[ib + 1], b2 = w[ib + 2], b3 = w[ib + 3], b4 = w[ib + 4];
+    return Head{__funnelshift_r(b0, b1, sb), __funnelshift_r(b1, b2, sb), __funnelshift_r(b2, b3, sb),
+                __funnelshift_r(b3, b4, sb)};
+}
+
 // try_candidate (lz77_hash_lookup.wgsl:99-121) on packed best = len<<16|dist.
 // A candidate that cannot beat the current best is dropped early: it must
-// agree with p at offset best_len, and best_len must be below the cap.
-__device__ __forceinline__ void try_cand(const uint8_t* win, const uint32_t* w32, uint32_t raw, uint32_t p,
-                                         uint32_t n, uint32_t w0, uint32_t& best) {
+// agree with p at offset best_len, and best_len must be below the cap.  The
+// first 16 bytes are compared with p's Head; only a candidate that agrees on
+// all of them continues in match_len.
+__device__ __forceinline__ void try_cand(const uint8_t* win, const uint32_t* w32, const Head& hp, uint32_t raw,
+                                         uint32_t p, uint32_t n, uint32_t w0, uint32_t& best) {
     if (raw == 0u || raw == kEmpty) return;
-    uint32_t cand = raw - 1u;
+    const uint32_t cand = raw - 1u;
     if (cand >= p) return;
-    uint32_t dist = p - cand;
+    const uint32_t dist = p - cand;
     if (dist > GPZ_WINDOW) return;
-    uint32_t limit = min(GPZ_MAX_MATCH, n - p);
-    uint32_t bl = best >> 16;
+    const uint32_t limit = min(GPZ_MAX_MATCH, n - p);
+    const uint32_t bl = best >> 16;
     if (bl >= limit) return;
-    uint32_t a = cand - w0, b = p - w0;
+    const uint32_t a = cand - w0, b = p - w0;
     if (bl >= 3u && win[a + bl] != win[b + bl]) return;
-    uint32_t len = match_len(w32, a, b, limit);
+    const uint32_t sa = (a & 3u) * 8u, ia = a >> 2;
+    const uint32_t a0 = w32[ia], a1 = w32[ia + 1], a2 = w32[ia + 2], a3 = w32[ia + 3], a4 = w32[ia + 4];
+    const uint32_t x0 = __funnelshift_r(a0, a1, sa) ^ hp.x0;
+    const uint32_t x1 = __funnelshift_r(a1, a2, sa) ^ hp.x1;
+    const uint32_t x2 = __funnelshift_r(a2, a3, sa) ^ hp.x2;
+    const uint32_t x3 = __funnelshift_r(a3, a4, sa) ^ hp.x3;
+    uint32_t len;
+    if (x0) len = __clz(__brev(x0)) >> 3;
+    else if (x1) len = 4u + (__clz(__brev(x1)) >> 3);
+    else if (x2) len = 8u + (__clz(__brev(x2)) >> 3);
+    else if (x3) len = 12u + (__clz(__brev(x3)) >> 3);
+    else len = limit > 16u ? 16u + match_len(w32, a + 16u, b + 16u, limit - 16u) : 16u;
+    len = min(len, limit);
     if (len >= 3u && len > bl) best = (len << 16) | dist;
 }
 
@@ -353,17 +381,36 @@ __global__ void __launch_bounds__(T, 1) k_lookup(BatchParams bp) {
             const uint16_t* gk = bp.seg_keys + (size_t)ts * GPZ_SEG;
             const uint32_t* go = bp.seg_on + (size_t)ts * GPZ_SEG;
             uint32_t* cb = cand + back * GPZ_SEG;
-            for (uint32_t j = tid; j < ns; j += T) {
-                const uint32_t h = gk[j];
-                uint32_t sl = slot_of(h);
-                for (int probe = 0; probe < kSlots; probe++) {
-                    const uint32_t wv = owntab[sl];
-                    if (wv == kEmpty) break;
-                    if ((wv & 0xFFFFu) == h) {
-                        cb[(wv >> 16) & (GPZ_SEG - 1)] = go[j];
-                        break;
+            // up to kJoinBatch keys per thread in flight: all loads first
+            // (each guarded by j < ns <= 4096, inside segment ts's arrays),
+            // then the probes
+            constexpr int kJoinBatch = 4;
+            for (uint32_t j0 = tid; j0 < ns; j0 += kJoinBatch * T) {
+                uint32_t hk[kJoinBatch], ov[kJoinBatch];
+#pragma unroll
+                for (int u = 0; u < kJoinBatch; u++) {
+                    const uint32_t j = j0 + (uint32_t)u * T;
+                    hk[u] = kEmpty;
+                    ov[u] = 0u;
+                    if (j < ns) {
+                        hk[u] = gk[j];
+                        ov[u] = go[j];
                     }
-                    sl = (sl + 1u) & (kSlots - 1);
+                }
+#pragma unroll
+                for (int u = 0; u < kJoinBatch; u++) {
+                    const uint32_t h = hk[u];
+                    if (h == kEmpty) continue;
+                    uint32_t sl = slot_of(h);
+                    for (int probe = 0; probe < kSlots; probe++) {
+                        const uint32_t wv = owntab[sl];
+                        if (wv == kEmpty) break;
+                        if ((wv & 0xFFFFu) == h) {
+                            cb[(wv >> 16) & (GPZ_SEG - 1)] = ov[u];
+                            break;
+                        }
+                        sl = (sl + 1u) & (kSlots - 1);
+                    }
                 }
             }
         }
@@ -378,16 +425,17 @@ __global__ void __launch_bounds__(T, 1) k_lookup(BatchParams bp) {
             const uint32_t id = myid[k], p = start + i;
             uint32_t best = 0;
             if (id != 0xFFFFu) {
-                try_cand(win, w32, start + (cand[id] >> 16) + 1u, p, n, w0, best);
+                const Head hp = load_head(w32, pl0 + i);
+                try_cand(win, w32, hp, start + (cand[id] >> 16) + 1u, p, n, w0, best);
                 for (uint32_t back = 1; back <= nback; back++) {
                     const uint32_t on = cand[back * GPZ_SEG + id];
                     if (on == kEmpty) continue;
                     const uint32_t qb = (S - back) << GPZ_SEG_LOG2;
                     const uint32_t rn = qb + (on & 0xFFFFu) + 1u;
-                    try_cand(win, w32, rn, p, n, w0, best);
+                    try_cand(win, w32, hp, rn, p, n, w0, best);
                     if ((best >> 16) < 16u) {
                         const uint32_t ro = qb + (on >> 16) + 1u;
-                        if (ro != rn) try_cand(win, w32, ro, p, n, w0, best);
+                        if (ro != rn) try_cand(win, w32, hp, ro, p, n, w0, best);
                     }
                 }
             }
@@ -400,74 +448,79 @@ __global__ void __launch_bounds__(T, 1) k_lookup(BatchParams bp) {
 
 // The lazy walk of lz77.rs:260-284 visits p, next(p), next(next(p)), ...
 // where next(p) depends only on pp[p] and pp[p+1].  Each 4 KiB tile is walked
-// independently by pointer jumping over next links: k_walk_exit computes,
-// for every position a walk can enter the tile at (its first 258 positions),
-// where it leaves; k_chain strings the tiles of a member together (entry of
-// tile b+1 = exit of tile b at its entry); k_walk_mark then marks the visited
-// positions from the known entry and emits them in order.
+// by one warp, 32 positions at a time: within a window of 32 positions the
+// links are resolved by pointer doubling over shuffles (5 rounds).
+// k_walk_exit computes, for every position a walk can enter the tile at (its
+// first 258), where it leaves, sweeping the windows from the top down;
+// k_chain strings the tiles of a member together (entry of tile b+1 = exit of
+// tile b at its entry); k_walk_mark walks forward from the known entry and
+// emits the visited tokens in order.
 
-struct WalkLinks {
-    uint32_t pps[GPZ_SEG + 1];              // pp of the tile and one lookahead
-    uint16_t nxt[GPZ_SEG];                  // next position, tile-relative
-    uint16_t J[2][GPZ_SEG + GPZ_EXITS];     // doubled links, absorbing past the tile
-};
+constexpr uint32_t kFull = 0xFFFFFFFFu;
 
-template <int T>
-__device__ void walk_links(const BatchParams& bp, const MemberDesc& md, uint32_t start, uint32_t cnt, WalkLinks& w) {
-    const uint32_t n = md.len;
-    const uint32_t* ppg = bp.pp + md.in_off + start;
-    for (uint32_t i = threadIdx.x; i < cnt; i += T) w.pps[i] = ppg[i];
-    if (threadIdx.x == 0) w.pps[cnt] = (start + cnt < n) ? ppg[cnt] : 0u;
-    for (uint32_t i = cnt + threadIdx.x; i < cnt + GPZ_EXITS; i += T) {
-        w.J[0][i] = (uint16_t)i;
-        w.J[1][i] = (uint16_t)i;
-    }
-    __syncthreads();
-    for (uint32_t i = threadIdx.x; i < cnt; i += T) {
-        const uint32_t l = w.pps[i] >> 16;
-        uint32_t nx = i + 1u;
-        if (l) {
-            const uint32_t l1 = w.pps[i + 1] >> 16;
-            const bool demote = (start + i + 1u < n) && l1 != 0u && l1 > l;  // lz77.rs:273-278
-            if (!demote) nx = i + l;
-        }
-        w.nxt[i] = (uint16_t)nx;
-        w.J[0][i] = (uint16_t)nx;
-    }
-    __syncthreads();
+// next(p) (lz77.rs:266-282): a literal advances by one; a match advances by
+// its length unless pp[p+1] is a longer match (lazy demotion to a literal).
+__device__ __forceinline__ uint32_t walk_next(uint32_t i, uint32_t v, uint32_t v1, bool has_next) {
+    const uint32_t l = v >> 16;
+    if (!l) return i + 1u;
+    const uint32_t l1 = v1 >> 16;
+    return (has_next && l1 != 0u && l1 > l) ? i + 1u : i + l;
 }
 
+// Warp-per-tile exit tables.  For position p of a full tile, exit(p) is
+// next(p) - 4096 if next(p) leaves the tile, else exit(next(p)); windows are
+// resolved from the top, so every link that leaves a window lands on a
+// position whose exit is known.  A link reaches at most 258 ahead, so only
+// the last 16 windows of exits are kept (ring of 512 per warp).
 template <int T>
 __global__ void __launch_bounds__(T) k_walk_exit(BatchParams bp) {
-    __shared__ WalkLinks w;
-    __shared__ uint32_t s_tile;
-    const int tid = threadIdx.x;
+    constexpr int W = T / 32;
+    constexpr uint32_t kRing = 512;
+    __shared__ uint16_t ring[W][kRing];
+    const int lane = threadIdx.x & 31;
+    uint16_t* ex = ring[threadIdx.x >> 5];
     const uint32_t ntiles = bp.dims[0];
     for (;;) {
-        __syncthreads();
-        if (tid == 0) s_tile = atomicAdd(&bp.counters[GPZ_CNT_EXIT], 1u);
-        __syncthreads();
-        const uint32_t t = s_tile;
+        uint32_t t = 0;
+        if (lane == 0) t = atomicAdd(&bp.counters[GPZ_CNT_EXIT], 1u);
+        t = __shfl_sync(kFull, t, 0);
         if (t >= ntiles) break;
         const TileDesc td = bp.tiles[t];
         const MemberDesc md = bp.members[td.member];
         if (td.seg + 1u == md.ntiles) continue;  // the member's last tile has no successor
-        const uint32_t start = td.seg << GPZ_SEG_LOG2, cnt = GPZ_SEG;
-        walk_links<T>(bp, md, start, cnt, w);
-        int cur = 0;
-        for (int r = 0; r < 16; r++) {
-            int ch = 0;
-            for (uint32_t i = tid; i < cnt; i += T) {
-                const uint32_t j = w.J[cur][i];
-                const uint32_t nj = j < cnt ? w.J[cur][j] : j;
-                w.J[cur ^ 1][i] = (uint16_t)nj;
-                ch |= nj != j;
+        // not the last tile: it is full and pp[4096] (the next tile's first
+        // position) exists
+        constexpr uint32_t cnt = GPZ_SEG;
+        const uint32_t* ppg = bp.pp + md.in_off + (td.seg << GPZ_SEG_LOG2);
+        uint32_t above = ppg[cnt];                  // pp just above the current window
+        uint32_t vnext = ppg[cnt - 32u + lane];     // the current window, prefetched
+        for (int base = (int)cnt - 32; base >= 0; base -= 32) {
+            const uint32_t v = vnext;
+            if (base >= 32) vnext = ppg[base - 32 + lane];
+            uint32_t v1 = __shfl_down_sync(kFull, v, 1);
+            if (lane == 31) v1 = above;
+            above = __shfl_sync(kFull, v, 0);
+            const uint32_t p = (uint32_t)base + lane;
+            const uint32_t nx = walk_next(p, v, v1, true);
+            uint32_t val = 0u, tgt = 32u;
+            if (nx >= cnt) val = nx - cnt;
+            else if (nx >= (uint32_t)base + 32u) val = ex[nx & (kRing - 1u)];
+            else tgt = nx - (uint32_t)base;
+#pragma unroll
+            for (int r = 0; r < 5; r++) {
+                const uint32_t pv = __shfl_sync(kFull, val, tgt & 31u);
+                const uint32_t pt = __shfl_sync(kFull, tgt, tgt & 31u);
+                if (tgt < 32u) {
+                    val = pv;
+                    tgt = pt;
+                }
             }
-            cur ^= 1;
-            if (!__syncthreads_or(ch)) break;
+            __syncwarp();
+            ex[p & (kRing - 1u)] = (uint16_t)val;
+            __syncwarp();
         }
-        for (int e = tid; e < GPZ_EXITS; e += T)
-            bp.tile_exit[(size_t)t * GPZ_EXITS + e] = (uint16_t)(w.J[cur][e] - cnt);
+        for (int e = lane; e < GPZ_EXITS; e += 32) bp.tile_exit[(size_t)t * GPZ_EXITS + e] = ex[e];
+        __syncwarp();
     }
 }
 
@@ -485,84 +538,86 @@ __global__ void k_chain(BatchParams bp) {
     }
 }
 
-struct MarkSmem {
-    WalkLinks w;
-    uint8_t mark[GPZ_SEG];
-    uint32_t hist[GPZ_NSYM];
-    uint32_t wsum[32];
-    uint32_t tile;
-};
-
+// Warp-per-tile forward walk from the tile's entry: per window of 32
+// positions (aligned), the lanes on the walk are found by doubling the links
+// from the entry lane; they emit their tokens in order (a demoted match
+// emits its literal byte) and count them in the warp's histogram; the walk
+// continues at the last one's next position.  The window after the current
+// one is prefetched, since the walk usually moves on to it.
 template <int T>
 __global__ void __launch_bounds__(T) k_walk_mark(BatchParams bp) {
-    constexpr int PER = GPZ_SEG / T;
-    __shared__ MarkSmem sm;
-    const int tid = threadIdx.x;
+    constexpr int W = T / 32;
+    __shared__ uint32_t hist_all[W][GPZ_NSYM];
+    const int lane = threadIdx.x & 31;
+    uint32_t* hist = hist_all[threadIdx.x >> 5];
     const uint32_t ntiles = bp.dims[0];
     for (;;) {
-        __syncthreads();
-        if (tid == 0) sm.tile = atomicAdd(&bp.counters[GPZ_CNT_MARK], 1u);
-        __syncthreads();
-        const uint32_t t = sm.tile;
+        uint32_t t = 0;
+        if (lane == 0) t = atomicAdd(&bp.counters[GPZ_CNT_MARK], 1u);
+        t = __shfl_sync(kFull, t, 0);
         if (t >= ntiles) break;
         const TileDesc td = bp.tiles[t];
         const MemberDesc md = bp.members[td.member];
         const uint32_t n = md.len, start = td.seg << GPZ_SEG_LOG2;
         const uint32_t cnt = min(GPZ_SEG, n - start);
-        for (int i = tid; i < GPZ_NSYM; i += T) sm.hist[i] = 0;
-        for (uint32_t i = tid; i < cnt; i += T) sm.mark[i] = 0xFF;
-        walk_links<T>(bp, md, start, cnt, sm.w);
-        const uint32_t entry = bp.tile_entry[t];
-        if (tid == 0 && entry < cnt) sm.mark[entry] = 0;
-        __syncthreads();
-        // before round r the marked positions are next^k(entry), k < 2^r
-        int cur = 0;
-        for (int r = 0; r < 16; r++) {
-            int add = 0;
-            for (uint32_t i = tid; i < cnt; i += T) {
-                const uint32_t j = sm.w.J[cur][i];
-                if (sm.mark[i] <= (uint32_t)r && j < cnt) {
-                    sm.mark[j] = (uint8_t)(r + 1);
-                    add = 1;
-                }
-                sm.w.J[cur ^ 1][i] = (uint16_t)(j < cnt ? sm.w.J[cur][j] : j);
-            }
-            cur ^= 1;
-            if (!__syncthreads_or(add)) break;
-        }
-
-        // compact the visited tokens in order, histogram their symbols
-        uint32_t vis = 0, c = 0;
-        const uint32_t i0 = tid * PER;
-#pragma unroll
-        for (int k = 0; k < PER; k++) {
-            const uint32_t i = i0 + k;
-            const bool v = i < cnt && sm.mark[i] != 0xFF;
-            vis |= (uint32_t)v << k;
-            c += v;
-        }
-        uint32_t total;
-        uint32_t idx = block_excl_scan<T>(c, sm.wsum, &total);
+        const uint32_t* ppg = bp.pp + md.in_off + start;
+        const uint8_t* ing = bp.in + md.in_off + start;
         uint32_t* tg = bp.tok + md.in_off + start;
-#pragma unroll
-        for (int k = 0; k < PER; k++) {
-            if (!((vis >> k) & 1u)) continue;
-            const uint32_t i = i0 + k;
-            uint32_t tv = sm.w.pps[i];
-            const uint32_t l = tv >> 16;
-            if (l && sm.w.nxt[i] == i + 1u) tv = bp.in[md.in_off + start + i];  // lazy demotion to a literal
-            tg[idx++] = tv;
-            if ((tv >> 16) == 0) {
-                atomicAdd(&sm.hist[tv & 0xFFu], 1u);
-            } else {
-                atomicAdd(&sm.hist[257u + len_row(tv >> 16)], 1u);
-                atomicAdd(&sm.hist[GPZ_NLIT + dist_row(tv & 0xFFFFu)], 1u);
+        // pp one past the tile: the next tile's first position, if any
+        const uint32_t past = (start + cnt < n) ? ppg[cnt] : 0u;
+        for (int s = lane; s < GPZ_NSYM; s += 32) hist[s] = 0u;
+        __syncwarp();
+        uint32_t cur = bp.tile_entry[t];
+        uint32_t ntok = 0;
+        uint32_t wbase = 0xFFFFFFFFu, v = 0u, vn = 0u;
+        while (cur < cnt) {
+            const uint32_t base = cur & ~31u;
+            if (base != wbase) {
+                if (base == wbase + 32u) {
+                    v = vn;
+                } else {
+                    const uint32_t q = base + lane;
+                    v = q < cnt ? ppg[q] : 0u;
+                }
+                wbase = base;
+                const uint32_t qn = base + 32u + lane;
+                vn = qn < cnt ? ppg[qn] : 0u;
             }
+            const uint32_t p = base + lane;
+            uint32_t v1 = __shfl_down_sync(kFull, v, 1);
+            const uint32_t vn0 = __shfl_sync(kFull, vn, 0);
+            if (lane == 31) v1 = base + 32u < cnt ? vn0 : past;
+            const bool inb = p < cnt;
+            const uint32_t nx = walk_next(p, v, v1, start + p + 1u < n);
+            // lanes on the walk in this window: doubling from the entry lane
+            uint32_t S = 1u << (cur - base);
+            uint32_t J = (inb && nx < base + 32u && nx < cnt) ? nx - base : 32u;
+#pragma unroll
+            for (int r = 0; r < 5; r++) {
+                const bool in = (S >> lane) & 1u;
+                S |= __reduce_or_sync(kFull, (in && J < 32u) ? (1u << J) : 0u);
+                const uint32_t Jp = __shfl_sync(kFull, J, J & 31u);
+                J = J < 32u ? Jp : 32u;
+            }
+            if ((S >> lane) & 1u) {
+                uint32_t tv = v;
+                if ((v >> 16) && nx == p + 1u) tv = ing[p];  // lazy demotion to a literal
+                tg[ntok + __popc(S & ((1u << lane) - 1u))] = tv;
+                if ((tv >> 16) == 0u) {
+                    atomicAdd(&hist[tv & 0xFFu], 1u);
+                } else {
+                    atomicAdd(&hist[257u + len_row(tv >> 16)], 1u);
+                    atomicAdd(&hist[GPZ_NLIT + dist_row(tv & 0xFFFFu)], 1u);
+                }
+            }
+            ntok += __popc(S);
+            cur = __shfl_sync(kFull, nx, 31 - __clz(S));  // next of the last lane on the walk
         }
-        __syncthreads();
+        __syncwarp();
         uint16_t* hg = bp.tile_hist + (size_t)t * GPZ_NSYM;
-        for (int s = tid; s < GPZ_NSYM; s += T) hg[s] = (uint16_t)sm.hist[s];
-        if (tid == 0) bp.tile_ntok[t] = total;
+        for (int s = lane; s < GPZ_NSYM; s += 32) hg[s] = (uint16_t)hist[s];
+        if (lane == 0) bp.tile_ntok[t] = ntok;
+        __syncwarp();
     }
 }
 

@@ -186,6 +186,8 @@ struct Slot {
     size_t h_err_cap = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t done = nullptr;
+    cudaEvent_t tv[3] = {nullptr, nullptr, nullptr};  // before the upload, after it, after the kernels
+    float last_h2d_ms = 0, last_kernel_ms = 0;          // of the last batch waited for
     cudaEvent_t ev[GPZ_STAGES + 1] = {};
     uint64_t gen = 1;  // bumps whenever a buffer the graphs capture moves
     struct Graph {
@@ -250,11 +252,13 @@ int fail(gpz_ctx* c, int code, const char* what, cudaError_t e = cudaSuccess) {
         if (_e != cudaSuccess) return fail((ctx), GPZ_E_CUDA, #call, _e); \
     } while (0)
 
-int ensure_dev(gpz_ctx* c, Slot& sl, DevArena& a, size_t bytes) {
+// capped: the growth counts against the context's pool cap (the serving
+// engine's fixed arenas, sized once at start, do not).
+int ensure_dev(gpz_ctx* c, Slot& sl, DevArena& a, size_t bytes, bool capped = true) {
     bytes = round_up(std::max<size_t>(bytes, 256), 256);
     if (a.cap >= bytes) return GPZ_OK;
     size_t grow = std::max(bytes, a.cap + a.cap / 2);
-    if (c->pool_used - a.cap + grow > c->pool_cap) {
+    if (capped && c->pool_used - a.cap + grow > c->pool_cap) {
         grow = bytes;
         if (c->pool_used - a.cap + grow > c->pool_cap) return fail(c, GPZ_E_ADMISSION, "device pool cap exceeded");
     }
@@ -336,34 +340,58 @@ size_t desc_bytes(size_t nm, size_t nt) { return kDescHeader + nm * sizeof(Membe
 // bump the slot's generation), so a captured graph stays valid for any batch
 // that fits them.
 
-// Sizes every device array (and the pinned staging) for the planned batch.
-int reserve(gpz_ctx* c, Slot& sl, size_t in_bytes, bool own_in, bool own_out, size_t out_bytes) {
-    const size_t nm = std::max<size_t>(sl.members.size(), 1), nt = std::max<size_t>(sl.tiles.size(), 1);
+// Sizes every device array (and the pinned descriptor / member-table
+// staging) for a batch of in_bytes input, nm members and nt tiles.  Arrays
+// only grow; a growth frees the old array (cudaFree synchronises the device)
+// and bumps the slot's generation.
+int reserve_counts(gpz_ctx* c, Slot& sl, size_t in_bytes, size_t nm, size_t nt, bool own_in, bool own_out,
+                   size_t out_bytes, bool capped = true) {
+    nm = std::max<size_t>(nm, 1);
+    nt = std::max<size_t>(nt, 1);
     int rc;
-    if (own_in && (rc = ensure_dev(c, sl, sl.d_in, in_bytes + 64))) return rc;
-    if ((rc = ensure_dev(c, sl, sl.d_pp, in_bytes * 4 + 64))) return rc;
-    if ((rc = ensure_dev(c, sl, sl.d_tok, in_bytes * 4 + 64))) return rc;
-    if (own_out && (rc = ensure_dev(c, sl, sl.d_out, out_bytes + 64))) return rc;
-    if ((rc = ensure_dev(c, sl, sl.d_skeys, nt * GPZ_SEG * 2))) return rc;
-    if ((rc = ensure_dev(c, sl, sl.d_son, nt * GPZ_SEG * 4))) return rc;
-    if ((rc = ensure_dev(c, sl, sl.d_sposid, nt * GPZ_SEG * 2))) return rc;
-    if ((rc = ensure_dev(c, sl, sl.d_snkeys, nt * 4))) return rc;
-    if ((rc = ensure_dev(c, sl, sl.d_tentry, nt * 4))) return rc;
-    if ((rc = ensure_dev(c, sl, sl.d_texit, nt * GPZ_EXITS * 2))) return rc;
-    if ((rc = ensure_dev(c, sl, sl.d_thist, nt * GPZ_NSYM * 2))) return rc;
-    if ((rc = ensure_dev(c, sl, sl.d_tntok, nt * 4))) return rc;
-    if ((rc = ensure_dev(c, sl, sl.d_tbit, nt * 4))) return rc;
-    if ((rc = ensure_dev(c, sl, sl.d_mcodes, nm * GPZ_NSYM * 4))) return rc;
-    if ((rc = ensure_dev(c, sl, sl.d_mhdr, nm * GPZ_HDR_WORDS * 4))) return rc;
-    if ((rc = ensure_dev(c, sl, sl.d_mout, nm * sizeof(MemberOut)))) return rc;
-    if ((rc = ensure_dev(c, sl, sl.d_cnt, GPZ_NCOUNTERS * 4 + 64))) return rc;
-    if ((rc = ensure_dev(c, sl, sl.d_members, nm * sizeof(MemberDesc)))) return rc;
-    if ((rc = ensure_dev(c, sl, sl.d_tiles, nt * sizeof(TileDesc)))) return rc;
-    if ((rc = ensure_dev(c, sl, sl.d_dims, kDescHeader))) return rc;
+    if (own_in && (rc = ensure_dev(c, sl, sl.d_in, in_bytes + 64, capped))) return rc;
+    if ((rc = ensure_dev(c, sl, sl.d_pp, in_bytes * 4 + 64, capped))) return rc;
+    if ((rc = ensure_dev(c, sl, sl.d_tok, in_bytes * 4 + 64, capped))) return rc;
+    if (own_out && (rc = ensure_dev(c, sl, sl.d_out, out_bytes + 64, capped))) return rc;
+    if ((rc = ensure_dev(c, sl, sl.d_skeys, nt * GPZ_SEG * 2, capped))) return rc;
+    if ((rc = ensure_dev(c, sl, sl.d_son, nt * GPZ_SEG * 4, capped))) return rc;
+    if ((rc = ensure_dev(c, sl, sl.d_sposid, nt * GPZ_SEG * 2, capped))) return rc;
+    if ((rc = ensure_dev(c, sl, sl.d_snkeys, nt * 4, capped))) return rc;
+    if ((rc = ensure_dev(c, sl, sl.d_tentry, nt * 4, capped))) return rc;
+    if ((rc = ensure_dev(c, sl, sl.d_texit, nt * GPZ_EXITS * 2, capped))) return rc;
+    if ((rc = ensure_dev(c, sl, sl.d_thist, nt * GPZ_NSYM * 2, capped))) return rc;
+    if ((rc = ensure_dev(c, sl, sl.d_tntok, nt * 4, capped))) return rc;
+    if ((rc = ensure_dev(c, sl, sl.d_tbit, nt * 4, capped))) return rc;
+    if ((rc = ensure_dev(c, sl, sl.d_mcodes, nm * GPZ_NSYM * 4, capped))) return rc;
+    if ((rc = ensure_dev(c, sl, sl.d_mhdr, nm * GPZ_HDR_WORDS * 4, capped))) return rc;
+    if ((rc = ensure_dev(c, sl, sl.d_mout, nm * sizeof(MemberOut), capped))) return rc;
+    if ((rc = ensure_dev(c, sl, sl.d_cnt, GPZ_NCOUNTERS * 4 + 64, capped))) return rc;
+    if ((rc = ensure_dev(c, sl, sl.d_members, nm * sizeof(MemberDesc), capped))) return rc;
+    if ((rc = ensure_dev(c, sl, sl.d_tiles, nt * sizeof(TileDesc), capped))) return rc;
+    if ((rc = ensure_dev(c, sl, sl.d_dims, kDescHeader, capped))) return rc;
     if ((rc = ensure_host(c, sl, sl.h_desc, sl.h_desc_cap, desc_bytes(nm, nt), false))) return rc;
     if ((rc = ensure_host(c, sl, sl.h_mout, sl.h_mout_cap, nm, true))) return rc;
     if ((rc = ensure_host(c, sl, sl.h_err, sl.h_err_cap, 16, true))) return rc;
     return GPZ_OK;
+}
+
+// Sizes the slot for its planned batch.
+int reserve(gpz_ctx* c, Slot& sl, size_t in_bytes, bool own_in, bool own_out, size_t out_bytes) {
+    return reserve_counts(c, sl, in_bytes, sl.members.size(), sl.tiles.size(), own_in, own_out, out_bytes);
+}
+
+// Sizes the slot once for every batch of at most max_bytes input in at most
+// max_items items (all arrays, pinned input staging and mapped output), so
+// that no batch within those limits allocates or frees anything.
+int reserve_limits(gpz_ctx* c, Slot& sl, size_t max_bytes, size_t max_items) {
+    const size_t in_bytes = max_bytes + 16 * max_items + 64;
+    const size_t nm = max_bytes / c->member_bytes + max_items;
+    const size_t nt = max_bytes / GPZ_SEG + max_items;
+    const size_t out_bytes = nm * member_bound(0) + 2 * max_bytes;
+    int rc;
+    if ((rc = reserve_counts(c, sl, in_bytes, nm, nt, true, true, out_bytes, false))) return rc;
+    if ((rc = ensure_host(c, sl, sl.h_in, sl.h_in_cap, in_bytes + 64, false))) return rc;
+    return ensure_host(c, sl, sl.h_out, sl.h_out_cap, out_bytes + 64, true);
 }
 
 BatchParams params_of(Slot& sl, const uint8_t* d_in, uint8_t* d_out) {
@@ -514,8 +542,17 @@ void add_time(gpz_ctx* c, int k, double ms) {
     c->host_ms[k] += ms;
 }
 
+// How a batch is launched.
+struct LaunchPolicy {
+    bool exact = false;     // grids sized to this batch (one CTA per item), no graph
+    bool autotune = true;   // tune the bucket's shape on its first use
+    bool graphs = true;     // per-(slot, bucket) CUDA graph
+};
+constexpr LaunchPolicy kPolicyBatched{false, true, true};
+constexpr LaunchPolicy kPolicyPlain{true, false, false};
+
 // Plans, uploads and launches one batch of host items on a slot (no wait).
-int submit_slot(gpz_ctx* c, Slot& sl, const gpz_desc* d, size_t count, bool plain) {
+int submit_slot(gpz_ctx* c, Slot& sl, const gpz_desc* d, size_t count, const LaunchPolicy& pol) {
     double t0 = now_ms();
     sl.spans.assign(count, Span{});
     size_t in_bytes = 0;
@@ -542,14 +579,16 @@ int submit_slot(gpz_ctx* c, Slot& sl, const gpz_desc* d, size_t count, bool plai
     t0 = now_ms();
     add_time(c, 1, t0 - t1);
     cudaStream_t s = sl.stream;
+    CU(c, cudaEventRecord(sl.tv[0], s));
     CU(c, cudaMemcpyAsync(sl.d_in.p, sl.h_in, in_bytes, cudaMemcpyHostToDevice, s));
     if ((rc = upload_desc(c, sl, s))) return rc;
+    CU(c, cudaEventRecord(sl.tv[1], s));
     BatchParams bp = params_of(sl, static_cast<const uint8_t*>(sl.d_in.p), static_cast<uint8_t*>(sl.d_out.p));
     DrainTarget dt{mapped_dev(sl.h_out), mapped_dev(sl.h_mout), mapped_dev(sl.h_err), c->sms * 4};
     if (!dt.h_out || !dt.h_mout || !dt.h_err) return fail(c, GPZ_E_CUDA, "mapped host memory");
     sl.bucket = bucket_of(sl.tiles.size());
     const bool timing = (c->flags & GPZ_FLAG_STAGE_TIMING) != 0;
-    if (plain) {
+    if (pol.exact) {
         // one launch per kernel, grids sized to this batch, no graph
         const LaunchShape exact{1024, 0, 512, 0, 512, 0, 0, 0};
         rc = launch(c, sl, bp, exact, false, &dt, timing, s);
@@ -559,13 +598,14 @@ int submit_slot(gpz_ctx* c, Slot& sl, const gpz_desc* d, size_t count, bool plai
             std::lock_guard<std::mutex> lk(c->tune_mu);
             tuned = c->tuned[sl.bucket];
         }
-        if (!tuned && !(c->flags & GPZ_FLAG_NO_AUTOTUNE) && !c->fixed.lookup_threads &&
+        if (pol.autotune && !tuned && !(c->flags & GPZ_FLAG_NO_AUTOTUNE) && !c->fixed.lookup_threads &&
             (rc = autotune(c, sl, bp, &dt, s)))
             return rc;
-        const bool graphs = !(c->flags & GPZ_FLAG_NO_GRAPHS) && !timing;
+        const bool graphs = pol.graphs && !(c->flags & GPZ_FLAG_NO_GRAPHS) && !timing;
         rc = launch(c, sl, bp, shape_for(c, sl.bucket), graphs, &dt, timing, s);
     }
     if (rc) return rc;
+    CU(c, cudaEventRecord(sl.tv[2], s));
     CU(c, cudaEventRecord(sl.done, s));
     sl.busy = true;
     add_time(c, 2, now_ms() - t0);
@@ -595,6 +635,8 @@ int wait_slot(gpz_ctx* c, Slot& sl) {
     const double t0 = now_ms();
     CU(c, cudaEventSynchronize(sl.done));
     add_time(c, 3, now_ms() - t0);
+    cudaEventElapsedTime(&sl.last_h2d_ms, sl.tv[0], sl.tv[1]);
+    cudaEventElapsedTime(&sl.last_kernel_ms, sl.tv[1], sl.tv[2]);
     if (c->flags & GPZ_FLAG_STAGE_TIMING)
         for (int i = 0; i < GPZ_STAGES; i++) cudaEventElapsedTime(&c->stage_ms[i], sl.ev[i], sl.ev[i + 1]);
     const uint32_t err = *sl.h_err;
@@ -662,7 +704,7 @@ int run_host_items(gpz_ctx* c, const gpz_desc* d, size_t count, gpz_out* outs, b
         const int k = plain ? 0 : c->next_slot;
         settle(k);
         if (fatal) break;
-        int rc = submit_slot(c, c->slots[k], d + i, j - i, plain);
+        int rc = submit_slot(c, c->slots[k], d + i, j - i, plain ? kPolicyPlain : kPolicyBatched);
         if (rc) {
             for (size_t q = i; q < j; q++) outs[q].status = rc;
             fatal = rc;
@@ -677,9 +719,11 @@ int run_host_items(gpz_ctx* c, const gpz_desc* d, size_t count, gpz_out* outs, b
     return fatal != GPZ_OK ? fatal : first_bad;
 }
 
-int init_slot(gpz_ctx* c, Slot& sl) {
-    CU(c, cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking));
+// priority: a CUDA stream priority (lower is more urgent; 0 is the default)
+int init_slot(gpz_ctx* c, Slot& sl, int priority = 0) {
+    CU(c, cudaStreamCreateWithPriority(&sl.stream, cudaStreamNonBlocking, priority));
     CU(c, cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
+    for (auto& e : sl.tv) CU(c, cudaEventCreate(&e));
     if (c->flags & GPZ_FLAG_STAGE_TIMING)
         for (auto& e : sl.ev) CU(c, cudaEventCreate(&e));
     return ensure_host(c, sl, sl.h_err, sl.h_err_cap, 16, true);
@@ -703,6 +747,8 @@ void free_slot(gpz_ctx* c, Slot& sl) {
     for (auto& e : sl.ev)
         if (e) cudaEventDestroy(e);
     if (sl.done) cudaEventDestroy(sl.done);
+    for (auto& e : sl.tv)
+        if (e) cudaEventDestroy(e);
     if (sl.stream) cudaStreamDestroy(sl.stream);
 }
 
@@ -732,48 +778,87 @@ struct Unit {
 
 }  // namespace
 
-// Continuous batching: requests are cut into 2 MiB units (whole members).
-// A launcher thread forms a batch whenever a pipeline slot is free -- units
-// of requests of at most 1 MiB first, then the rest in arrival order, up to
-// the batch cap -- and launches it while the other slots' batches are still
-// on the device; a completer thread retires finished batches in launch order
-// (framing, copies into the requests).  A request completes when its last
-// unit does, and its gzip stream is its units' members in order: byte for
-// byte what gpz_compress_chunk returns for it alone.  Admission: a request is
-// rejected (GPZ_E_BUSY) while the bytes queued or on the device would exceed
-// the pool cap.
+// Continuous batching over two lanes.  Requests of at most 1 MiB go to the
+// small lane, larger ones (cut into 2 MiB units, whole members) to the large
+// lane.  Each lane has pipeline slots (three small, two large), a launcher
+// thread that forms a batch from the lane's queue (arrival order, up to the
+// lane's batch cap) whenever one of its slots is free and launches it while
+// the other slots' batches are still on the device, and a completer thread
+// that retires the lane's batches in launch order (framing, copies into the
+// requests).
+//
+// The lanes share the GPU through stream priorities: the small lane's
+// streams are the most urgent, and the large lane launches grids of one CTA
+// per tile (no persistent CTAs), so the small lane's CTAs take SMs as soon
+// as the large lane's current CTAs retire instead of waiting for whole
+// kernels.  Every slot is sized once at start for its lane's batch limits,
+// so serving never allocates or frees device memory (cudaFree would
+// synchronise the device).
+//
+// A request completes when its last unit does; its gzip stream is its
+// units' members in order: byte for byte what gpz_compress_chunk returns for
+// it alone.  Admission: a request is rejected (GPZ_E_BUSY) while the bytes
+// queued or on the device would exceed the pool cap.
 struct ServeEngine {
-    static constexpr int kSlots = 3;
     static constexpr size_t kUnit = 2u << 20;
     static constexpr size_t kSmall = 1u << 20;
+    static constexpr int kLaneSlots = 3;
+
+    struct Lane {
+        int nslots = 2;         // pipeline slots in use (at most kLaneSlots)
+        size_t batch_cap = 0;   // input bytes per batch
+        size_t max_units = 0;   // units per batch
+        LaunchPolicy pol;
+        Slot slots[kLaneSlots];
+        bool slot_free[kLaneSlots] = {true, true, true};
+        std::vector<Unit> inflight[kLaneSlots];
+        int launch_rc[kLaneSlots] = {0, 0, 0};
+        std::deque<Unit> q;
+        std::deque<int> inflight_q;  // slots in launch order
+        std::condition_variable cv_work, cv_inflight;
+        std::thread launcher, completer;
+        double t_launch[kLaneSlots] = {0, 0, 0}, t_submitted[kLaneSlots] = {0, 0, 0};
+        gpz_lane_stats st{};  // guarded by the engine mutex
+    };
 
     gpz_ctx* c = nullptr;
-    Slot slots[kSlots];
-    std::thread launcher, completer;
+    Lane lanes[2];  // 0: requests <= 1 MiB, 1: larger
     std::mutex mu;
-    std::condition_variable cv_work, cv_done, cv_inflight, cv_free;
-    std::deque<Unit> small_q, large_q;
-    std::deque<int> inflight_q;  // slots in launch order
-    bool slot_free[kSlots] = {true, true, true};
+    std::condition_variable cv_done;
     std::unordered_map<uint64_t, std::shared_ptr<Request>> reqs;
     uint64_t next_id = 1;
     bool stop = false;
     size_t queued_bytes = 0;
-    size_t batch_cap = 16u << 20;
     std::vector<double> lat_all, lat_small;
     uint64_t rejected = 0, batches = 0, bytes_in = 0, bytes_out = 0;
     double max_queue_ms = 0;
-    std::vector<Unit> inflight[kSlots];
 
     int start(gpz_ctx* ctx) {
         c = ctx;
         cudaSetDevice(c->device);
-        for (auto& s : slots) {
-            const int rc = init_slot(c, s);
-            if (rc) return rc;
+        int least = 0, greatest = 0;
+        cudaDeviceGetStreamPriorityRange(&least, &greatest);
+        Lane& sm = lanes[0];
+        sm.nslots = 3;
+        sm.batch_cap = 4u << 20;
+        sm.max_units = 1024;
+        sm.pol = LaunchPolicy{false, false, true};  // persistent default shape, graphs, no tuning pass
+        Lane& lg = lanes[1];
+        lg.nslots = 2;
+        lg.batch_cap = 16u << 20;
+        lg.max_units = 16;
+        lg.pol = LaunchPolicy{true, false, false};  // one CTA per tile
+        for (int l = 0; l < 2; l++)
+            for (int k = 0; k < lanes[l].nslots; k++) {
+                Slot& s = lanes[l].slots[k];
+                int rc = init_slot(c, s, l == 0 ? greatest : least);
+                if (!rc) rc = reserve_limits(c, s, lanes[l].batch_cap, lanes[l].max_units);
+                if (rc) return rc;
+            }
+        for (auto& L : lanes) {
+            L.launcher = std::thread([this, &L] { launch_loop(L); });
+            L.completer = std::thread([this, &L] { complete_loop(L); });
         }
-        launcher = std::thread([this] { launch_loop(); });
-        completer = std::thread([this] { complete_loop(); });
         return GPZ_OK;
     }
 
@@ -782,12 +867,16 @@ struct ServeEngine {
             std::lock_guard<std::mutex> lk(mu);
             stop = true;
         }
-        cv_work.notify_all();
-        cv_inflight.notify_all();
-        cv_free.notify_all();
-        if (launcher.joinable()) launcher.join();
-        if (completer.joinable()) completer.join();
-        for (auto& s : slots) free_slot(c, s);
+        for (auto& L : lanes) {
+            L.cv_work.notify_all();
+            L.cv_inflight.notify_all();
+        }
+        for (auto& L : lanes) {
+            if (L.launcher.joinable()) L.launcher.join();
+            if (L.completer.joinable()) L.completer.join();
+        }
+        for (auto& L : lanes)
+            for (auto& s : L.slots) free_slot(c, s);
     }
 
     int submit(const gpz_desc* d, uint64_t* ticket, bool copy) {
@@ -811,15 +900,14 @@ struct ServeEngine {
             r->src = d->in;  // the caller keeps it alive until the result is polled
         }
         r->n = d->n;
+        Lane& L = lanes[r->small ? 0 : 1];
         std::lock_guard<std::mutex> lk(mu);
         r->id = next_id++;
-        for (size_t u = 0; u < r->units; u++) {
-            const Unit un{r, u, u * kUnit, std::min(kUnit, d->n - std::min(d->n, u * kUnit))};
-            (r->small ? small_q : large_q).push_back(un);
-        }
+        for (size_t u = 0; u < r->units; u++)
+            L.q.push_back(Unit{r, u, u * kUnit, std::min(kUnit, d->n - std::min(d->n, u * kUnit))});
         reqs[r->id] = r;
         *ticket = r->id;
-        cv_work.notify_one();
+        L.cv_work.notify_one();
         return GPZ_OK;
     }
 
@@ -855,83 +943,87 @@ struct ServeEngine {
         return GPZ_OK;
     }
 
-    // The next batch of units, small requests first (caller holds mu).
-    std::vector<Unit> take_batch() {
+    // The lane's next batch, in arrival order (caller holds mu).
+    static std::vector<Unit> take_batch(Lane& L) {
         std::vector<Unit> b;
         size_t bytes = 0;
-        for (auto* q : {&small_q, &large_q}) {
-            while (!q->empty() && (b.empty() || bytes + q->front().n <= batch_cap)) {
-                bytes += q->front().n;
-                b.push_back(q->front());
-                q->pop_front();
-            }
+        while (!L.q.empty() && b.size() < L.max_units && (b.empty() || bytes + L.q.front().n <= L.batch_cap)) {
+            bytes += L.q.front().n;
+            b.push_back(L.q.front());
+            L.q.pop_front();
         }
         return b;
     }
 
-    void launch_loop() {
+    static int free_slot_of(const Lane& L) {
+        for (int i = 0; i < L.nslots; i++)
+            if (L.slot_free[i]) return i;
+        return -1;
+    }
+
+    void launch_loop(Lane& L) {
         cudaSetDevice(c->device);
         for (;;) {
             int k = -1;
             std::vector<Unit> batch;
             {
                 std::unique_lock<std::mutex> lk(mu);
-                cv_free.wait(lk, [&] {
-                    if (stop) return true;
-                    for (int i = 0; i < kSlots; i++)
-                        if (slot_free[i]) return true;
-                    return false;
-                });
-                cv_work.wait(lk, [&] { return stop || !small_q.empty() || !large_q.empty(); });
+                L.cv_work.wait(lk, [&] { return stop || (!L.q.empty() && free_slot_of(L) >= 0); });
                 if (stop) return;
-                for (int i = 0; i < kSlots; i++)
-                    if (slot_free[i]) {
-                        k = i;
-                        break;
-                    }
-                if (k < 0) continue;
-                batch = take_batch();
-                if (batch.empty()) continue;
-                slot_free[k] = false;
-                max_queue_ms = std::max(max_queue_ms, now_ms() - batch.front().req->t_arrive);
+                k = free_slot_of(L);
+                batch = take_batch(L);
+                L.slot_free[k] = false;
+                const double tl = now_ms(), q = tl - batch.front().req->t_arrive;
+                max_queue_ms = std::max(max_queue_ms, q);
+                L.st.queue_ms += q;
+                L.st.max_queue_ms = std::max(L.st.max_queue_ms, q);
+                L.t_launch[k] = tl;
             }
             std::vector<gpz_desc> ds(batch.size());
             for (size_t i = 0; i < batch.size(); i++)
                 ds[i] = gpz_desc{batch[i].req->src + batch[i].off, batch[i].n, 0};
-            inflight[k] = std::move(batch);
-            const int rc = submit_slot(c, slots[k], ds.data(), ds.size(), false);
+            L.inflight[k] = std::move(batch);
+            const int rc = submit_slot(c, L.slots[k], ds.data(), ds.size(), L.pol);
             std::lock_guard<std::mutex> lk(mu);
+            L.t_submitted[k] = now_ms();
+            L.st.submit_ms += L.t_submitted[k] - L.t_launch[k];
             if (rc == GPZ_OK) batches++;
-            else slots[k].busy = false;
-            launch_rc[k] = rc;
-            inflight_q.push_back(k);
-            cv_inflight.notify_one();
+            else L.slots[k].busy = false;
+            L.launch_rc[k] = rc;
+            L.inflight_q.push_back(k);
+            L.cv_inflight.notify_one();
         }
     }
 
-    void complete_loop() {
+    void complete_loop(Lane& L) {
         cudaSetDevice(c->device);
         for (;;) {
             int k;
             {
                 std::unique_lock<std::mutex> lk(mu);
-                cv_inflight.wait(lk, [&] { return (stop && inflight_q.empty()) || !inflight_q.empty(); });
-                if (inflight_q.empty()) return;
-                k = inflight_q.front();
-                inflight_q.pop_front();
+                L.cv_inflight.wait(lk, [&] { return stop || !L.inflight_q.empty(); });
+                if (L.inflight_q.empty()) return;
+                k = L.inflight_q.front();
+                L.inflight_q.pop_front();
             }
-            int rc = launch_rc[k];
-            if (rc == GPZ_OK) rc = wait_slot(c, slots[k]);
-            complete(k, rc);
+            int rc = L.launch_rc[k];
+            if (rc == GPZ_OK) rc = wait_slot(c, L.slots[k]);
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                L.st.wait_ms += now_ms() - L.t_submitted[k];
+                L.st.h2d_ms += L.slots[k].last_h2d_ms;
+                L.st.kernel_ms += L.slots[k].last_kernel_ms;
+            }
+            complete(L, k, rc);
             std::lock_guard<std::mutex> lk(mu);
-            slot_free[k] = true;
-            cv_free.notify_one();
+            L.slot_free[k] = true;
+            L.cv_work.notify_one();
         }
     }
 
-    void complete(int k, int rc) {
-        Slot& sl = slots[k];
-        std::vector<Unit>& units = inflight[k];
+    void complete(Lane& L, int k, int rc) {
+        Slot& sl = L.slots[k];
+        std::vector<Unit>& units = L.inflight[k];
         const double t0 = now_ms();
         std::vector<std::vector<uint8_t>> outs(units.size());
         if (rc == GPZ_OK) {
@@ -946,6 +1038,11 @@ struct ServeEngine {
         const double t = now_ms();
         add_time(c, 4, t - t0);
         std::lock_guard<std::mutex> lk(mu);
+        L.st.complete_ms += t - t0;
+        L.st.batches++;
+        L.st.units += units.size();
+        for (auto& u : units) L.st.bytes += u.n;
+        L.st.max_batch_ms = std::max(L.st.max_batch_ms, t - L.t_launch[k]);
         for (size_t i = 0; i < units.size(); i++) {
             auto& r = units[i].req;
             queued_bytes -= units[i].n;
@@ -968,8 +1065,6 @@ struct ServeEngine {
         units.clear();
         cv_done.notify_all();
     }
-
-    int launch_rc[kSlots] = {0, 0, 0};
 
     static double pct(std::vector<double> v, double q) {
         if (v.empty()) return 0;
@@ -1226,10 +1321,20 @@ int gpz_serve_stats_get(gpz_ctx* c, gpz_serve_stats* st) {
     return GPZ_OK;
 }
 
+int gpz_serve_lane_stats(gpz_ctx* c, int lane, gpz_lane_stats* st) {
+    if (!c || !st || lane < 0 || lane > 1) return GPZ_E_ARG;
+    std::memset(st, 0, sizeof *st);
+    if (!c->serve) return GPZ_OK;
+    std::lock_guard<std::mutex> lk(c->serve->mu);
+    *st = c->serve->lanes[lane].st;
+    return GPZ_OK;
+}
+
 int gpz_serve_reset_stats(gpz_ctx* c) {
     if (!c) return GPZ_E_ARG;
     if (!c->serve) return GPZ_OK;
     std::lock_guard<std::mutex> lk(c->serve->mu);
+    for (auto& L : c->serve->lanes) L.st = gpz_lane_stats{};
     c->serve->lat_all.clear();
     c->serve->lat_small.clear();
     c->serve->rejected = c->serve->batches = c->serve->bytes_in = c->serve->bytes_out = 0;

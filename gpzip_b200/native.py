@@ -30,7 +30,7 @@ EXPORTS = [
     "gpz_compress_batch", "gpz_compress_batch_plain", "gpz_compress_device", "gpz_frame_host",
     "gpz_debug_chunk", "gpz_submit", "gpz_poll", "gpz_serve_stats_get", "gpz_strerror", "gpz_last_error",
     "gpz_get_shape", "gpz_set_shape", "gpz_last_launches", "gpz_stage_times", "gpz_compress_member_static",
-    "gpz_serve_reset_stats", "gpz_submit_ref", "gpz_host_times",
+    "gpz_serve_reset_stats", "gpz_submit_ref", "gpz_host_times", "gpz_serve_lane_stats",
 ]
 
 
@@ -66,6 +66,13 @@ class ServeStats(ctypes.Structure):
                 ("completed_small", ctypes.c_uint64), ("p50_small_ms", ctypes.c_double),
                 ("p99_small_ms", ctypes.c_double), ("p999_small_ms", ctypes.c_double),
                 ("queued_bytes", ctypes.c_uint64)]
+
+
+class LaneStats(ctypes.Structure):
+    _fields_ = [("batches", ctypes.c_uint64), ("units", ctypes.c_uint64), ("bytes", ctypes.c_uint64),
+                ("queue_ms", ctypes.c_double), ("submit_ms", ctypes.c_double), ("h2d_ms", ctypes.c_double),
+                ("kernel_ms", ctypes.c_double), ("wait_ms", ctypes.c_double), ("complete_ms", ctypes.c_double),
+                ("max_queue_ms", ctypes.c_double), ("max_batch_ms", ctypes.c_double)]
 
 
 _lib = None
@@ -112,6 +119,8 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.gpz_serve_reset_stats.restype = ctypes.c_int
     L.gpz_submit_ref.argtypes = [vp, ctypes.POINTER(Desc), ctypes.POINTER(ctypes.c_uint64)]
     L.gpz_submit_ref.restype = ctypes.c_int
+    L.gpz_serve_lane_stats.argtypes = [vp, ctypes.c_int, ctypes.POINTER(LaneStats)]
+    L.gpz_serve_lane_stats.restype = ctypes.c_int
     L.gpz_host_times.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.c_int]
     L.gpz_host_times.restype = ctypes.c_int
     L.gpz_strerror.argtypes = [ctypes.c_int]
@@ -297,6 +306,17 @@ class Context:
 
     def serve_reset_stats(self):
         self._check(self.L.gpz_serve_reset_stats(self._h), "gpz_serve_reset_stats")
+
+    def lane_stats(self, lane: int) -> dict:
+        """Per-lane serving breakdown (lane 0: requests <= 1 MiB); times are
+        per-batch means in ms, maxima per batch."""
+        s = LaneStats()
+        self._check(self.L.gpz_serve_lane_stats(self._h, lane, ctypes.byref(s)), "gpz_serve_lane_stats")
+        d = {f: getattr(s, f) for f, _ in LaneStats._fields_}
+        b = max(1, d["batches"])
+        for k in ("queue_ms", "submit_ms", "h2d_ms", "kernel_ms", "wait_ms", "complete_ms"):
+            d[k] = d[k] / b
+        return d
 
     def serve_stats(self) -> dict:
         s = ServeStats()

@@ -159,6 +159,22 @@ typedef struct gpz_serve_stats {
 GPZ_API int gpz_serve_stats_get(gpz_ctx* ctx, gpz_serve_stats* st);
 GPZ_API int gpz_serve_reset_stats(gpz_ctx* ctx);
 
+/* Where a serving lane's time goes, since the engine started or its
+ * statistics were last reset.  Lane 0 serves requests of at most 1 MiB,
+ * lane 1 the larger ones.  Times are ms summed over the lane's batches
+ * (divide by batches for means); the maxima are per batch. */
+typedef struct gpz_lane_stats {
+    uint64_t batches, units, bytes;
+    double queue_ms;     /* oldest unit: arrival to its batch's launch */
+    double submit_ms;    /* host: plan, staging copy, enqueue */
+    double h2d_ms;       /* device: input and descriptor upload */
+    double kernel_ms;    /* device: kernels and drain */
+    double wait_ms;      /* host: enqueue done to batch done */
+    double complete_ms;  /* host: framing and copies into the requests */
+    double max_queue_ms, max_batch_ms;  /* max_batch_ms: launch to completion */
+} gpz_lane_stats;
+GPZ_API int gpz_serve_lane_stats(gpz_ctx* ctx, int lane, gpz_lane_stats* st);
+
 GPZ_API const char* gpz_strerror(int status);
 
 /* Last CUDA / device diagnostic of this context (static storage). */
