@@ -24,6 +24,7 @@
 #define GPZ_ERRBIT_SPIN 1u      // a bounded wait expired
 #define GPZ_ERRBIT_BITS 2u      // emitted bit count disagreed with the plan
 #define GPZ_ERRBIT_HUFF 4u      // code construction failed (never expected)
+#define GPZ_ERRBIT_DESC 8u      // a fetched descriptor block exceeded the arenas
 
 struct MemberDesc {
     uint64_t in_off;     // first input byte of the member in the batch input (16-byte aligned)
@@ -109,11 +110,27 @@ struct DrainTarget {
     int grid;
 };
 
+// Host-mapped pinned sources of k_fetch: the descriptor block (64-byte
+// header: tiles, members, input bytes as u64 at byte 8; then the members and
+// the tiles) and the batch input, copied by the SMs into the device arenas
+// (no copy-engine transfer on the batch's path).  The capacities bound what
+// the header may ask for.
+struct FetchSource {
+    const uint8_t* h_desc;
+    const uint8_t* h_in;
+    uint32_t* d_dims;
+    MemberDesc* d_members;
+    TileDesc* d_tiles;
+    uint8_t* d_in;
+    uint64_t members_cap, tiles_cap, in_cap;
+};
+
 // Kernel launchers (gpz_kernels.cu).
-// events: NULL or 5 cudaEvent_t recorded before each stage and after the last.
+// events: NULL or GPZ_STAGES + 1 cudaEvent_t recorded at the stage boundaries.
 // drain: NULL, or where k_drain streams the output, member table and error.
+// fetch: NULL, or the mapped sources k_fetch copies in before the first stage.
 int gpz_launch_batch(const BatchParams& bp, const LaunchShape& ls, void* stream, void* const* events,
-                     const DrainTarget* drain);
+                     const DrainTarget* drain, const FetchSource* fetch = nullptr);
 // Persistent grid sizes (SMs x resident CTAs) for the shape's thread counts.
 int gpz_occupancy(LaunchShape* persistent);
 int gpz_kernel_smem_setup();

@@ -492,11 +492,14 @@ __global__ void __launch_bounds__(T) k_walk_exit(BatchParams bp) {
         // position) exists
         constexpr uint32_t cnt = GPZ_SEG;
         const uint32_t* ppg = bp.pp + md.in_off + (td.seg << GPZ_SEG_LOG2);
-        uint32_t above = ppg[cnt];                  // pp just above the current window
-        uint32_t vnext = ppg[cnt - 32u + lane];     // the current window, prefetched
+        uint32_t above = ppg[cnt];  // pp just above the current window
+        // the current window and the next two below it, loaded ahead
+        uint32_t q0 = ppg[cnt - 32u + lane], q1 = ppg[cnt - 64u + lane], q2 = ppg[cnt - 96u + lane];
         for (int base = (int)cnt - 32; base >= 0; base -= 32) {
-            const uint32_t v = vnext;
-            if (base >= 32) vnext = ppg[base - 32 + lane];
+            const uint32_t v = q0;
+            q0 = q1;
+            q1 = q2;
+            if (base >= 96) q2 = ppg[base - 96 + lane];
             uint32_t v1 = __shfl_down_sync(kFull, v, 1);
             if (lane == 31) v1 = above;
             above = __shfl_sync(kFull, v, 0);
@@ -506,8 +509,8 @@ __global__ void __launch_bounds__(T) k_walk_exit(BatchParams bp) {
             if (nx >= cnt) val = nx - cnt;
             else if (nx >= (uint32_t)base + 32u) val = ex[nx & (kRing - 1u)];
             else tgt = nx - (uint32_t)base;
-#pragma unroll
-            for (int r = 0; r < 5; r++) {
+            // at most 5 rounds; done as soon as every lane is resolved
+            for (int r = 0; r < 5 && __any_sync(kFull, tgt < 32u); r++) {
                 const uint32_t pv = __shfl_sync(kFull, val, tgt & 31u);
                 const uint32_t pt = __shfl_sync(kFull, tgt, tgt & 31u);
                 if (tgt < 32u) {
@@ -542,8 +545,9 @@ __global__ void k_chain(BatchParams bp) {
 // positions (aligned), the lanes on the walk are found by doubling the links
 // from the entry lane; they emit their tokens in order (a demoted match
 // emits its literal byte) and count them in the warp's histogram; the walk
-// continues at the last one's next position.  The window after the current
-// one is prefetched, since the walk usually moves on to it.
+// continues at the last one's next position.  The three windows after the
+// current one (pp and input bytes) are loaded ahead, since the walk usually
+// moves on to them.
 template <int T>
 __global__ void __launch_bounds__(T) k_walk_mark(BatchParams bp) {
     constexpr int W = T / 32;
@@ -569,39 +573,65 @@ __global__ void __launch_bounds__(T) k_walk_mark(BatchParams bp) {
         __syncwarp();
         uint32_t cur = bp.tile_entry[t];
         uint32_t ntok = 0;
-        uint32_t wbase = 0xFFFFFFFFu, v = 0u, vn = 0u;
+        // the current window (pp v, input byte b) and the next three, loaded
+        // ahead; the byte is what a lazily demoted match emits
+        struct Win {
+            uint32_t v, b;
+        };
+        auto ld = [&](uint32_t q) {
+            return q + lane < cnt ? Win{ppg[q + lane], (uint32_t)ing[q + lane]} : Win{0u, 0u};
+        };
+        uint32_t wbase = 0xFFFFFFFFu;
+        Win w0{0u, 0u}, w1{0u, 0u}, w2{0u, 0u}, w3{0u, 0u};
         while (cur < cnt) {
             const uint32_t base = cur & ~31u;
             if (base != wbase) {
                 if (base == wbase + 32u) {
-                    v = vn;
+                    w0 = w1;
+                    w1 = w2;
+                    w2 = w3;
+                    w3 = ld(base + 96u);
+                } else if (base == wbase + 64u) {
+                    w0 = w2;
+                    w1 = w3;
+                    w2 = ld(base + 64u);
+                    w3 = ld(base + 96u);
+                } else if (base == wbase + 96u) {
+                    w0 = w3;
+                    w1 = ld(base + 32u);
+                    w2 = ld(base + 64u);
+                    w3 = ld(base + 96u);
                 } else {
-                    const uint32_t q = base + lane;
-                    v = q < cnt ? ppg[q] : 0u;
+                    w0 = ld(base);
+                    w1 = ld(base + 32u);
+                    w2 = ld(base + 64u);
+                    w3 = ld(base + 96u);
                 }
                 wbase = base;
-                const uint32_t qn = base + 32u + lane;
-                vn = qn < cnt ? ppg[qn] : 0u;
             }
+            const uint32_t v = w0.v, vn1 = w1.v;
             const uint32_t p = base + lane;
             uint32_t v1 = __shfl_down_sync(kFull, v, 1);
-            const uint32_t vn0 = __shfl_sync(kFull, vn, 0);
+            const uint32_t vn0 = __shfl_sync(kFull, vn1, 0);
             if (lane == 31) v1 = base + 32u < cnt ? vn0 : past;
             const bool inb = p < cnt;
             const uint32_t nx = walk_next(p, v, v1, start + p + 1u < n);
             // lanes on the walk in this window: doubling from the entry lane
             uint32_t S = 1u << (cur - base);
             uint32_t J = (inb && nx < base + 32u && nx < cnt) ? nx - base : 32u;
-#pragma unroll
+            // S holds the walk's first 2^r positions in the window after r
+            // rounds; a round that adds nothing means the walk has left
             for (int r = 0; r < 5; r++) {
                 const bool in = (S >> lane) & 1u;
-                S |= __reduce_or_sync(kFull, (in && J < 32u) ? (1u << J) : 0u);
+                const uint32_t add = __reduce_or_sync(kFull, (in && J < 32u) ? (1u << J) : 0u);
+                if ((add & ~S) == 0u) break;
+                S |= add;
                 const uint32_t Jp = __shfl_sync(kFull, J, J & 31u);
                 J = J < 32u ? Jp : 32u;
             }
             if ((S >> lane) & 1u) {
                 uint32_t tv = v;
-                if ((v >> 16) && nx == p + 1u) tv = ing[p];  // lazy demotion to a literal
+                if ((v >> 16) && nx == p + 1u) tv = w0.b;  // lazy demotion to a literal
                 tg[ntok + __popc(S & ((1u << lane) - 1u))] = tv;
                 if ((tv >> 16) == 0u) {
                     atomicAdd(&hist[tv & 0xFFu], 1u);
@@ -803,6 +833,170 @@ struct HuffSmem {
     uint32_t member, hbits, total, nrle, nlit, ndist, ok, crc;
 };
 
+// Codes one run of L equal code lengths v emits (rle_encode_lengths,
+// deflate.rs:254-326): a zero run as 18s (11-138), then 17s (3-10), then
+// single zeros; a non-zero run as the value, then 16s (3-6 repeats), then
+// single values.  Writes them at out (if not NULL); returns their number.
+__device__ int run_codes(uint32_t v, int L, uint8_t* code, uint8_t* extra) {
+    int k = 0;
+    auto emit = [&](uint32_t c, uint32_t e) {
+        if (code) {
+            code[k] = (uint8_t)c;
+            extra[k] = (uint8_t)e;
+        }
+        k++;
+    };
+    int r = L;
+    if (v == 0) {
+        while (r >= 11) {
+            const int q = r < 138 ? r : 138;
+            emit(18, (uint32_t)(q - 11));
+            r -= q;
+        }
+        while (r >= 3) {
+            const int q = r < 10 ? r : 10;
+            emit(17, (uint32_t)(q - 3));
+            r -= q;
+        }
+        while (r > 0) {
+            emit(0, 0);
+            r--;
+        }
+    } else {
+        emit(v, 0);
+        r--;
+        while (r >= 3) {
+            const int q = r < 6 ? r : 6;
+            emit(16, (uint32_t)(q - 3));
+            r -= q;
+        }
+        while (r > 0) {
+            emit(v, 0);
+            r--;
+        }
+    }
+    return k;
+}
+
+// HLIT / HDIST trims (trim_to_min: at least 257 / 1 codes) and the run-length
+// coding of the combined code lengths, by one warp: each lane owns 10
+// consecutive lengths and codes the runs that start in them; a run's end is
+// the next start, in the lane's chunk or the first one above it.
+template <class Smem>
+__device__ void warp_rle(Smem& sm, int lane) {
+    const uint8_t* ll = sm.lens;
+    const uint8_t* dl = sm.lens + GPZ_NLIT;
+    int lastl = 0;  // 1 + index of the last non-zero length code >= 257
+    for (int i = 257 + lane; i < GPZ_NLIT; i += 32)
+        if (ll[i]) lastl = i + 1;
+    lastl = __reduce_max_sync(0xFFFFFFFFu, lastl);
+    const int lastd = __reduce_max_sync(0xFFFFFFFFu, (lane < GPZ_NDIST && dl[lane]) ? lane + 1 : 0);
+    const int nlit = lastl > 257 ? lastl : 257;
+    const int ndist = lastd > 1 ? lastd : 1;
+    const int n = nlit + ndist;
+    for (int i = lane; i < n; i += 32) sm.comb[i] = i < nlit ? ll[i] : dl[i - nlit];
+    if (lane < 19) sm.meta_freq[lane] = 0;
+    __syncwarp();
+    constexpr int C = 10;  // 32 x 10 >= 286 + 30
+    const int lo = lane * C, hi = min(n, lo + C);
+    auto is_start = [&](int i) { return i == 0 || sm.comb[i] != sm.comb[i - 1]; };
+    int first = n;
+    for (int i = lo; i < hi; i++)
+        if (is_start(i)) {
+            first = i;
+            break;
+        }
+    // first run start in the lanes above this one
+    int sfx = first;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_down_sync(0xFFFFFFFFu, sfx, o);
+        if (lane + o < 32) sfx = y < sfx ? y : sfx;
+    }
+    int above = __shfl_down_sync(0xFFFFFFFFu, sfx, 1);
+    if (lane == 31) above = n;
+    auto run_end = [&](int i) {
+        int j = i + 1;
+        while (j < hi && sm.comb[j] == sm.comb[i]) j++;
+        return j < hi ? j : above;
+    };
+    int mine = 0;
+    for (int i = lo; i < hi; i++)
+        if (is_start(i)) mine += run_codes(sm.comb[i], run_end(i) - i, nullptr, nullptr);
+    int off = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xFFFFFFFFu, off, o);
+        if (lane >= o) off += y;
+    }
+    const int total = __shfl_sync(0xFFFFFFFFu, off, 31);
+    off -= mine;
+    for (int i = lo; i < hi; i++)
+        if (is_start(i)) off += run_codes(sm.comb[i], run_end(i) - i, sm.rle_code + off, sm.rle_extra + off);
+    __syncwarp();
+    for (int q = lane; q < total; q += 32) atomicAdd(&sm.meta_freq[sm.rle_code[q]], 1u);
+    if (lane == 0) {
+        sm.nrle = (uint32_t)total;
+        sm.nlit = (uint32_t)nlit;
+        sm.ndist = (uint32_t)ndist;
+    }
+    __syncwarp();
+}
+
+// The dynamic block header bits (deflate.rs:911-932) by one warp: 3 + 5 + 5 +
+// 4 fixed bits, 3 bits per meta length in META_ORDER, then per RLE entry its
+// meta code and extra bits; every field's bit position comes from a scan
+// and the fields are ORed into zeroed words, LSB first.
+template <class Smem>
+__device__ void warp_header(Smem& sm, int lane) {
+    int hclen = 0;  // 1 + last non-zero meta length in META_ORDER, at least 4
+    if (lane < 19 && sm.meta_lens[c_meta_order[lane]]) hclen = lane + 1;
+    hclen = __reduce_max_sync(0xFFFFFFFFu, hclen);
+    if (hclen < 4) hclen = 4;
+    for (int w = lane; w < GPZ_HDR_WORDS; w += 32) sm.hdr[w] = 0u;
+    __syncwarp();
+    auto put_at = [&](uint32_t pos, uint32_t v, uint32_t k) {
+        if (!k) return;
+        const uint32_t w = pos >> 5, sh = pos & 31u;
+        atomicOr(&sm.hdr[w], v << sh);
+        if (sh + k > 32u) atomicOr(&sm.hdr[w + 1], v >> (32u - sh));
+    };
+    if (lane == 0) {
+        put_at(0, 5u, 3);
+        put_at(3, sm.nlit - 257u, 5);
+        put_at(8, sm.ndist - 1u, 5);
+        put_at(13, (uint32_t)hclen - 4u, 4);
+    }
+    if (lane < hclen) put_at(17u + 3u * lane, sm.meta_lens[c_meta_order[lane]], 3);
+    const uint32_t base = 17u + 3u * (uint32_t)hclen;
+    const int nrle = (int)sm.nrle;
+    constexpr int C = 10;
+    const int lo = lane * C, hi = min(nrle, lo + C);
+    auto field = [&](int q, uint32_t& v) {
+        const uint32_t c = sm.rle_code[q], mc = sm.meta_codes[c];
+        const uint32_t cl = mc >> 16, eb = c == 16 ? 2u : c == 17 ? 3u : c == 18 ? 7u : 0u;
+        v = (mc & 0xFFFFu) | ((uint32_t)sm.rle_extra[q] << cl);
+        return cl + eb;
+    };
+    uint32_t mine = 0, v;
+    for (int q = lo; q < hi; q++) mine += field(q, v);
+    uint32_t off = mine;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, off, o);
+        if (lane >= o) off += y;
+    }
+    const uint32_t total = __shfl_sync(0xFFFFFFFFu, off, 31);
+    uint32_t pos = base + off - mine;
+    for (int q = lo; q < hi; q++) {
+        const uint32_t k = field(q, v);
+        put_at(pos, v, k);
+        pos += k;
+    }
+    if (lane == 0) sm.hbits = base + total;
+    __syncwarp();
+}
+
 // Per member: code lengths and codes, the dynamic block header
 // (deflate.rs:830-932), the exact bit plan of every tile, the member's
 // DEFLATE size and its CRC-32.  Members are independent: no waiting.
@@ -856,14 +1050,25 @@ __global__ void __launch_bounds__(kHuffThreads) k_huff(BatchParams bp) {
             if (tid < kCrcSlices) {
                 const uint2* words = reinterpret_cast<const uint2*>(bp.in + md.in_off);
                 uint32_t c = 0;
-                for (uint32_t v = tid * per; v < (tid + 1) * per; v++) {
-                    if (v < padw) continue;
-                    const uint2 wv = __ldg(words + (v - padw));
-                    const uint32_t lo = wv.x ^ c, hi = wv.y;
-                    c = sm.crctab[7 * 256 + (lo & 0xFFu)] ^ sm.crctab[6 * 256 + ((lo >> 8) & 0xFFu)] ^
-                        sm.crctab[5 * 256 + ((lo >> 16) & 0xFFu)] ^ sm.crctab[4 * 256 + (lo >> 24)] ^
-                        sm.crctab[3 * 256 + (hi & 0xFFu)] ^ sm.crctab[2 * 256 + ((hi >> 8) & 0xFFu)] ^
-                        sm.crctab[1 * 256 + ((hi >> 16) & 0xFFu)] ^ sm.crctab[hi >> 24];
+                // eight words loaded ahead of the fold (a padding word is zero)
+                constexpr uint32_t kAhead = 8;
+                for (uint32_t v0 = tid * per; v0 < (tid + 1) * per; v0 += kAhead) {
+                    uint2 wv[kAhead];
+#pragma unroll
+                    for (uint32_t u = 0; u < kAhead; u++) {
+                        const uint32_t v = v0 + u;
+                        wv[u] = make_uint2(0u, 0u);
+                        if (v < (tid + 1) * per && v >= padw) wv[u] = __ldg(words + (v - padw));
+                    }
+#pragma unroll
+                    for (uint32_t u = 0; u < kAhead; u++) {
+                        if (v0 + u >= (tid + 1) * per) break;
+                        const uint32_t lo = wv[u].x ^ c, hi = wv[u].y;
+                        c = sm.crctab[7 * 256 + (lo & 0xFFu)] ^ sm.crctab[6 * 256 + ((lo >> 8) & 0xFFu)] ^
+                            sm.crctab[5 * 256 + ((lo >> 16) & 0xFFu)] ^ sm.crctab[4 * 256 + (lo >> 24)] ^
+                            sm.crctab[3 * 256 + (hi & 0xFFu)] ^ sm.crctab[2 * 256 + ((hi >> 8) & 0xFFu)] ^
+                            sm.crctab[1 * 256 + ((hi >> 16) & 0xFFu)] ^ sm.crctab[hi >> 24];
+                    }
                 }
                 sm.crcv[tid] = c;
             }
@@ -926,68 +1131,7 @@ __global__ void __launch_bounds__(kHuffThreads) k_huff(BatchParams bp) {
         // canonical codes (warps 0, 1); trims + RLE (deflate.rs:254-335) on warp 2
         if (warp == 0) warp_canonical(sm.lens, GPZ_NLIT, sm.codes);
         else if (warp == 1) warp_canonical(sm.lens + GPZ_NLIT, GPZ_NDIST, sm.codes + GPZ_NLIT);
-        else if (warp == 2 && lane == 0) {
-            const uint8_t* ll = sm.lens;
-            const uint8_t* dl = sm.lens + GPZ_NLIT;
-            int nlit = GPZ_NLIT;
-            while (nlit > 257 && ll[nlit - 1] == 0) nlit--;
-            int ndist = GPZ_NDIST;
-            while (ndist > 1 && dl[ndist - 1] == 0) ndist--;
-            for (int i = 0; i < nlit; i++) sm.comb[i] = ll[i];
-            for (int i = 0; i < ndist; i++) sm.comb[nlit + i] = dl[i];
-            const int n = nlit + ndist;
-            int k = 0, i = 0;
-            while (i < n) {
-                const uint8_t cur = sm.comb[i];
-                int run = 1;
-                while (i + run < n && sm.comb[i + run] == cur) run++;
-                if (cur == 0) {
-                    while (run >= 11) {
-                        const int q = run < 138 ? run : 138;
-                        sm.rle_code[k] = 18;
-                        sm.rle_extra[k++] = (uint8_t)(q - 11);
-                        run -= q;
-                        i += q;
-                    }
-                    while (run >= 3) {
-                        const int q = run < 10 ? run : 10;
-                        sm.rle_code[k] = 17;
-                        sm.rle_extra[k++] = (uint8_t)(q - 3);
-                        run -= q;
-                        i += q;
-                    }
-                    while (run > 0) {
-                        sm.rle_code[k] = 0;
-                        sm.rle_extra[k++] = 0;
-                        run--;
-                        i++;
-                    }
-                } else {
-                    sm.rle_code[k] = cur;
-                    sm.rle_extra[k++] = 0;
-                    i++;
-                    run--;
-                    while (run >= 3) {
-                        const int q = run < 6 ? run : 6;
-                        sm.rle_code[k] = 16;
-                        sm.rle_extra[k++] = (uint8_t)(q - 3);
-                        run -= q;
-                        i += q;
-                    }
-                    while (run > 0) {
-                        sm.rle_code[k] = cur;
-                        sm.rle_extra[k++] = 0;
-                        run--;
-                        i++;
-                    }
-                }
-            }
-            for (int q = 0; q < 19; q++) sm.meta_freq[q] = 0;
-            for (int q = 0; q < k; q++) sm.meta_freq[sm.rle_code[q]]++;
-            sm.nrle = (uint32_t)k;
-            sm.nlit = (uint32_t)nlit;
-            sm.ndist = (uint32_t)ndist;
-        }
+        else if (warp == 2) warp_rle(sm, lane);
         __syncthreads();
         // meta code lengths, 7-bit limit (deflate.rs:896-903), and codes
         if (warp == 0) {
@@ -997,37 +1141,8 @@ __global__ void __launch_bounds__(kHuffThreads) k_huff(BatchParams bp) {
             warp_canonical(sm.meta_lens, 19, sm.meta_codes);
         }
         __syncthreads();
-        // header bits (deflate.rs:911-932), LSB first, one 64-bit accumulator
-        if (tid == 0) {
-            int hclen = 19;
-            while (hclen > 4 && sm.meta_lens[c_meta_order[hclen - 1]] == 0) hclen--;
-            unsigned long long acc = 0;
-            uint32_t nb = 0, wpos = 0, pos = 0;
-            auto put = [&](uint32_t v, uint32_t k) {
-                acc |= (unsigned long long)v << nb;
-                nb += k;
-                pos += k;
-                if (nb >= 32u) {
-                    sm.hdr[wpos++] = (uint32_t)acc;
-                    acc >>= 32;
-                    nb -= 32u;
-                }
-            };
-            put(5u, 3);
-            put(sm.nlit - 257u, 5);
-            put(sm.ndist - 1u, 5);
-            put((uint32_t)hclen - 4u, 4);
-            for (int q = 0; q < hclen; q++) put(sm.meta_lens[c_meta_order[q]], 3);
-            for (uint32_t q = 0; q < sm.nrle; q++) {
-                const uint32_t c = sm.rle_code[q], mc = sm.meta_codes[c];
-                put(mc & 0xFFFFu, mc >> 16);
-                if (c == 16) put(sm.rle_extra[q], 2);
-                else if (c == 17) put(sm.rle_extra[q], 3);
-                else if (c == 18) put(sm.rle_extra[q], 7);
-            }
-            if (nb) sm.hdr[wpos++] = (uint32_t)acc;
-            sm.hbits = pos;
-        }
+        // header bits (deflate.rs:911-932), LSB first
+        if (warp == 0) warp_header(sm, lane);
         __syncthreads();
 
         // bits per symbol occurrence (code + extra); total member bits
@@ -1294,6 +1409,64 @@ __global__ void k_drain(BatchParams bp, uint8_t* h_out, MemberOut* h_mout, uint3
 
 }  // namespace
 
+// ================================================================= k_fetch
+
+constexpr int kFetchBlocksPerSm = 2;  // grid: 2 x 74 x this, one wave on 148 SMs
+
+// Copies a batch's descriptor block and input from mapped host memory into
+// the device arenas with SM loads over PCIe.  Sizes come from the block's
+// header; a header that asks for more than an arena holds sets the
+// descriptor error bit, empties the batch and copies nothing (the batch then
+// reports an error).
+__global__ void k_fetch(FetchSource f, uint32_t* counters) {
+    // the work counters and the error word start at zero (in place of the
+    // memset that precedes a batch without k_fetch)
+    uint32_t* err = counters + GPZ_NCOUNTERS;
+    if (blockIdx.x == 0)
+        for (int i = threadIdx.x; i < GPZ_NCOUNTERS + 16; i += blockDim.x) counters[i] = 0u;
+    __syncthreads();
+    const uint32_t* hdr = reinterpret_cast<const uint32_t*>(f.h_desc);
+    const uint64_t nt = hdr[0], nm = hdr[1];
+    const uint64_t in_bytes = reinterpret_cast<const unsigned long long*>(f.h_desc)[1];
+    if (nt > f.tiles_cap || nm > f.members_cap || in_bytes > f.in_cap || (in_bytes & 15u)) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            f.d_dims[0] = 0u;  // the batch's kernels then find no work
+            f.d_dims[1] = 0u;
+            *err = GPZ_ERRBIT_DESC;
+        }
+        return;
+    }
+    const uint64_t tid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t nthr = (uint64_t)gridDim.x * blockDim.x;
+    // descriptors: 4-byte words (the member records are 24 bytes, the tile
+    // block starts 8-byte aligned)
+    const uint64_t hw = 16, mw = nm * sizeof(MemberDesc) / 4, tw = nt * sizeof(TileDesc) / 4;
+    const uint32_t* src = hdr;
+    for (uint64_t i = tid; i < hw + mw + tw; i += nthr) {
+        const uint32_t v = src[i];
+        if (i < hw) f.d_dims[i] = v;
+        else if (i < hw + mw) reinterpret_cast<uint32_t*>(f.d_members)[i - hw] = v;
+        else reinterpret_cast<uint32_t*>(f.d_tiles)[i - hw - mw] = v;
+    }
+    // input: 16-byte vectors, four in flight per thread
+    const uint4* si = reinterpret_cast<const uint4*>(f.h_in);
+    uint4* di = reinterpret_cast<uint4*>(f.d_in);
+    const uint64_t nv = in_bytes / 16;
+    for (uint64_t i = tid; i < nv; i += 4 * nthr) {
+        uint4 v[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const uint64_t j = i + u * nthr;
+            if (j < nv) v[u] = si[j];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const uint64_t j = i + u * nthr;
+            if (j < nv) di[j] = v[u];
+        }
+    }
+}
+
 // ================================================================ launchers
 
 size_t gpz_lookup_smem_bytes() { return LookupSmem::kBytes; }
@@ -1329,8 +1502,9 @@ int gpz_kernel_smem_setup() {
 }
 
 int gpz_launch_batch(const BatchParams& bp, const LaunchShape& ls, void* stream, void* const* events,
-                     const DrainTarget* drain) {
+                     const DrainTarget* drain, const FetchSource* fetch) {
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (fetch) k_fetch<<<2 * kFetchBlocksPerSm * 74, 256, 0, s>>>(*fetch, bp.counters);
     auto mark = [&](int i) {
         if (events) cudaEventRecord(static_cast<cudaEvent_t>(events[i]), s);
     };

@@ -15,6 +15,7 @@
 //    the stage kernels with the bucket's autotuned launch shape, and the
 //    drain into mapped host memory;
 //  * a continuous-batching serving engine (gpz_submit / gpz_poll).
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -369,7 +370,7 @@ int reserve_counts(gpz_ctx* c, Slot& sl, size_t in_bytes, size_t nm, size_t nt, 
     if ((rc = ensure_dev(c, sl, sl.d_members, nm * sizeof(MemberDesc), capped))) return rc;
     if ((rc = ensure_dev(c, sl, sl.d_tiles, nt * sizeof(TileDesc), capped))) return rc;
     if ((rc = ensure_dev(c, sl, sl.d_dims, kDescHeader, capped))) return rc;
-    if ((rc = ensure_host(c, sl, sl.h_desc, sl.h_desc_cap, desc_bytes(nm, nt), false))) return rc;
+    if ((rc = ensure_host(c, sl, sl.h_desc, sl.h_desc_cap, desc_bytes(nm, nt), true))) return rc;
     if ((rc = ensure_host(c, sl, sl.h_mout, sl.h_mout_cap, nm, true))) return rc;
     if ((rc = ensure_host(c, sl, sl.h_err, sl.h_err_cap, 16, true))) return rc;
     return GPZ_OK;
@@ -390,7 +391,7 @@ int reserve_limits(gpz_ctx* c, Slot& sl, size_t max_bytes, size_t max_items) {
     const size_t out_bytes = nm * member_bound(0) + 2 * max_bytes;
     int rc;
     if ((rc = reserve_counts(c, sl, in_bytes, nm, nt, true, true, out_bytes, false))) return rc;
-    if ((rc = ensure_host(c, sl, sl.h_in, sl.h_in_cap, in_bytes + 64, false))) return rc;
+    if ((rc = ensure_host(c, sl, sl.h_in, sl.h_in_cap, in_bytes + 64, true))) return rc;
     return ensure_host(c, sl, sl.h_out, sl.h_out_cap, out_bytes + 64, true);
 }
 
@@ -423,18 +424,28 @@ BatchParams params_of(Slot& sl, const uint8_t* d_in, uint8_t* d_out) {
     return bp;
 }
 
-// Descriptors staged as [dims][members][tiles] in pinned memory, uploaded
-// into their three arenas.
-int upload_desc(gpz_ctx* c, Slot& sl, cudaStream_t s) {
+// Descriptors staged as [dims][members][tiles] in pinned memory: the
+// 64-byte header holds the tile and member counts (u32 at bytes 0 and 4) and
+// the batch's input bytes (u64 at byte 8).
+void write_desc(Slot& sl) {
     const size_t nm = sl.members.size(), nt = sl.tiles.size();
     uint32_t* dims = reinterpret_cast<uint32_t*>(sl.h_desc);
     std::memset(dims, 0, kDescHeader);
     dims[0] = (uint32_t)nt;
     dims[1] = (uint32_t)nm;
+    const uint64_t in_bytes = sl.in_bytes;
+    std::memcpy(sl.h_desc + 8, &in_bytes, 8);
+    uint8_t* hm = sl.h_desc + kDescHeader;
+    std::memcpy(hm, sl.members.data(), nm * sizeof(MemberDesc));
+    if (nt) std::memcpy(hm + nm * sizeof(MemberDesc), sl.tiles.data(), nt * sizeof(TileDesc));
+}
+
+// ... uploaded into their three arenas by copies on stream s.
+int upload_desc(gpz_ctx* c, Slot& sl, cudaStream_t s) {
+    const size_t nm = sl.members.size(), nt = sl.tiles.size();
+    write_desc(sl);
     uint8_t* hm = sl.h_desc + kDescHeader;
     uint8_t* ht = hm + nm * sizeof(MemberDesc);
-    std::memcpy(hm, sl.members.data(), nm * sizeof(MemberDesc));
-    if (nt) std::memcpy(ht, sl.tiles.data(), nt * sizeof(TileDesc));
     CU(c, cudaMemcpyAsync(sl.d_dims.p, sl.h_desc, kDescHeader, cudaMemcpyHostToDevice, s));
     CU(c, cudaMemcpyAsync(sl.d_members.p, hm, nm * sizeof(MemberDesc), cudaMemcpyHostToDevice, s));
     if (nt) CU(c, cudaMemcpyAsync(sl.d_tiles.p, ht, nt * sizeof(TileDesc), cudaMemcpyHostToDevice, s));
@@ -461,10 +472,12 @@ LaunchShape shape_for(gpz_ctx* c, int bucket) {
 // Stage kernels (+ drain) for the slot's planned batch, as a CUDA graph per
 // (slot, bucket) or as direct launches on stream s.
 int launch(gpz_ctx* c, Slot& sl, const BatchParams& bp, const LaunchShape& shape, bool use_graph,
-           const DrainTarget* drain, bool timing, cudaStream_t s) {
+           const DrainTarget* drain, bool timing, cudaStream_t s, const FetchSource* fetch = nullptr) {
     if (!use_graph) {
-        CU(c, cudaMemsetAsync(sl.d_cnt.p, 0, GPZ_NCOUNTERS * 4 + 64, s));
-        if (gpz_launch_batch(bp, shape, s, timing ? reinterpret_cast<void* const*>(sl.ev) : nullptr, drain) != 0)
+        // with k_fetch, the fetch kernel zeroes the counters itself
+        if (!fetch) CU(c, cudaMemsetAsync(sl.d_cnt.p, 0, GPZ_NCOUNTERS * 4 + 64, s));
+        if (gpz_launch_batch(bp, shape, s, timing ? reinterpret_cast<void* const*>(sl.ev) : nullptr, drain,
+                             fetch) != 0)
             return fail(c, GPZ_E_CUDA, "kernel launch", cudaGetLastError());
         c->launches = 10 + (drain ? 1 : 0);
         return GPZ_OK;
@@ -477,8 +490,8 @@ int launch(gpz_ctx* c, Slot& sl, const BatchParams& bp, const LaunchShape& shape
     if (!g.exec) {
         cudaGraph_t graph = nullptr;
         CU(c, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-        cudaMemsetAsync(sl.d_cnt.p, 0, GPZ_NCOUNTERS * 4 + 64, s);
-        gpz_launch_batch(bp, shape, s, nullptr, drain);
+        if (!fetch) cudaMemsetAsync(sl.d_cnt.p, 0, GPZ_NCOUNTERS * 4 + 64, s);
+        gpz_launch_batch(bp, shape, s, nullptr, drain, fetch);
         cudaError_t e = cudaStreamEndCapture(s, &graph);
         if (e != cudaSuccess) return fail(c, GPZ_E_CUDA, "graph capture", e);
         e = cudaGraphInstantiate(&g.exec, graph, 0);
@@ -547,9 +560,11 @@ struct LaunchPolicy {
     bool exact = false;     // grids sized to this batch (one CTA per item), no graph
     bool autotune = true;   // tune the bucket's shape on its first use
     bool graphs = true;     // per-(slot, bucket) CUDA graph
+    bool fetch = false;     // SMs fetch input and descriptors from mapped memory (k_fetch)
+    int grid_pct = 100;     // persistent grids at this percentage of full occupancy
 };
-constexpr LaunchPolicy kPolicyBatched{false, true, true};
-constexpr LaunchPolicy kPolicyPlain{true, false, false};
+constexpr LaunchPolicy kPolicyBatched{false, true, true, false, 100};
+constexpr LaunchPolicy kPolicyPlain{true, false, false, false, 100};
 
 // Plans, uploads and launches one batch of host items on a slot (no wait).
 int submit_slot(gpz_ctx* c, Slot& sl, const gpz_desc* d, size_t count, const LaunchPolicy& pol) {
@@ -566,7 +581,7 @@ int submit_slot(gpz_ctx* c, Slot& sl, const gpz_desc* d, size_t count, const Lau
     const size_t obound = out_bound_of_plan(sl);
     int rc;
     if ((rc = reserve(c, sl, in_bytes, true, true, obound))) return rc;
-    if ((rc = ensure_host(c, sl, sl.h_in, sl.h_in_cap, in_bytes + 64, false))) return rc;
+    if ((rc = ensure_host(c, sl, sl.h_in, sl.h_in_cap, in_bytes + 64, true))) return rc;
     if ((rc = ensure_host(c, sl, sl.h_out, sl.h_out_cap, obound + 64, true))) return rc;
     double t1 = now_ms();
     add_time(c, 0, t1 - t0);
@@ -580,8 +595,23 @@ int submit_slot(gpz_ctx* c, Slot& sl, const gpz_desc* d, size_t count, const Lau
     add_time(c, 1, t0 - t1);
     cudaStream_t s = sl.stream;
     CU(c, cudaEventRecord(sl.tv[0], s));
-    CU(c, cudaMemcpyAsync(sl.d_in.p, sl.h_in, in_bytes, cudaMemcpyHostToDevice, s));
-    if ((rc = upload_desc(c, sl, s))) return rc;
+    FetchSource fs{};
+    if (pol.fetch) {
+        write_desc(sl);
+        fs.h_desc = mapped_dev(sl.h_desc);
+        fs.h_in = mapped_dev(sl.h_in);
+        if (!fs.h_desc || !fs.h_in) return fail(c, GPZ_E_CUDA, "mapped host memory");
+        fs.d_dims = static_cast<uint32_t*>(sl.d_dims.p);
+        fs.d_members = static_cast<MemberDesc*>(sl.d_members.p);
+        fs.d_tiles = static_cast<TileDesc*>(sl.d_tiles.p);
+        fs.d_in = static_cast<uint8_t*>(sl.d_in.p);
+        fs.members_cap = sl.d_members.cap / sizeof(MemberDesc);
+        fs.tiles_cap = sl.d_tiles.cap / sizeof(TileDesc);
+        fs.in_cap = sl.d_in.cap;
+    } else {
+        CU(c, cudaMemcpyAsync(sl.d_in.p, sl.h_in, in_bytes, cudaMemcpyHostToDevice, s));
+        if ((rc = upload_desc(c, sl, s))) return rc;
+    }
     CU(c, cudaEventRecord(sl.tv[1], s));
     BatchParams bp = params_of(sl, static_cast<const uint8_t*>(sl.d_in.p), static_cast<uint8_t*>(sl.d_out.p));
     DrainTarget dt{mapped_dev(sl.h_out), mapped_dev(sl.h_mout), mapped_dev(sl.h_err), c->sms * 4};
@@ -602,7 +632,13 @@ int submit_slot(gpz_ctx* c, Slot& sl, const gpz_desc* d, size_t count, const Lau
             (rc = autotune(c, sl, bp, &dt, s)))
             return rc;
         const bool graphs = pol.graphs && !(c->flags & GPZ_FLAG_NO_GRAPHS) && !timing;
-        rc = launch(c, sl, bp, shape_for(c, sl.bucket), graphs, &dt, timing, s);
+        LaunchShape shape = shape_for(c, sl.bucket);
+        if (pol.grid_pct < 100) {
+            for (int* g : {&shape.lookup_grid, &shape.walk_grid, &shape.emit_grid, &shape.segtab_grid,
+                           &shape.huff_grid})
+                *g = std::max(1, *g * pol.grid_pct / 100);
+        }
+        rc = launch(c, sl, bp, shape, graphs, &dt, timing, s, pol.fetch ? &fs : nullptr);
     }
     if (rc) return rc;
     CU(c, cudaEventRecord(sl.tv[2], s));
@@ -778,6 +814,81 @@ struct Unit {
 
 }  // namespace
 
+// SM partitions (green contexts) for the serving lanes.  The driver entry
+// points are resolved at run time through the CUDA runtime, so the library
+// does not link libcuda.  A partition is a CUcontext restricted to a set of
+// SMs; memory, streams, events and graphs made while it is current belong to
+// it, and kernels launched on its streams run only on its SMs.
+struct GreenApi {
+    CUresult (*dev_get)(CUdevice*, int) = nullptr;
+    CUresult (*get_res)(CUdevice, CUdevResource*, CUdevResourceType) = nullptr;
+    CUresult (*split)(CUdevResource*, unsigned*, const CUdevResource*, CUdevResource*, unsigned, unsigned) = nullptr;
+    CUresult (*gen_desc)(CUdevResourceDesc*, CUdevResource*, unsigned) = nullptr;
+    CUresult (*create)(CUgreenCtx*, CUdevResourceDesc, CUdevice, unsigned) = nullptr;
+    CUresult (*destroy)(CUgreenCtx) = nullptr;
+    CUresult (*to_ctx)(CUcontext*, CUgreenCtx) = nullptr;
+    CUresult (*set_cur)(CUcontext) = nullptr;
+    CUresult (*get_cur)(CUcontext*) = nullptr;
+    bool ok = false;
+
+    GreenApi() {
+        auto get = [](const char* name, auto& fn) {
+            void* p = nullptr;
+            cudaDriverEntryPointQueryResult q;
+            if (cudaGetDriverEntryPoint(name, &p, cudaEnableDefault, &q) != cudaSuccess ||
+                q != cudaDriverEntryPointSuccess) {
+                cudaGetLastError();
+                return false;
+            }
+            fn = reinterpret_cast<std::remove_reference_t<decltype(fn)>>(p);
+            return true;
+        };
+        ok = get("cuDeviceGet", dev_get) && get("cuDeviceGetDevResource", get_res) &&
+             get("cuDevSmResourceSplitByCount", split) && get("cuDevResourceGenerateDesc", gen_desc) &&
+             get("cuGreenCtxCreate", create) && get("cuGreenCtxDestroy", destroy) &&
+             get("cuCtxFromGreenCtx", to_ctx) && get("cuCtxSetCurrent", set_cur) && get("cuCtxGetCurrent", get_cur);
+    }
+};
+
+GreenApi& green_api() {
+    static GreenApi api;
+    return api;
+}
+
+struct SmPartition {
+    CUgreenCtx green = nullptr;
+    CUcontext ctx = nullptr;
+    int sms = 0;
+};
+
+// Splits the device's SMs into `first` SMs (rounded as the driver requires)
+// and the rest.  Returns false (and leaves nothing behind) if the driver
+// cannot.
+bool make_partitions(int device, int first, SmPartition out[2]) {
+    GreenApi& g = green_api();
+    if (!g.ok) return false;
+    CUdevice dev;
+    CUdevResource all, part[1], rest;
+    unsigned nb = 1;
+    CUdevResourceDesc d[2];
+    if (g.dev_get(&dev, device) != CUDA_SUCCESS || g.get_res(dev, &all, CU_DEV_RESOURCE_TYPE_SM) != CUDA_SUCCESS ||
+        g.split(part, &nb, &all, &rest, 0, (unsigned)first) != CUDA_SUCCESS || nb != 1 || rest.sm.smCount == 0 ||
+        g.gen_desc(&d[0], &part[0], 1) != CUDA_SUCCESS || g.gen_desc(&d[1], &rest, 1) != CUDA_SUCCESS)
+        return false;
+    for (int i = 0; i < 2; i++) {
+        if (g.create(&out[i].green, d[i], dev, CU_GREEN_CTX_DEFAULT_STREAM) != CUDA_SUCCESS ||
+            g.to_ctx(&out[i].ctx, out[i].green) != CUDA_SUCCESS) {
+            for (int j = 0; j <= i; j++)
+                if (out[j].green) g.destroy(out[j].green);
+            out[0] = out[1] = SmPartition{};
+            return false;
+        }
+    }
+    out[0].sms = (int)part[0].sm.smCount;
+    out[1].sms = (int)rest.sm.smCount;
+    return true;
+}
+
 // Continuous batching over two lanes.  Requests of at most 1 MiB go to the
 // small lane, larger ones (cut into 2 MiB units, whole members) to the large
 // lane.  Each lane has pipeline slots (three small, two large), a launcher
@@ -787,11 +898,16 @@ struct Unit {
 // that retires the lane's batches in launch order (framing, copies into the
 // requests).
 //
-// The lanes share the GPU through stream priorities: the small lane's
-// streams are the most urgent, and the large lane launches grids of one CTA
-// per tile (no persistent CTAs), so the small lane's CTAs take SMs as soon
-// as the large lane's current CTAs retire instead of waiting for whole
-// kernels.  Every slot is sized once at start for its lane's batch limits,
+// The lanes share the GPU through stream priorities and grid sizes: the
+// small lane's streams are the most urgent and the large lane's persistent
+// grids cover three quarters of the GPU's resident CTAs, so the small lane's
+// CTAs find SMs as the large lane's CTAs retire.  With GPZ_FLAG_SM_PARTITION
+// the lanes run on two SM partitions instead (green contexts: 32 SMs for the
+// small lane, the rest for the large one): strict isolation, at the price of
+// the small lane's peak throughput.  The small
+// lane fetches its input and descriptors with SM loads from mapped memory
+// (k_fetch), so it never queues behind the large lane's uploads on a copy
+// engine.  Every slot is sized once at start for its lane's batch limits,
 // so serving never allocates or frees device memory (cudaFree would
 // synchronise the device).
 //
@@ -823,6 +939,9 @@ struct ServeEngine {
 
     gpz_ctx* c = nullptr;
     Lane lanes[2];  // 0: requests <= 1 MiB, 1: larger
+    SmPartition part[2];  // per lane, when the GPU is partitioned
+    bool partitioned = false;
+    static constexpr int kSmallLaneSms = 32;
     std::mutex mu;
     std::condition_variable cv_done;
     std::unordered_map<uint64_t, std::shared_ptr<Request>> reqs;
@@ -833,28 +952,55 @@ struct ServeEngine {
     uint64_t rejected = 0, batches = 0, bytes_in = 0, bytes_out = 0;
     double max_queue_ms = 0;
 
+    // Makes lane l's partition (or the device's primary context) current on
+    // the calling thread.
+    void bind(int l) {
+        if (partitioned) green_api().set_cur(part[l].ctx);
+        else cudaSetDevice(c->device);
+    }
+
     int start(gpz_ctx* ctx) {
         c = ctx;
         cudaSetDevice(c->device);
+        cudaFree(nullptr);  // the primary context exists before partitioning
+        CUcontext primary = nullptr;
+        if ((c->flags & GPZ_FLAG_SM_PARTITION) && c->sms >= 4 * kSmallLaneSms && green_api().ok &&
+            green_api().get_cur(&primary) == CUDA_SUCCESS)
+            partitioned = make_partitions(c->device, kSmallLaneSms, part);
         int least = 0, greatest = 0;
         cudaDeviceGetStreamPriorityRange(&least, &greatest);
         Lane& sm = lanes[0];
         sm.nslots = 3;
         sm.batch_cap = 4u << 20;
         sm.max_units = 1024;
-        sm.pol = LaunchPolicy{false, false, true};  // persistent default shape, graphs, no tuning pass
+        sm.pol = LaunchPolicy{false, false, true, true, 100};  // persistent default shape, graphs, k_fetch
         Lane& lg = lanes[1];
         lg.nslots = 2;
         lg.batch_cap = 16u << 20;
         lg.max_units = 16;
-        lg.pol = LaunchPolicy{true, false, false};  // one CTA per tile
-        for (int l = 0; l < 2; l++)
-            for (int k = 0; k < lanes[l].nslots; k++) {
+        // without partitions: persistent grids on three quarters of the GPU,
+        // the rest stays free for the small lane's CTAs; copy-engine upload
+        lg.pol = LaunchPolicy{false, false, true, false, 75};
+        if (partitioned) {
+            // each lane's persistent grids cover its own SMs
+            sm.pol.grid_pct = std::max(1, 100 * part[0].sms / c->sms);
+            lg.pol.grid_pct = std::max(1, 100 * part[1].sms / c->sms);
+        }
+        int rc = GPZ_OK;
+        for (int l = 0; l < 2 && !rc; l++) {
+            bind(l);
+            if (partitioned && gpz_kernel_smem_setup() != 0) rc = fail(c, GPZ_E_CUDA, "partition setup");
+            for (int k = 0; k < lanes[l].nslots && !rc; k++) {
                 Slot& s = lanes[l].slots[k];
-                int rc = init_slot(c, s, l == 0 ? greatest : least);
+                rc = init_slot(c, s, l == 0 ? greatest : least);
                 if (!rc) rc = reserve_limits(c, s, lanes[l].batch_cap, lanes[l].max_units);
-                if (rc) return rc;
             }
+        }
+        if (partitioned) green_api().set_cur(primary);
+        if (rc) {
+            shutdown();  // frees what was made; no thread runs yet
+            return rc;
+        }
         for (auto& L : lanes) {
             L.launcher = std::thread([this, &L] { launch_loop(L); });
             L.completer = std::thread([this, &L] { complete_loop(L); });
@@ -875,8 +1021,17 @@ struct ServeEngine {
             if (L.launcher.joinable()) L.launcher.join();
             if (L.completer.joinable()) L.completer.join();
         }
-        for (auto& L : lanes)
-            for (auto& s : L.slots) free_slot(c, s);
+        CUcontext primary = nullptr;
+        if (partitioned) green_api().get_cur(&primary);
+        for (int l = 0; l < 2; l++) {
+            bind(l);
+            for (auto& s : lanes[l].slots) free_slot(c, s);
+        }
+        if (partitioned) {
+            green_api().set_cur(primary);
+            for (auto& p : part) green_api().destroy(p.green);
+            partitioned = false;
+        }
     }
 
     int submit(const gpz_desc* d, uint64_t* ticket, bool copy) {
@@ -962,7 +1117,7 @@ struct ServeEngine {
     }
 
     void launch_loop(Lane& L) {
-        cudaSetDevice(c->device);
+        bind(&L == &lanes[0] ? 0 : 1);
         for (;;) {
             int k = -1;
             std::vector<Unit> batch;
@@ -996,7 +1151,7 @@ struct ServeEngine {
     }
 
     void complete_loop(Lane& L) {
-        cudaSetDevice(c->device);
+        bind(&L == &lanes[0] ? 0 : 1);
         for (;;) {
             int k;
             {

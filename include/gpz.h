@@ -64,6 +64,7 @@ typedef struct gpz_config {
 #define GPZ_FLAG_NO_GRAPHS 1    /* launch kernels directly instead of per-bucket CUDA graphs */
 #define GPZ_FLAG_NO_AUTOTUNE 2  /* keep the default launch shapes */
 #define GPZ_FLAG_STAGE_TIMING 4 /* record CUDA events around each stage (gpz_stage_times) */
+#define GPZ_FLAG_SM_PARTITION 8 /* serving: run the small- and large-request lanes on separate SM partitions */
 
 typedef struct gpz_desc {
     const uint8_t* in;   /* one chunk or file */
