@@ -448,13 +448,17 @@ __global__ void __launch_bounds__(T, 1) k_lookup(BatchParams bp) {
 
 // The lazy walk of lz77.rs:260-284 visits p, next(p), next(next(p)), ...
 // where next(p) depends only on pp[p] and pp[p+1].  Each 4 KiB tile is walked
-// by one warp, 32 positions at a time: within a window of 32 positions the
-// links are resolved by pointer doubling over shuffles (5 rounds).
-// k_walk_exit computes, for every position a walk can enter the tile at (its
-// first 258), where it leaves, sweeping the windows from the top down;
-// k_chain strings the tiles of a member together (entry of tile b+1 = exit of
-// tile b at its entry); k_walk_mark walks forward from the known entry and
-// emits the visited tokens in order.
+// on its own: k_walk_exit computes, for every position a walk can enter the
+// tile at (its first 258), where it leaves; k_chain strings the tiles of a
+// member together (entry of tile b+1 = exit of tile b at its entry);
+// k_walk_mark walks from the known entry and emits the visited tokens in
+// order with the tile's symbol histogram.  Two forms with identical output:
+//   warp  one warp per tile, 32 positions at a time, links inside a window
+//         resolved by pointer doubling over shuffles: little shared memory,
+//         many tiles in flight per SM -- the throughput form;
+//   block one CTA per tile, pointer doubling over all 4096 links in shared
+//         memory (13 rounds): the lowest latency per tile -- the form for
+//         small batches, where a tile's latency is the batch's.
 
 constexpr uint32_t kFull = 0xFFFFFFFFu;
 
@@ -473,7 +477,7 @@ __device__ __forceinline__ uint32_t walk_next(uint32_t i, uint32_t v, uint32_t v
 // position whose exit is known.  A link reaches at most 258 ahead, so only
 // the last 16 windows of exits are kept (ring of 512 per warp).
 template <int T>
-__global__ void __launch_bounds__(T) k_walk_exit(BatchParams bp) {
+__global__ void __launch_bounds__(T) k_walk_exit_warp(BatchParams bp) {
     constexpr int W = T / 32;
     constexpr uint32_t kRing = 512;
     __shared__ uint16_t ring[W][kRing];
@@ -527,6 +531,73 @@ __global__ void __launch_bounds__(T) k_walk_exit(BatchParams bp) {
     }
 }
 
+// ---- block form: one CTA per tile
+
+struct WalkLinks {
+    uint32_t pps[GPZ_SEG + 1];              // pp of the tile and one lookahead
+    uint16_t nxt[GPZ_SEG];                  // next position, tile-relative
+    uint16_t J[2][GPZ_SEG + GPZ_EXITS];     // doubled links, absorbing past the tile
+};
+
+template <int T>
+__device__ void walk_links(const BatchParams& bp, const MemberDesc& md, uint32_t start, uint32_t cnt, WalkLinks& w) {
+    const uint32_t n = md.len;
+    const uint32_t* ppg = bp.pp + md.in_off + start;
+    for (uint32_t i = threadIdx.x; i < cnt; i += T) w.pps[i] = ppg[i];
+    if (threadIdx.x == 0) w.pps[cnt] = (start + cnt < n) ? ppg[cnt] : 0u;
+    for (uint32_t i = cnt + threadIdx.x; i < cnt + GPZ_EXITS; i += T) {
+        w.J[0][i] = (uint16_t)i;
+        w.J[1][i] = (uint16_t)i;
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < cnt; i += T) {
+        const uint32_t l = w.pps[i] >> 16;
+        uint32_t nx = i + 1u;
+        if (l) {
+            const uint32_t l1 = w.pps[i + 1] >> 16;
+            const bool demote = (start + i + 1u < n) && l1 != 0u && l1 > l;  // lz77.rs:273-278
+            if (!demote) nx = i + l;
+        }
+        w.nxt[i] = (uint16_t)nx;
+        w.J[0][i] = (uint16_t)nx;
+    }
+    __syncthreads();
+}
+
+template <int T>
+__global__ void __launch_bounds__(T) k_walk_exit_blk(BatchParams bp) {
+    __shared__ WalkLinks w;
+    __shared__ uint32_t s_tile;
+    const int tid = threadIdx.x;
+    const uint32_t ntiles = bp.dims[0];
+    for (;;) {
+        __syncthreads();
+        if (tid == 0) s_tile = atomicAdd(&bp.counters[GPZ_CNT_EXIT], 1u);
+        __syncthreads();
+        const uint32_t t = s_tile;
+        if (t >= ntiles) break;
+        const TileDesc td = bp.tiles[t];
+        const MemberDesc md = bp.members[td.member];
+        if (td.seg + 1u == md.ntiles) continue;  // the member's last tile has no successor
+        const uint32_t start = td.seg << GPZ_SEG_LOG2, cnt = GPZ_SEG;
+        walk_links<T>(bp, md, start, cnt, w);
+        int cur = 0;
+        for (int r = 0; r < 16; r++) {
+            int ch = 0;
+            for (uint32_t i = tid; i < cnt; i += T) {
+                const uint32_t j = w.J[cur][i];
+                const uint32_t nj = j < cnt ? w.J[cur][j] : j;
+                w.J[cur ^ 1][i] = (uint16_t)nj;
+                ch |= nj != j;
+            }
+            cur ^= 1;
+            if (!__syncthreads_or(ch)) break;
+        }
+        for (int e = tid; e < GPZ_EXITS; e += T)
+            bp.tile_exit[(size_t)t * GPZ_EXITS + e] = (uint16_t)(w.J[cur][e] - cnt);
+    }
+}
+
 // Entry offset of every tile: one thread per member follows the exit tables.
 __global__ void k_chain(BatchParams bp) {
     const uint32_t nmembers = bp.dims[1];
@@ -541,6 +612,87 @@ __global__ void k_chain(BatchParams bp) {
     }
 }
 
+struct MarkSmem {
+    WalkLinks w;
+    uint8_t mark[GPZ_SEG];
+    uint32_t hist[GPZ_NSYM];
+    uint32_t wsum[32];
+    uint32_t tile;
+};
+
+template <int T>
+__global__ void __launch_bounds__(T) k_walk_mark_blk(BatchParams bp) {
+    constexpr int PER = GPZ_SEG / T;
+    __shared__ MarkSmem sm;
+    const int tid = threadIdx.x;
+    const uint32_t ntiles = bp.dims[0];
+    for (;;) {
+        __syncthreads();
+        if (tid == 0) sm.tile = atomicAdd(&bp.counters[GPZ_CNT_MARK], 1u);
+        __syncthreads();
+        const uint32_t t = sm.tile;
+        if (t >= ntiles) break;
+        const TileDesc td = bp.tiles[t];
+        const MemberDesc md = bp.members[td.member];
+        const uint32_t n = md.len, start = td.seg << GPZ_SEG_LOG2;
+        const uint32_t cnt = min(GPZ_SEG, n - start);
+        for (int i = tid; i < GPZ_NSYM; i += T) sm.hist[i] = 0;
+        for (uint32_t i = tid; i < cnt; i += T) sm.mark[i] = 0xFF;
+        walk_links<T>(bp, md, start, cnt, sm.w);
+        const uint32_t entry = bp.tile_entry[t];
+        if (tid == 0 && entry < cnt) sm.mark[entry] = 0;
+        __syncthreads();
+        // before round r the marked positions are next^k(entry), k < 2^r
+        int cur = 0;
+        for (int r = 0; r < 16; r++) {
+            int add = 0;
+            for (uint32_t i = tid; i < cnt; i += T) {
+                const uint32_t j = sm.w.J[cur][i];
+                if (sm.mark[i] <= (uint32_t)r && j < cnt) {
+                    sm.mark[j] = (uint8_t)(r + 1);
+                    add = 1;
+                }
+                sm.w.J[cur ^ 1][i] = (uint16_t)(j < cnt ? sm.w.J[cur][j] : j);
+            }
+            cur ^= 1;
+            if (!__syncthreads_or(add)) break;
+        }
+
+        // compact the visited tokens in order, histogram their symbols
+        uint32_t vis = 0, c = 0;
+        const uint32_t i0 = tid * PER;
+#pragma unroll
+        for (int k = 0; k < PER; k++) {
+            const uint32_t i = i0 + k;
+            const bool v = i < cnt && sm.mark[i] != 0xFF;
+            vis |= (uint32_t)v << k;
+            c += v;
+        }
+        uint32_t total;
+        uint32_t idx = block_excl_scan<T>(c, sm.wsum, &total);
+        uint32_t* tg = bp.tok + md.in_off + start;
+#pragma unroll
+        for (int k = 0; k < PER; k++) {
+            if (!((vis >> k) & 1u)) continue;
+            const uint32_t i = i0 + k;
+            uint32_t tv = sm.w.pps[i];
+            const uint32_t l = tv >> 16;
+            if (l && sm.w.nxt[i] == i + 1u) tv = bp.in[md.in_off + start + i];  // lazy demotion to a literal
+            tg[idx++] = tv;
+            if ((tv >> 16) == 0) {
+                atomicAdd(&sm.hist[tv & 0xFFu], 1u);
+            } else {
+                atomicAdd(&sm.hist[257u + len_row(tv >> 16)], 1u);
+                atomicAdd(&sm.hist[GPZ_NLIT + dist_row(tv & 0xFFFFu)], 1u);
+            }
+        }
+        __syncthreads();
+        uint16_t* hg = bp.tile_hist + (size_t)t * GPZ_NSYM;
+        for (int s = tid; s < GPZ_NSYM; s += T) hg[s] = (uint16_t)sm.hist[s];
+        if (tid == 0) bp.tile_ntok[t] = total;
+    }
+}
+
 // Warp-per-tile forward walk from the tile's entry: per window of 32
 // positions (aligned), the lanes on the walk are found by doubling the links
 // from the entry lane; they emit their tokens in order (a demoted match
@@ -549,7 +701,7 @@ __global__ void k_chain(BatchParams bp) {
 // current one (pp and input bytes) are loaded ahead, since the walk usually
 // moves on to them.
 template <int T>
-__global__ void __launch_bounds__(T) k_walk_mark(BatchParams bp) {
+__global__ void __launch_bounds__(T) k_walk_mark_warp(BatchParams bp) {
     constexpr int W = T / 32;
     __shared__ uint32_t hist_all[W][GPZ_NSYM];
     const int lane = threadIdx.x & 31;
@@ -658,6 +810,7 @@ constexpr int kCrcSlices = 256;  // threads folding member bytes into the CRC
 
 struct TreeScratch {
     uint32_t key[512];  // (weight << 9 | symbol), sorted; unused = 0xFFFFFFFF
+    uint32_t ukey[GPZ_NLIT];  // the same keys in symbol order (block builder)
     uint32_t w[GPZ_NLIT];
     uint32_t ifreq[GPZ_NLIT];
     uint16_t lparent[GPZ_NLIT];
@@ -831,6 +984,7 @@ struct HuffSmem {
     uint32_t crcv[kCrcSlices];
     uint32_t crcx[8];
     uint32_t member, hbits, total, nrle, nlit, ndist, ok, crc;
+    uint32_t bt_used[2], bt_only[2], bt_max[2], bt_done[2];
 };
 
 // Codes one run of L equal code lengths v emits (rle_encode_lengths,
@@ -895,7 +1049,6 @@ __device__ void warp_rle(Smem& sm, int lane) {
     const int ndist = lastd > 1 ? lastd : 1;
     const int n = nlit + ndist;
     for (int i = lane; i < n; i += 32) sm.comb[i] = i < nlit ? ll[i] : dl[i - nlit];
-    if (lane < 19) sm.meta_freq[lane] = 0;
     __syncwarp();
     constexpr int C = 10;  // 32 x 10 >= 286 + 30
     const int lo = lane * C, hi = min(n, lo + C);
@@ -934,7 +1087,20 @@ __device__ void warp_rle(Smem& sm, int lane) {
     for (int i = lo; i < hi; i++)
         if (is_start(i)) off += run_codes(sm.comb[i], run_end(i) - i, sm.rle_code + off, sm.rle_extra + off);
     __syncwarp();
-    for (int q = lane; q < total; q += 32) atomicAdd(&sm.meta_freq[sm.rle_code[q]], 1u);
+    // meta symbol counts: each lane holds up to 10 codes, one warp sum per symbol
+    uint32_t mc[C];
+#pragma unroll
+    for (int u = 0; u < C; u++) {
+        const int q = lane + 32 * u;
+        mc[u] = q < total ? sm.rle_code[q] : 0xFFu;
+    }
+    for (uint32_t c = 0; c < 19; c++) {
+        uint32_t k = 0;
+#pragma unroll
+        for (int u = 0; u < C; u++) k += mc[u] == c;
+        k = __reduce_add_sync(0xFFFFFFFFu, k);
+        if (lane == 0) sm.meta_freq[c] = k;
+    }
     if (lane == 0) {
         sm.nrle = (uint32_t)total;
         sm.nlit = (uint32_t)nlit;
@@ -995,6 +1161,162 @@ __device__ void warp_header(Smem& sm, int lane) {
     }
     if (lane == 0) sm.hbits = base + total;
     __syncwarp();
+}
+
+// try_build_code_lengths (huffman.rs:26-60) for the litlen and distance
+// alphabets at once (15-bit limit), by the whole CTA: the same two-queue
+// evaluation of standard_huffman's (freq, id) heap as warp_code_lengths, with
+// the leaves ranked by all threads (rank = number of smaller keys), one
+// thread per alphabet for the merge (the next leaf and the next two internal
+// nodes kept in registers), and depths by pointer jumping over all threads.
+// Each alphabet halves its weights until its longest code fits, on its own.
+// Leaves sm.ok = 0 if an alphabet cannot be coded (never expected).
+template <int T, class Smem>
+__device__ void block_code_lengths(Smem& sm, int tid) {
+    constexpr int kMax = 15;
+    const int nsym[2] = {GPZ_NLIT, GPZ_NDIST};
+    const int nall = GPZ_NLIT + GPZ_NDIST;
+    auto alpha = [&](int idx, int& i) {
+        const int a = idx < GPZ_NLIT ? 0 : 1;
+        i = idx - (a ? GPZ_NLIT : 0);
+        return a;
+    };
+    if (tid < 2) {
+        sm.bt_used[tid] = 0;
+        sm.bt_only[tid] = 0;
+        sm.bt_done[tid] = 0;
+    }
+    __syncthreads();
+    for (int idx = tid; idx < nall; idx += T) {
+        int i;
+        const int a = alpha(idx, i);
+        const uint32_t f = sm.freq[idx];
+        sm.tree[a].w[i] = f;
+        sm.lens[idx] = 0;
+        if (f) {
+            atomicAdd(&sm.bt_used[a], 1u);
+            atomicMax(&sm.bt_only[a], (uint32_t)i);
+        }
+    }
+    __syncthreads();
+    if (tid < 2) {
+        const uint32_t used = sm.bt_used[tid];
+        if (used <= 1) {
+            if (used == 1) sm.lens[(tid ? GPZ_NLIT : 0) + sm.bt_only[tid]] = 1;
+            sm.bt_done[tid] = 1;
+        } else if (used > (1u << kMax)) {
+            sm.bt_done[tid] = 1;
+            sm.ok = 0;
+        }
+    }
+    __syncthreads();
+    for (int iter = 0; iter < 64 && !(sm.bt_done[0] && sm.bt_done[1]); iter++) {
+        for (int idx = tid; idx < nall; idx += T) {
+            int i;
+            const int a = alpha(idx, i);
+            const uint32_t w = sm.tree[a].w[i];
+            sm.tree[a].ukey[i] = w ? ((w << 9) | (uint32_t)i) : 0xFFFFFFFFu;
+        }
+        if (tid < 2) sm.bt_max[tid] = 0;
+        __syncthreads();
+        // leaves in (weight, symbol) order: rank = number of smaller keys
+        for (int idx = tid; idx < nall; idx += T) {
+            int i;
+            const int a = alpha(idx, i);
+            if (sm.bt_done[a]) continue;
+            const uint32_t k = sm.tree[a].ukey[i];
+            if (k == 0xFFFFFFFFu) continue;
+            uint32_t r = 0;
+            for (int j = 0; j < nsym[a]; j++) r += sm.tree[a].ukey[j] < k;
+            sm.tree[a].key[r] = k;
+        }
+        __syncthreads();
+        // two-queue merge, one thread per alphabet (warps 0 and 1)
+        if ((tid == 0 || tid == 32) && !sm.bt_done[tid >> 5]) {
+            TreeScratch& s = sm.tree[tid >> 5];
+            const uint32_t used = sm.bt_used[tid >> 5];
+            const uint32_t INF = 0xFFFFFFFFu;
+            const int nint = (int)used - 1;
+            int li = 0, ii = 0, ni = 0;
+            uint32_t lf = s.key[0] >> 9, lf2 = used > 1 ? s.key[1] >> 9 : INF;
+            uint32_t fi = INF, fi2 = INF;  // front and second of the internal queue [ii, ni)
+            for (int k = 0; k < nint; k++) {
+                uint32_t f2[2];
+#pragma unroll
+                for (int q = 0; q < 2; q++) {
+                    if (li < (int)used && lf <= fi) {
+                        f2[q] = lf;
+                        s.lparent[li++] = (uint16_t)ni;
+                        lf = lf2;
+                        lf2 = li + 1 < (int)used ? s.key[li + 1] >> 9 : INF;
+                    } else {
+                        f2[q] = fi;
+                        s.iparent[ii++] = (uint16_t)ni;
+                        fi = fi2;
+                        fi2 = ii + 1 < ni ? s.ifreq[ii + 1] : INF;
+                    }
+                }
+                const uint32_t nf = f2[0] + f2[1];
+                s.ifreq[ni] = nf;
+                if (ii == ni) fi = nf;
+                else if (ii + 1 == ni) fi2 = nf;
+                ni++;
+            }
+        }
+        __syncthreads();
+        // depths: pointer jumping over the internal nodes' parent links
+        const int nint0 = sm.bt_done[0] ? 0 : (int)sm.bt_used[0] - 1;
+        const int nint1 = sm.bt_done[1] ? 0 : (int)sm.bt_used[1] - 1;
+        for (int idx = tid; idx < nint0 + nint1; idx += T) {
+            const int a = idx < nint0 ? 0 : 1;
+            const int j = idx - (a ? nint0 : 0), root = (a ? nint1 : nint0) - 1;
+            TreeScratch& s = sm.tree[a];
+            s.anc[0][j] = (uint16_t)(j == root ? root : s.iparent[j]);
+            s.dep[0][j] = (uint16_t)(j == root ? 0 : 1);
+        }
+        __syncthreads();
+        int cur = 0;
+        for (int r = 0; r < 9; r++) {
+            for (int idx = tid; idx < nint0 + nint1; idx += T) {
+                const int a = idx < nint0 ? 0 : 1;
+                const int j = idx - (a ? nint0 : 0);
+                TreeScratch& s = sm.tree[a];
+                const int an = s.anc[cur][j];
+                s.dep[cur ^ 1][j] = (uint16_t)(s.dep[cur][j] + s.dep[cur][an]);
+                s.anc[cur ^ 1][j] = s.anc[cur][an];
+            }
+            cur ^= 1;
+            __syncthreads();
+        }
+        const int u0 = sm.bt_done[0] ? 0 : (int)sm.bt_used[0];
+        const int u1 = sm.bt_done[1] ? 0 : (int)sm.bt_used[1];
+        for (int idx = tid; idx < u0 + u1; idx += T) {
+            const int a = idx < u0 ? 0 : 1;
+            const int k = idx - (a ? u0 : 0);
+            TreeScratch& s = sm.tree[a];
+            const uint32_t d = s.dep[cur][s.lparent[k]] + 1u;
+            sm.lens[(a ? GPZ_NLIT : 0) + (s.key[k] & 511u)] = (uint8_t)d;
+            atomicMax(&sm.bt_max[a], d);
+        }
+        __syncthreads();
+        // an alphabet whose longest code fits is done; the other halves
+        const bool fit0 = sm.bt_done[0] || sm.bt_max[0] <= (uint32_t)kMax;
+        const bool fit1 = sm.bt_done[1] || sm.bt_max[1] <= (uint32_t)kMax;
+        for (int idx = tid; idx < nall; idx += T) {
+            int i;
+            const int a = alpha(idx, i);
+            if (a == 0 ? fit0 : fit1) continue;
+            uint32_t& w = sm.tree[a].w[i];
+            if (w > 1u) w >>= 1;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            if (fit0) sm.bt_done[0] = 1;
+            if (fit1) sm.bt_done[1] = 1;
+        }
+        __syncthreads();
+    }
+    if (tid == 0 && !(sm.bt_done[0] && sm.bt_done[1])) sm.ok = 0;
 }
 
 // Per member: code lengths and codes, the dynamic block header
@@ -1093,13 +1415,8 @@ __global__ void __launch_bounds__(kHuffThreads) k_huff(BatchParams bp) {
             }
         }
 
-        // litlen (warp 0) and distance (warp 1) code lengths, 15-bit limit
-        if (warp < 2) {
-            const bool ok = warp == 0 ? warp_code_lengths(sm.freq, GPZ_NLIT, 15, sm.lens, sm.tree[0])
-                                      : warp_code_lengths(sm.freq + GPZ_NLIT, GPZ_NDIST, 15, sm.lens + GPZ_NLIT,
-                                                          sm.tree[1]);
-            if (!ok && lane == 0) sm.ok = 0;
-        }
+        // litlen and distance code lengths, 15-bit limit, by the whole CTA
+        block_code_lengths<kHuffThreads>(sm, tid);
         __syncthreads();
 
         // fix-ups (deflate.rs:854-867)
@@ -1522,18 +1839,25 @@ int gpz_launch_batch(const BatchParams& bp, const LaunchShape& ls, void* stream,
         default: k_lookup<1024><<<gl, 1024, LookupSmem::kBytes, s>>>(bp); break;
     }
     mark(2);
+    // walk form: 1024 selects the block form (512 threads per tile CTA);
+    // 256 / 512 the warp form with that many threads per CTA
     const int gw = grid_of(ls.walk_grid, bp.ntiles);
     const int gc = ls.huff_grid > 0 ? ls.huff_grid : (nm + 127) / 128;
     switch (ls.walk_threads) {
-        case 256:
-            k_walk_exit<256><<<gw, 256, 0, s>>>(bp);
+        case 1024:
+            k_walk_exit_blk<512><<<gw, 512, 0, s>>>(bp);
             k_chain<<<gc, 128, 0, s>>>(bp);
-            k_walk_mark<256><<<gw, 256, 0, s>>>(bp);
+            k_walk_mark_blk<512><<<gw, 512, 0, s>>>(bp);
+            break;
+        case 256:
+            k_walk_exit_warp<256><<<gw, 256, 0, s>>>(bp);
+            k_chain<<<gc, 128, 0, s>>>(bp);
+            k_walk_mark_warp<256><<<gw, 256, 0, s>>>(bp);
             break;
         default:
-            k_walk_exit<512><<<gw, 512, 0, s>>>(bp);
+            k_walk_exit_warp<512><<<gw, 512, 0, s>>>(bp);
             k_chain<<<gc, 128, 0, s>>>(bp);
-            k_walk_mark<512><<<gw, 512, 0, s>>>(bp);
+            k_walk_mark_warp<512><<<gw, 512, 0, s>>>(bp);
             break;
     }
     mark(3);
@@ -1565,9 +1889,10 @@ int gpz_occupancy(LaunchShape* persistent) {
     persistent->lookup_grid = sms * occ(persistent->lookup_threads == 512 ? (const void*)k_lookup<512>
                                                                            : (const void*)k_lookup<1024>,
                                         persistent->lookup_threads, LookupSmem::kBytes);
-    persistent->walk_grid = sms * occ(persistent->walk_threads == 256 ? (const void*)k_walk_mark<256>
-                                                                       : (const void*)k_walk_mark<512>,
-                                      persistent->walk_threads, 0);
+    const void* walk_fn = persistent->walk_threads == 1024 ? (const void*)k_walk_mark_blk<512>
+                          : persistent->walk_threads == 256  ? (const void*)k_walk_mark_warp<256>
+                                                             : (const void*)k_walk_mark_warp<512>;
+    persistent->walk_grid = sms * occ(walk_fn, persistent->walk_threads == 1024 ? 512 : persistent->walk_threads, 0);
     persistent->huff_grid = sms * occ((const void*)k_huff, kHuffThreads, 0);
     persistent->emit_grid = sms * occ(persistent->emit_threads == 256 ? (const void*)k_emit<256>
                                                                        : (const void*)k_emit<512>,

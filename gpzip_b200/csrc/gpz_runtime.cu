@@ -508,9 +508,11 @@ int launch(gpz_ctx* c, Slot& sl, const BatchParams& bp, const LaunchShape& shape
 }
 
 // Persistent default shape for every bucket; tuned lazily on first use.
+// Small batches (up to 512 tiles) walk in the block form, whose latency per
+// tile is lowest; larger ones in the warp form, whose throughput is highest.
 void default_shapes(gpz_ctx* c) {
     for (int b = 0; b < kBuckets; b++) {
-        LaunchShape s{1024, 0, 512, 0, 512, 0, 0, 0};
+        LaunchShape s{1024, 0, b <= 1 ? 1024 : 512, 0, 512, 0, 0, 0};
         gpz_occupancy(&s);
         c->shape[b] = s;
     }
@@ -520,7 +522,7 @@ void default_shapes(gpz_ctx* c) {
 // CTA, with persistent grids from occupancy) runs the batch once -- every
 // shape gives the same output -- and the fastest becomes the bucket's shape.
 int autotune(gpz_ctx* c, Slot& sl, const BatchParams& bp, const DrainTarget* dt, cudaStream_t s) {
-    const int lt[2] = {1024, 512}, wt[2] = {512, 256}, et[2] = {512, 256};
+    const int lt[2] = {1024, 512}, wt[2] = {512, 1024}, et[2] = {512, 256};
     float best = 1e30f;
     LaunchShape best_s = c->shape[sl.bucket];
     cudaEvent_t a, b;
@@ -620,7 +622,7 @@ int submit_slot(gpz_ctx* c, Slot& sl, const gpz_desc* d, size_t count, const Lau
     const bool timing = (c->flags & GPZ_FLAG_STAGE_TIMING) != 0;
     if (pol.exact) {
         // one launch per kernel, grids sized to this batch, no graph
-        const LaunchShape exact{1024, 0, 512, 0, 512, 0, 0, 0};
+        const LaunchShape exact{1024, 0, 1024, 0, 512, 0, 0, 0};
         rc = launch(c, sl, bp, exact, false, &dt, timing, s);
     } else {
         bool tuned;
@@ -971,7 +973,7 @@ struct ServeEngine {
         cudaDeviceGetStreamPriorityRange(&least, &greatest);
         Lane& sm = lanes[0];
         sm.nslots = 3;
-        sm.batch_cap = 4u << 20;
+        sm.batch_cap = 2u << 20;  // <= 512 tiles + one per unit: the low-latency buckets
         sm.max_units = 1024;
         sm.pol = LaunchPolicy{false, false, true, true, 100};  // persistent default shape, graphs, k_fetch
         Lane& lg = lanes[1];
@@ -1530,8 +1532,8 @@ int gpz_get_shape(gpz_ctx* c, gpz_shape* s) {
 int gpz_set_shape(gpz_ctx* c, const gpz_shape* s) {
     if (!c || !s) return GPZ_E_ARG;
     auto ok_t = [](int t) { return t == 256 || t == 512; };
-    if (!(s->lookup_threads == 512 || s->lookup_threads == 1024) || !ok_t(s->walk_threads) ||
-        !ok_t(s->emit_threads) || s->lookup_grid < 0 || s->walk_grid < 0 || s->emit_grid < 0)
+    if (!(s->lookup_threads == 512 || s->lookup_threads == 1024) ||
+        !(s->walk_threads == 256 || s->walk_threads == 512 || s->walk_threads == 1024) || !ok_t(s->emit_threads) || s->lookup_grid < 0 || s->walk_grid < 0 || s->emit_grid < 0)
         return GPZ_E_ARG;
     std::lock_guard<std::mutex> lk(c->mu);
     c->fixed = LaunchShape{s->lookup_threads, s->lookup_grid, s->walk_threads, s->walk_grid, s->emit_threads,

@@ -53,7 +53,7 @@ def test_every_launch_shape_gives_the_same_bytes(ctx):
     want = O.gzip_chunk(data, 131072)
     keep = ctx.get_shape()
     for lt in (1024, 512):
-        for wt in (512, 256):
+        for wt in (1024, 512, 256):
             for et in (512, 256):
                 ctx.set_shape(native.Shape(lt, 0, wt, 0, et, 0))
                 assert ctx.compress_chunk(data) == want, (lt, wt, et)
