@@ -58,6 +58,7 @@ def parse():
     ap.add_argument("--serve-only", action="store_true", help="run only the serving measurement")
     ap.add_argument("--cpu-sample-mib", type=int, default=8)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baselines (quick runs)")
+    ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-file batched vs plain measurement")
     ap.add_argument("--device-only", action="store_true",
                     help="only the device-resident steps (no e2e, no CPU baselines): for profiling")
     return ap.parse_args()
@@ -489,6 +490,14 @@ def main():
         rates = [int(x) for x in args.serve_rates.split(",") if x]
         serving = run_serving(local, args.serve_seconds, rates)
 
+    # the 1,000-file uneven mix: batched persistent path vs the plain
+    # one-launch-per-chunk path through the host API
+    uneven = None
+    if rank == 0 and not (args.device_only or args.no_uneven):
+        uctx = native.Context(device=local, member_bytes=MEMBER)
+        uneven = run_uneven(uctx, argparse.Namespace(steps=2, warmup=1), torch.cuda.current_stream())
+        uctx.close()
+
     if world > 1:
         dist.barrier()
     if rank == 0:
@@ -514,6 +523,7 @@ def main():
             "ratio": round(ratio, 5),
             "parity": parity,
             "serving": serving,
+            "uneven": uneven,
         }
         print(json.dumps(line), flush=True)
     ctx.close()

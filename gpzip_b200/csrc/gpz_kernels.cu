@@ -805,7 +805,7 @@ __global__ void __launch_bounds__(T) k_walk_mark_warp(BatchParams bp) {
 
 // ================================================================== k_huff
 
-constexpr int kHuffThreads = 256;
+constexpr int kHuffThreads = 512;  // two groups of 256: code construction and CRC
 constexpr int kCrcSlices = 256;  // threads folding member bytes into the CRC
 
 struct TreeScratch {
@@ -1171,8 +1171,8 @@ __device__ void warp_header(Smem& sm, int lane) {
 // nodes kept in registers), and depths by pointer jumping over all threads.
 // Each alphabet halves its weights until its longest code fits, on its own.
 // Leaves sm.ok = 0 if an alphabet cannot be coded (never expected).
-template <int T, class Smem>
-__device__ void block_code_lengths(Smem& sm, int tid) {
+template <int T, class Smem, class Sync>
+__device__ void block_code_lengths(Smem& sm, int tid, Sync sync) {
     constexpr int kMax = 15;
     const int nsym[2] = {GPZ_NLIT, GPZ_NDIST};
     const int nall = GPZ_NLIT + GPZ_NDIST;
@@ -1186,7 +1186,7 @@ __device__ void block_code_lengths(Smem& sm, int tid) {
         sm.bt_only[tid] = 0;
         sm.bt_done[tid] = 0;
     }
-    __syncthreads();
+    sync();
     for (int idx = tid; idx < nall; idx += T) {
         int i;
         const int a = alpha(idx, i);
@@ -1198,7 +1198,7 @@ __device__ void block_code_lengths(Smem& sm, int tid) {
             atomicMax(&sm.bt_only[a], (uint32_t)i);
         }
     }
-    __syncthreads();
+    sync();
     if (tid < 2) {
         const uint32_t used = sm.bt_used[tid];
         if (used <= 1) {
@@ -1209,7 +1209,7 @@ __device__ void block_code_lengths(Smem& sm, int tid) {
             sm.ok = 0;
         }
     }
-    __syncthreads();
+    sync();
     for (int iter = 0; iter < 64 && !(sm.bt_done[0] && sm.bt_done[1]); iter++) {
         for (int idx = tid; idx < nall; idx += T) {
             int i;
@@ -1218,7 +1218,7 @@ __device__ void block_code_lengths(Smem& sm, int tid) {
             sm.tree[a].ukey[i] = w ? ((w << 9) | (uint32_t)i) : 0xFFFFFFFFu;
         }
         if (tid < 2) sm.bt_max[tid] = 0;
-        __syncthreads();
+        sync();
         // leaves in (weight, symbol) order: rank = number of smaller keys
         for (int idx = tid; idx < nall; idx += T) {
             int i;
@@ -1230,7 +1230,7 @@ __device__ void block_code_lengths(Smem& sm, int tid) {
             for (int j = 0; j < nsym[a]; j++) r += sm.tree[a].ukey[j] < k;
             sm.tree[a].key[r] = k;
         }
-        __syncthreads();
+        sync();
         // two-queue merge, one thread per alphabet (warps 0 and 1)
         if ((tid == 0 || tid == 32) && !sm.bt_done[tid >> 5]) {
             TreeScratch& s = sm.tree[tid >> 5];
@@ -1263,7 +1263,7 @@ __device__ void block_code_lengths(Smem& sm, int tid) {
                 ni++;
             }
         }
-        __syncthreads();
+        sync();
         // depths: pointer jumping over the internal nodes' parent links
         const int nint0 = sm.bt_done[0] ? 0 : (int)sm.bt_used[0] - 1;
         const int nint1 = sm.bt_done[1] ? 0 : (int)sm.bt_used[1] - 1;
@@ -1274,7 +1274,7 @@ __device__ void block_code_lengths(Smem& sm, int tid) {
             s.anc[0][j] = (uint16_t)(j == root ? root : s.iparent[j]);
             s.dep[0][j] = (uint16_t)(j == root ? 0 : 1);
         }
-        __syncthreads();
+        sync();
         int cur = 0;
         for (int r = 0; r < 9; r++) {
             for (int idx = tid; idx < nint0 + nint1; idx += T) {
@@ -1286,7 +1286,7 @@ __device__ void block_code_lengths(Smem& sm, int tid) {
                 s.anc[cur ^ 1][j] = s.anc[cur][an];
             }
             cur ^= 1;
-            __syncthreads();
+            sync();
         }
         const int u0 = sm.bt_done[0] ? 0 : (int)sm.bt_used[0];
         const int u1 = sm.bt_done[1] ? 0 : (int)sm.bt_used[1];
@@ -1298,7 +1298,7 @@ __device__ void block_code_lengths(Smem& sm, int tid) {
             sm.lens[(a ? GPZ_NLIT : 0) + (s.key[k] & 511u)] = (uint8_t)d;
             atomicMax(&sm.bt_max[a], d);
         }
-        __syncthreads();
+        sync();
         // an alphabet whose longest code fits is done; the other halves
         const bool fit0 = sm.bt_done[0] || sm.bt_max[0] <= (uint32_t)kMax;
         const bool fit1 = sm.bt_done[1] || sm.bt_max[1] <= (uint32_t)kMax;
@@ -1309,12 +1309,12 @@ __device__ void block_code_lengths(Smem& sm, int tid) {
             uint32_t& w = sm.tree[a].w[i];
             if (w > 1u) w >>= 1;
         }
-        __syncthreads();
+        sync();
         if (tid == 0) {
             if (fit0) sm.bt_done[0] = 1;
             if (fit1) sm.bt_done[1] = 1;
         }
-        __syncthreads();
+        sync();
     }
     if (tid == 0 && !(sm.bt_done[0] && sm.bt_done[1])) sm.ok = 0;
 }
@@ -1325,7 +1325,13 @@ __device__ void block_code_lengths(Smem& sm, int tid) {
 __global__ void __launch_bounds__(kHuffThreads) k_huff(BatchParams bp) {
     __shared__ HuffSmem sm;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    constexpr int NW = kHuffThreads / 32;
+    // threads [0, 256): code construction, header and bit plan (named
+    // barrier 1); threads [256, 512): the member's CRC-32 (named barrier 2).
+    // The two groups run side by side and meet once per member.
+    constexpr int G = kHuffThreads / 2, NW = G / 32;
+    const bool hgroup = tid < G;
+    auto hsync = [] { asm volatile("bar.sync 1, %0;" ::"n"(G) : "memory"); };
+    auto csync = [] { asm volatile("bar.sync 2, %0;" ::"n"(G) : "memory"); };
 
     // slice-by-8 CRC tables: crctab[k][b] = CRC of byte b followed by k zeros
     for (int i = tid; i < 256; i += kHuffThreads) {
@@ -1351,40 +1357,33 @@ __global__ void __launch_bounds__(kHuffThreads) k_huff(BatchParams bp) {
         if (m >= nmembers) break;
         const MemberDesc md = bp.members[m];
 
-        // member symbol counts = sum of its tiles' histograms, + EOB
-        for (int q = tid; q < GPZ_NSYM; q += kHuffThreads) {
-            uint32_t f = 0;
-            const uint16_t* h = bp.tile_hist + (size_t)md.tile_base * GPZ_NSYM + q;
-            for (uint32_t j = 0; j < md.ntiles; j++) f += h[(size_t)j * GPZ_NSYM];
-            sm.freq[q] = f + (q == 256 ? 1u : 0u);
-        }
-        if (tid == 0) sm.ok = 1;
-
-        // CRC-32 of the member (crc32fast at deflate.rs:974).  The aligned
-        // 8-byte words are cut into kCrcSlices equal slices, front-padded
-        // with zero words (which a zero-init CRC ignores); each slice is
-        // folded with slice-by-8, then the slices are combined pairwise,
-        // crc(A||B) = crc(A) * x^(8|B|) + crc(B), in a tree.
-        {
+        if (!hgroup) {
+            // CRC-32 of the member (crc32fast at deflate.rs:974).  The
+            // aligned 8-byte words are cut into kCrcSlices equal slices,
+            // front-padded with zero words (which a zero-init CRC ignores);
+            // each slice is folded with slice-by-8, then the slices are
+            // combined pairwise, crc(A||B) = crc(A) * x^(8|B|) + crc(B), in a
+            // tree.
+            const int ct = tid - G;
             const uint32_t L = md.len, W = L >> 3;
             const uint32_t per = (W + kCrcSlices - 1) / kCrcSlices;
             const uint32_t padw = per * kCrcSlices - W;
-            if (tid < kCrcSlices) {
+            {
                 const uint2* words = reinterpret_cast<const uint2*>(bp.in + md.in_off);
                 uint32_t c = 0;
                 // eight words loaded ahead of the fold (a padding word is zero)
                 constexpr uint32_t kAhead = 8;
-                for (uint32_t v0 = tid * per; v0 < (tid + 1) * per; v0 += kAhead) {
+                for (uint32_t v0 = ct * per; v0 < (ct + 1) * per; v0 += kAhead) {
                     uint2 wv[kAhead];
 #pragma unroll
                     for (uint32_t u = 0; u < kAhead; u++) {
                         const uint32_t v = v0 + u;
                         wv[u] = make_uint2(0u, 0u);
-                        if (v < (tid + 1) * per && v >= padw) wv[u] = __ldg(words + (v - padw));
+                        if (v < (ct + 1) * per && v >= padw) wv[u] = __ldg(words + (v - padw));
                     }
 #pragma unroll
                     for (uint32_t u = 0; u < kAhead; u++) {
-                        if (v0 + u >= (tid + 1) * per) break;
+                        if (v0 + u >= (ct + 1) * per) break;
                         const uint32_t lo = wv[u].x ^ c, hi = wv[u].y;
                         c = sm.crctab[7 * 256 + (lo & 0xFFu)] ^ sm.crctab[6 * 256 + ((lo >> 8) & 0xFFu)] ^
                             sm.crctab[5 * 256 + ((lo >> 16) & 0xFFu)] ^ sm.crctab[4 * 256 + (lo >> 24)] ^
@@ -1392,98 +1391,107 @@ __global__ void __launch_bounds__(kHuffThreads) k_huff(BatchParams bp) {
                             sm.crctab[1 * 256 + ((hi >> 16) & 0xFFu)] ^ sm.crctab[hi >> 24];
                     }
                 }
-                sm.crcv[tid] = c;
+                sm.crcv[ct] = c;
             }
-            if (tid == 0) {
+            if (ct == 0) {
                 uint32_t x = x8pow(8u * per);
                 for (int j = 0; j < 8; j++) {
                     sm.crcx[j] = x;
                     x = gf2_mulmod(x, x);
                 }
             }
-            __syncthreads();
+            csync();
             for (int j = 0; j < 8; j++) {
                 const int span = 1 << j;
-                if (tid < kCrcSlices && (tid & (2 * span - 1)) == 0)
-                    sm.crcv[tid] = gf2_mulmod(sm.crcv[tid], sm.crcx[j]) ^ sm.crcv[tid + span];
-                __syncthreads();
+                if ((ct & (2 * span - 1)) == 0) sm.crcv[ct] = gf2_mulmod(sm.crcv[ct], sm.crcx[j]) ^ sm.crcv[ct + span];
+                csync();
             }
-            if (tid == 0) {
+            if (ct == 0) {
                 uint32_t c = sm.crcv[0];
                 for (uint32_t i = W << 3; i < L; i++) c = sm.crctab[(c ^ bp.in[md.in_off + i]) & 0xFFu] ^ (c >> 8);
                 sm.crc = ~(gf2_mulmod(0xFFFFFFFFu, x8pow(L)) ^ c);
             }
-        }
-
-        // litlen and distance code lengths, 15-bit limit, by the whole CTA
-        block_code_lengths<kHuffThreads>(sm, tid);
-        __syncthreads();
-
-        // fix-ups (deflate.rs:854-867)
-        if (warp == 0) {
-            uint8_t* ll = sm.lens;
-            uint8_t* dl = sm.lens + GPZ_NLIT;
-            const uint32_t dm = __ballot_sync(0xFFFFFFFFu, lane < GPZ_NDIST && dl[lane] != 0);
-            int used_l = 0;
-            for (int i = lane; i < GPZ_NLIT; i += 32) used_l += ll[i] != 0;
-            used_l = __reduce_add_sync(0xFFFFFFFFu, used_l);
-            __syncwarp();
-            if (lane == 0) {
-                if (dm == 0) {
-                    dl[0] = 1;
-                    dl[1] = 1;
-                } else if (__popc(dm) == 1) {
-                    const int only = __ffs(dm) - 1;
-                    dl[only] = 1;
-                    dl[1 - (only < 1 ? only : 1)] = 1;
-                }
-                if (used_l < 2) {
-                    ll[0] = 1;
-                    ll[256] = 1;
-                }
+        } else {
+            // member symbol counts = sum of its tiles' histograms, + EOB
+            for (int q = tid; q < GPZ_NSYM; q += G) {
+                uint32_t f = 0;
+                const uint16_t* h = bp.tile_hist + (size_t)md.tile_base * GPZ_NSYM + q;
+                for (uint32_t j = 0; j < md.ntiles; j++) f += h[(size_t)j * GPZ_NSYM];
+                sm.freq[q] = f + (q == 256 ? 1u : 0u);
             }
-            __syncwarp();
-        }
-        __syncthreads();
-        // canonical codes (warps 0, 1); trims + RLE (deflate.rs:254-335) on warp 2
-        if (warp == 0) warp_canonical(sm.lens, GPZ_NLIT, sm.codes);
-        else if (warp == 1) warp_canonical(sm.lens + GPZ_NLIT, GPZ_NDIST, sm.codes + GPZ_NLIT);
-        else if (warp == 2) warp_rle(sm, lane);
-        __syncthreads();
-        // meta code lengths, 7-bit limit (deflate.rs:896-903), and codes
-        if (warp == 0) {
-            const bool ok = warp_code_lengths(sm.meta_freq, 19, 7, sm.meta_lens, sm.tree[0]);
-            if (!ok && lane == 0) sm.ok = 0;
-            __syncwarp();
-            warp_canonical(sm.meta_lens, 19, sm.meta_codes);
-        }
-        __syncthreads();
-        // header bits (deflate.rs:911-932), LSB first
-        if (warp == 0) warp_header(sm, lane);
-        __syncthreads();
+            if (tid == 0) sm.ok = 1;
+            hsync();
 
-        // bits per symbol occurrence (code + extra); total member bits
-        uint32_t part = 0;
-        for (int q = tid; q < GPZ_NSYM; q += kHuffThreads) {
-            const uint32_t cl = sm.codes[q] >> 16;
-            uint32_t extra = 0;
-            if (q >= 257 && q < GPZ_NLIT) extra = len_extra_bits((uint32_t)q - 257u);
-            else if (q >= GPZ_NLIT) extra = dist_extra_bits((uint32_t)q - GPZ_NLIT);
-            sm.blen[q] = cl + extra;
-            part += sm.freq[q] * (cl + extra);
+            // litlen and distance code lengths, 15-bit limit
+            block_code_lengths<G>(sm, tid, hsync);
+            hsync();
+
+            // fix-ups (deflate.rs:854-867)
+            if (warp == 0) {
+                uint8_t* ll = sm.lens;
+                uint8_t* dl = sm.lens + GPZ_NLIT;
+                const uint32_t dm = __ballot_sync(0xFFFFFFFFu, lane < GPZ_NDIST && dl[lane] != 0);
+                int used_l = 0;
+                for (int i = lane; i < GPZ_NLIT; i += 32) used_l += ll[i] != 0;
+                used_l = __reduce_add_sync(0xFFFFFFFFu, used_l);
+                __syncwarp();
+                if (lane == 0) {
+                    if (dm == 0) {
+                        dl[0] = 1;
+                        dl[1] = 1;
+                    } else if (__popc(dm) == 1) {
+                        const int only = __ffs(dm) - 1;
+                        dl[only] = 1;
+                        dl[1 - (only < 1 ? only : 1)] = 1;
+                    }
+                    if (used_l < 2) {
+                        ll[0] = 1;
+                        ll[256] = 1;
+                    }
+                }
+                __syncwarp();
+            }
+            hsync();
+            // canonical codes (warps 0, 1); trims + RLE (deflate.rs:254-335) on warp 2
+            if (warp == 0) warp_canonical(sm.lens, GPZ_NLIT, sm.codes);
+            else if (warp == 1) warp_canonical(sm.lens + GPZ_NLIT, GPZ_NDIST, sm.codes + GPZ_NLIT);
+            else if (warp == 2) warp_rle(sm, lane);
+            hsync();
+            // meta code lengths, 7-bit limit (deflate.rs:896-903), and codes
+            if (warp == 0) {
+                const bool ok = warp_code_lengths(sm.meta_freq, 19, 7, sm.meta_lens, sm.tree[0]);
+                if (!ok && lane == 0) sm.ok = 0;
+                __syncwarp();
+                warp_canonical(sm.meta_lens, 19, sm.meta_codes);
+            }
+            hsync();
+            // header bits (deflate.rs:911-932), LSB first
+            if (warp == 0) warp_header(sm, lane);
+            hsync();
+
+            // bits per symbol occurrence (code + extra); total member bits
+            uint32_t part = 0;
+            for (int q = tid; q < GPZ_NSYM; q += G) {
+                const uint32_t cl = sm.codes[q] >> 16;
+                uint32_t extra = 0;
+                if (q >= 257 && q < GPZ_NLIT) extra = len_extra_bits((uint32_t)q - 257u);
+                else if (q >= GPZ_NLIT) extra = dist_extra_bits((uint32_t)q - GPZ_NLIT);
+                sm.blen[q] = cl + extra;
+                part += sm.freq[q] * (cl + extra);
+            }
+            part = __reduce_add_sync(0xFFFFFFFFu, part);
+            if (lane == 0) sm.red[warp] = part;
+            // exact bit plan per tile from the tile histograms
+            hsync();
+            for (uint32_t j = warp; j < md.ntiles; j += NW) {
+                const uint16_t* h = bp.tile_hist + (size_t)(md.tile_base + j) * GPZ_NSYM;
+                uint32_t sbits = 0;
+                for (int q = lane; q < GPZ_NSYM; q += 32) sbits += (uint32_t)h[q] * sm.blen[q];
+                sbits = __reduce_add_sync(0xFFFFFFFFu, sbits);
+                if (lane == 0) sm.tile_bits[j] = sbits;
+            }
         }
-        part = __reduce_add_sync(0xFFFFFFFFu, part);
-        if (lane == 0) sm.red[warp] = part;
-        // exact bit plan per tile from the tile histograms
-        __syncthreads();
-        for (uint32_t j = warp; j < md.ntiles; j += NW) {
-            const uint16_t* h = bp.tile_hist + (size_t)(md.tile_base + j) * GPZ_NSYM;
-            uint32_t sbits = 0;
-            for (int q = lane; q < GPZ_NSYM; q += 32) sbits += (uint32_t)h[q] * sm.blen[q];
-            sbits = __reduce_add_sync(0xFFFFFFFFu, sbits);
-            if (lane == 0) sm.tile_bits[j] = sbits;
-        }
-        __syncthreads();
+        __syncthreads();  // the CRC and the bit plan are both ready
         if (tid == 0) {
             uint32_t tot = sm.hbits;
             for (int w = 0; w < NW; w++) tot += sm.red[w];
