@@ -43,6 +43,9 @@ constexpr size_t kDefaultBatch = 32u << 20;
 constexpr size_t kDefaultPool = 40ull << 30;
 constexpr int kBuckets = 5;
 constexpr size_t kDescHeader = 64;  // batch dimensions at the start of a descriptor block
+// kernels of one batch without k_fetch / k_drain: segtab, lookup, walk exit,
+// chain, walk mark, huff, place, frame, emit
+constexpr uint64_t kStageKernels = 9;
 
 size_t round_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
@@ -479,7 +482,7 @@ int launch(gpz_ctx* c, Slot& sl, const BatchParams& bp, const LaunchShape& shape
         if (gpz_launch_batch(bp, shape, s, timing ? reinterpret_cast<void* const*>(sl.ev) : nullptr, drain,
                              fetch) != 0)
             return fail(c, GPZ_E_CUDA, "kernel launch", cudaGetLastError());
-        c->launches = 10 + (drain ? 1 : 0);
+        c->launches = kStageKernels + (drain ? 1 : 0) + (fetch ? 1 : 0);
         return GPZ_OK;
     }
     Slot::Graph& g = sl.graphs[sl.bucket];
@@ -503,7 +506,7 @@ int launch(gpz_ctx* c, Slot& sl, const BatchParams& bp, const LaunchShape& shape
         g.gen = sl.gen;
     }
     CU(c, cudaGraphLaunch(g.exec, s));
-    c->launches = 10 + (drain ? 1 : 0);
+    c->launches = kStageKernels + (drain ? 1 : 0) + (fetch ? 1 : 0);
     return GPZ_OK;
 }
 
@@ -732,13 +735,19 @@ int run_host_items(gpz_ctx* c, const gpz_desc* d, size_t count, gpz_out* outs, b
         }
     };
     size_t i = 0;
+    int pass = 0;
     while (i < count && fatal == GPZ_OK) {
         size_t j = i, bytes = 0;
         if (plain) {
             j = i + 1;
         } else {
-            while (j < count && (j == i || bytes + d[j].n <= c->batch_bytes)) bytes += d[j++].n;
+            // ramp up: the first passes are a quarter and a half of the pass
+            // size, so the device starts computing while later passes are
+            // still being staged and uploaded
+            const size_t cap = c->batch_bytes >> (pass < 2 ? 2 - pass : 0);
+            while (j < count && (j == i || bytes + d[j].n <= cap)) bytes += d[j++].n;
         }
+        pass++;
         const int k = plain ? 0 : c->next_slot;
         settle(k);
         if (fatal) break;

@@ -203,14 +203,23 @@ class Context:
                     "gpz_compress_chunk")
         return out[:n.value].tobytes()
 
-    def _batch(self, fn, items, level: int = 5):
-        """One output allocation for all items; results are zero-copy views."""
+    def batch_bound(self, items) -> int:
+        """Output bytes compress_batch needs for these items (sum of bounds)."""
+        return max(1, sum(self.bound(len(x)) for x in items))
+
+    def _batch(self, fn, items, level: int = 5, out=None):
+        """One output buffer for all items (`out`, a uint8 array of at least
+        batch_bound(items) bytes that the caller may reuse across calls, or a
+        fresh allocation); results are zero-copy views into it."""
         arrs = [_u8(x) for x in items]
         k = len(arrs)
         descs = (Desc * max(k, 1))()
         outs = (Out * max(k, 1))()
         bounds = [self.bound(a.size) for a in arrs]
-        out = np.empty(max(1, sum(bounds)), dtype=np.uint8)
+        if out is None:
+            out = np.empty(max(1, sum(bounds)), dtype=np.uint8)
+        elif out.dtype != np.uint8 or not out.flags.c_contiguous or out.size < sum(bounds):
+            raise ValueError("out must be a contiguous uint8 array of at least batch_bound(items) bytes")
         base = out.ctypes.data
         off = 0
         for i, a in enumerate(arrs):
@@ -228,11 +237,11 @@ class Context:
             off += bounds[i]
         return res
 
-    def compress_batch(self, items, level: int = 5):
-        return self._batch(self.L.gpz_compress_batch, items, level)
+    def compress_batch(self, items, level: int = 5, out=None):
+        return self._batch(self.L.gpz_compress_batch, items, level, out)
 
-    def compress_batch_plain(self, items, level: int = 5):
-        return self._batch(self.L.gpz_compress_batch_plain, items, level)
+    def compress_batch_plain(self, items, level: int = 5, out=None):
+        return self._batch(self.L.gpz_compress_batch_plain, items, level, out)
 
     def debug_chunk(self, data):
         """(pp, tokens, gzip bytes) of one chunk through the device path."""
