@@ -209,7 +209,6 @@ __device__ __forceinline__ uint32_t slot_of(uint32_t h) { return (h * 0x85EBCA6B
 template <int T>
 __global__ void __launch_bounds__(T, 2) k_segtab(BatchParams bp) {
     constexpr int PER = GPZ_SEG / T;
-    constexpr int SPT = kSlots / T;  // slots per thread in the compaction
     extern __shared__ __align__(16) uint8_t smem[];
     uint32_t* keyt = reinterpret_cast<uint32_t*>(smem);
     uint32_t* oldt = keyt + kSlots;
@@ -262,22 +261,45 @@ __global__ void __launch_bounds__(T, 2) k_segtab(BatchParams bp) {
             }
         }
         __syncthreads();
-        // dense ids of the occupied slots, in slot order
-        uint32_t occ = 0;
+        // dense ids of the occupied slots, in slot order: warp w owns slots
+        // [w * SW, (w + 1) * SW), read 32 at a time; ballots give each
+        // occupied slot its rank, a scan over the warps' counts the base
+        constexpr int NWARP = T / 32, SW = kSlots / NWARP, KW = SW / 32;
+        const int warp = tid >> 5;
+        const uint32_t lt = (1u << lane) - 1u;
+        uint32_t kv[KW];
+        uint32_t wcount = 0;
 #pragma unroll
-        for (int q = 0; q < SPT; q++) occ += keyt[tid * SPT + q] != kEmpty;
-        uint32_t nkeys;
-        uint32_t id = block_excl_scan<T>(occ, wsum, &nkeys);
+        for (int k = 0; k < KW; k++) {
+            kv[k] = keyt[warp * SW + k * 32 + lane];
+            wcount += __popc(__ballot_sync(0xFFFFFFFFu, kv[k] != kEmpty));
+        }
+        if (lane == 0) wsum[warp] = wcount;
+        __syncthreads();
+        uint32_t wbase = 0, nkeys = 0;
+        {
+            const uint32_t c = lane < NWARP ? wsum[lane] : 0u;
+            uint32_t x = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+                if (lane >= o) x += y;
+            }
+            wbase = __shfl_sync(0xFFFFFFFFu, x - c, warp);
+            nkeys = __shfl_sync(0xFFFFFFFFu, x, NWARP - 1);
+        }
         uint16_t* keys = bp.seg_keys + (size_t)t * GPZ_SEG;
         uint32_t* on = bp.seg_on + (size_t)t * GPZ_SEG;
 #pragma unroll
-        for (int q = 0; q < SPT; q++) {
-            const uint32_t sl = tid * SPT + q, kv = keyt[sl];
-            if (kv == kEmpty) continue;
-            keys[id] = (uint16_t)kv;
-            on[id] = newt[sl] | (oldt[sl] << 16);
-            oldt[sl] = id;  // slot -> id from here on
-            id++;
+        for (int k = 0; k < KW; k++) {
+            const uint32_t m = __ballot_sync(0xFFFFFFFFu, kv[k] != kEmpty);
+            if (kv[k] != kEmpty) {
+                const uint32_t sl = warp * SW + k * 32 + lane, id = wbase + __popc(m & lt);
+                keys[id] = (uint16_t)kv[k];
+                on[id] = newt[sl] | (oldt[sl] << 16);
+                oldt[sl] = id;  // slot -> id from here on
+            }
+            wbase += __popc(m);
         }
         __syncthreads();
         uint16_t* pos_id = bp.seg_posid + (size_t)t * GPZ_SEG;
