@@ -341,7 +341,7 @@ __global__ void __launch_bounds__(T, 1) k_lookup(BatchParams bp) {
     uint32_t* w32 = reinterpret_cast<uint32_t*>(win);
     uint32_t* cand = reinterpret_cast<uint32_t*>(smem + LookupSmem::kCand);
     uint32_t* owntab = reinterpret_cast<uint32_t*>(smem + LookupSmem::kOwnTab);
-    __shared__ uint32_t s_tile;
+    __shared__ uint32_t s_tile, s_nback_keys[8];
     const int tid = threadIdx.x;
 
     const uint32_t ntiles = bp.dims[0];
@@ -370,6 +370,8 @@ __global__ void __launch_bounds__(T, 1) k_lookup(BatchParams bp) {
             const uint32_t nvec = (wvalid + 15u) >> 4;
             for (uint32_t i = tid; i < nvec; i += T) dst[i] = __ldg(src + i);
             const uint32_t* go = bp.seg_on + (size_t)t * GPZ_SEG;
+            // key counts of the segments the join reads, all loaded at once
+            if (tid < nback) s_nback_keys[tid] = bp.seg_nkeys[t - 1u - tid];
             for (uint32_t i = tid; i < nown; i += T) cand[i] = go[i];
             for (uint32_t i = tid; i < nback * GPZ_SEG; i += T) cand[GPZ_SEG + i] = kEmpty;
             for (int i = tid; i < kSlots; i += T) owntab[i] = kEmpty;
@@ -399,7 +401,7 @@ __global__ void __launch_bounds__(T, 1) k_lookup(BatchParams bp) {
         // tile's table (each segment writes its own candidate row)
         for (uint32_t back = 1; back <= nback; back++) {
             const uint32_t ts = t - back;  // a member's tiles are consecutive
-            const uint32_t ns = min(bp.seg_nkeys[ts], GPZ_SEG);
+            const uint32_t ns = min(s_nback_keys[back - 1], GPZ_SEG);
             const uint16_t* gk = bp.seg_keys + (size_t)ts * GPZ_SEG;
             const uint32_t* go = bp.seg_on + (size_t)ts * GPZ_SEG;
             uint32_t* cb = cand + back * GPZ_SEG;
