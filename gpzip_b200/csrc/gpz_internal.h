@@ -26,6 +26,9 @@
 #define GPZ_ERRBIT_HUFF 4u      // code construction failed (never expected)
 #define GPZ_ERRBIT_DESC 8u      // a fetched descriptor block exceeded the arenas
 
+// BatchParams.flags
+#define GPZ_BATCH_FIXED 1u      // every member as one fixed-Huffman block (RFC 1951 BTYPE 01)
+
 struct MemberDesc {
     uint64_t in_off;     // first input byte of the member in the batch input (16-byte aligned)
     uint32_t len;        // member length in bytes
@@ -76,6 +79,7 @@ struct BatchParams {
     uint32_t nmembers;        // host-side copies, used only to size exact grids
     uint32_t ntiles;
     uint64_t out_base;        // byte offset added to every member's gz_off
+    uint32_t flags;           // GPZ_BATCH_* below
 };
 
 enum {

@@ -1446,8 +1446,15 @@ __global__ void __launch_bounds__(kHuffThreads) k_huff(BatchParams bp) {
             if (tid == 0) sm.ok = 1;
             hsync();
 
-            // litlen and distance code lengths, 15-bit limit
-            block_code_lengths<G>(sm, tid, hsync);
+            // litlen and distance code lengths, 15-bit limit (skipped when
+            // the batch asks for fixed blocks)
+            const bool force_fixed = (bp.flags & GPZ_BATCH_FIXED) != 0u;
+            if (force_fixed) {
+                for (int q = tid; q < GPZ_NSYM; q += G) sm.lens[q] = 0;
+                if (tid == 0) sm.ok = 0;
+            } else {
+                block_code_lengths<G>(sm, tid, hsync);
+            }
             hsync();
 
             // fix-ups (deflate.rs:854-867)
@@ -1489,8 +1496,36 @@ __global__ void __launch_bounds__(kHuffThreads) k_huff(BatchParams bp) {
                 warp_canonical(sm.meta_lens, 19, sm.meta_codes);
             }
             hsync();
-            // header bits (deflate.rs:911-932), LSB first
-            if (warp == 0) warp_header(sm, lane);
+            // header bits (deflate.rs:911-932), LSB first; or, where a code
+            // could not be built (encode_block_fast, deflate.rs:752-761) or
+            // fixed blocks were asked for, the fixed block's codes and its
+            // 3-bit header (write_fixed_block_fast, deflate.rs:763-828)
+            if (sm.ok) {
+                if (warp == 0) warp_header(sm, lane);
+            } else {
+                for (int q = tid; q < GPZ_NSYM; q += G) {
+                    uint32_t code, bits;
+                    if (q >= GPZ_NLIT) {
+                        code = (uint32_t)(q - GPZ_NLIT);
+                        bits = 5;
+                    } else if (q <= 143) {
+                        code = 0x30u + q;
+                        bits = 8;
+                    } else if (q <= 255) {
+                        code = 0x190u + (q - 144);
+                        bits = 9;
+                    } else if (q <= 279) {
+                        code = (uint32_t)(q - 256);
+                        bits = 7;
+                    } else {
+                        code = 0xC0u + (q - 280);
+                        bits = 8;
+                    }
+                    sm.codes[q] = rev_code(code, bits) | (bits << 16);
+                }
+                for (int w = tid; w < GPZ_HDR_WORDS; w += G) sm.hdr[w] = w == 0 ? 3u : 0u;  // BFINAL 1, BTYPE 01
+                if (tid == 0) sm.hbits = 3;
+            }
             hsync();
 
             // bits per symbol occurrence (code + extra); total member bits
@@ -1526,7 +1561,6 @@ __global__ void __launch_bounds__(kHuffThreads) k_huff(BatchParams bp) {
                 off += sm.tile_bits[j];
             }
             if (off + (sm.codes[256] >> 16) != tot) atomicOr(bp.err, GPZ_ERRBIT_BITS);
-            if (!sm.ok) atomicOr(bp.err, GPZ_ERRBIT_HUFF);
             MemberOut mo;
             mo.gz_off = 0;
             mo.deflate_bytes = (tot + 7u) >> 3;

@@ -398,7 +398,7 @@ int reserve_limits(gpz_ctx* c, Slot& sl, size_t max_bytes, size_t max_items) {
     return ensure_host(c, sl, sl.h_out, sl.h_out_cap, out_bytes + 64, true);
 }
 
-BatchParams params_of(Slot& sl, const uint8_t* d_in, uint8_t* d_out) {
+BatchParams params_of(const gpz_ctx* c, Slot& sl, const uint8_t* d_in, uint8_t* d_out) {
     BatchParams bp{};
     bp.in = d_in;
     bp.dims = static_cast<const uint32_t*>(sl.d_dims.p);
@@ -424,6 +424,7 @@ BatchParams params_of(Slot& sl, const uint8_t* d_in, uint8_t* d_out) {
     bp.nmembers = (uint32_t)sl.members.size();
     bp.ntiles = (uint32_t)sl.tiles.size();
     bp.out_base = 0;
+    bp.flags = (c->flags & GPZ_FLAG_FIXED_BLOCKS) ? GPZ_BATCH_FIXED : 0u;
     return bp;
 }
 
@@ -618,7 +619,7 @@ int submit_slot(gpz_ctx* c, Slot& sl, const gpz_desc* d, size_t count, const Lau
         if ((rc = upload_desc(c, sl, s))) return rc;
     }
     CU(c, cudaEventRecord(sl.tv[1], s));
-    BatchParams bp = params_of(sl, static_cast<const uint8_t*>(sl.d_in.p), static_cast<uint8_t*>(sl.d_out.p));
+    BatchParams bp = params_of(c, sl, static_cast<const uint8_t*>(sl.d_in.p), static_cast<uint8_t*>(sl.d_out.p));
     DrainTarget dt{mapped_dev(sl.h_out), mapped_dev(sl.h_mout), mapped_dev(sl.h_err), c->sms * 4};
     if (!dt.h_out || !dt.h_mout || !dt.h_err) return fail(c, GPZ_E_CUDA, "mapped host memory");
     sl.bucket = bucket_of(sl.tiles.size());
@@ -1360,7 +1361,7 @@ int gpz_compress_device(gpz_ctx* c, const void* d_in, const uint64_t* in_off, co
     if ((rc = reserve(c, sl, in_end, false, false, 0))) return rc;
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : sl.stream;
     if ((rc = upload_desc(c, sl, s))) return rc;
-    BatchParams bp = params_of(sl, static_cast<const uint8_t*>(d_in), static_cast<uint8_t*>(d_out));
+    BatchParams bp = params_of(c, sl, static_cast<const uint8_t*>(d_in), static_cast<uint8_t*>(d_out));
     sl.bucket = bucket_of(sl.tiles.size());
     const bool timing = (c->flags & GPZ_FLAG_STAGE_TIMING) != 0;
     if ((rc = launch(c, sl, bp, shape_for(c, sl.bucket), false, nullptr, timing, s))) return rc;

@@ -22,6 +22,7 @@ GPZ_FLAG_NO_GRAPHS = 1
 GPZ_FLAG_NO_AUTOTUNE = 2
 GPZ_FLAG_STAGE_TIMING = 4
 GPZ_FLAG_SM_PARTITION = 8
+GPZ_FLAG_FIXED_BLOCKS = 16
 # gpz_stage_times order (GPZ_STAGES values): the kernels each stage covers
 STAGE_NAMES = ["k_segtab", "k_lookup", "k_walk", "k_huff", "k_emit"]
 

@@ -65,6 +65,8 @@ typedef struct gpz_config {
 #define GPZ_FLAG_NO_AUTOTUNE 2  /* keep the default launch shapes */
 #define GPZ_FLAG_STAGE_TIMING 4 /* record CUDA events around each stage (gpz_stage_times) */
 #define GPZ_FLAG_SM_PARTITION 8 /* serving: run the small- and large-request lanes on separate SM partitions */
+#define GPZ_FLAG_FIXED_BLOCKS 16 /* every member as one fixed-Huffman block (RFC 1951 BTYPE 01), the block
+                                  encode_block_fast falls back to (deflate.rs:752-799) */
 
 typedef struct gpz_desc {
     const uint8_t* in;   /* one chunk or file */

@@ -548,6 +548,16 @@ static int write_dynamic_block(const uint32_t* tokens, size_t count, bitw* w) {
 }
 
 /* deflate.rs:752-761 */
+/* write_fixed_block_fast alone (deflate.rs:763-799): the block the
+ * reference falls back to, for tests of the fixed-block path. */
+size_t gpzo_encode_block_fixed(const uint32_t* tokens, size_t count, uint8_t* out, size_t cap) {
+    bitw w = {out, 0, cap, 0, 0, 0};
+    write_fixed_block(tokens, count, &w);
+    bw_finish(&w);
+    if (w.overflow) return 0;
+    return w.len;
+}
+
 size_t gpzo_encode_block_fast(const uint32_t* tokens, size_t count, uint8_t* out, size_t cap) {
     bitw w = {out, 0, cap, 0, 0, 0};
     if (!write_dynamic_block(tokens, count, &w)) {

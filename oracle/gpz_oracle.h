@@ -48,6 +48,7 @@ void gpzo_canonical_codes(const uint8_t* lens, int nsym, uint32_t* codes);
 /* deflate.rs:752-761 (encode_block_fast).  Returns the byte count written to
  * out, or 0 if cap is too small. */
 size_t gpzo_encode_block_fast(const uint32_t* tokens, size_t count, uint8_t* out, size_t cap);
+size_t gpzo_encode_block_fixed(const uint32_t* tokens, size_t count, uint8_t* out, size_t cap);
 
 /* CRC-32 (IEEE 802.3, reflected, init/xorout 0xFFFFFFFF) as crc32fast 1.5.0
  * computes it at deflate.rs:974. */

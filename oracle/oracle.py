@@ -15,6 +15,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libgpz_oracle.so")
 MEMBER_BYTES = 128 * 1024
+# the 10-byte member header of deflate.rs:962-980 (GPZIP_HEADER, parallel_decompress.rs:29)
+GZIP_HEADER = bytes([0x1F, 0x8B, 0x08, 0x00, 0x00, 0x00, 0x00, 0x00, 0x00, 0xFF])
 
 _lib = None
 
@@ -42,6 +44,8 @@ def lib() -> ctypes.CDLL:
         L.gpzo_build_code_lengths.restype = ctypes.c_int
         L.gpzo_encode_block_fast.argtypes = [u8p, ctypes.c_size_t, u8p, ctypes.c_size_t]
         L.gpzo_encode_block_fast.restype = ctypes.c_size_t
+        L.gpzo_encode_block_fixed.argtypes = [u8p, ctypes.c_size_t, u8p, ctypes.c_size_t]
+        L.gpzo_encode_block_fixed.restype = ctypes.c_size_t
         L.gpzo_crc32.argtypes = [u8p, ctypes.c_size_t]
         L.gpzo_crc32.restype = ctypes.c_uint32
         L.gpzo_gzip_member.argtypes = [u8p, ctypes.c_uint32, u8p, ctypes.c_size_t]
@@ -115,6 +119,33 @@ def encode_block_fast(toks: np.ndarray) -> bytes:
     if k == 0:
         raise RuntimeError("oracle encode overflow")
     return out[:k].tobytes()
+
+
+def encode_block_fixed(toks: np.ndarray) -> bytes:
+    """write_fixed_block_fast alone (deflate.rs:763-799)."""
+    t = np.ascontiguousarray(toks, dtype=np.uint32)
+    cap = 64 + 4 * t.size + 64
+    out = np.zeros(cap, dtype=np.uint8)
+    k = lib().gpzo_encode_block_fixed(_ptr(t), t.size, _ptr(out), cap)
+    if k == 0:
+        raise RuntimeError("oracle encode overflow")
+    return out[:k].tobytes()
+
+
+def gzip_member_fixed(data) -> bytes:
+    """A gzip member whose DEFLATE block is the fixed-Huffman one
+    (deflate.rs:962-980 around write_fixed_block_fast)."""
+    import struct
+    a = _u8(data)
+    body = encode_block_fixed(tokens(a)) if a.size else encode_block_fixed(np.zeros(0, np.uint32))
+    return GZIP_HEADER + body + struct.pack("<II", crc32(a), a.size & 0xFFFFFFFF)
+
+
+def gzip_chunk_fixed(data, member_bytes: int = MEMBER_BYTES) -> bytes:
+    a = _u8(data)
+    if a.size <= member_bytes:
+        return gzip_member_fixed(a)
+    return b"".join(gzip_member_fixed(a[o:o + member_bytes]) for o in range(0, a.size, member_bytes))
 
 
 def crc32(data) -> int:

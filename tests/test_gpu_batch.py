@@ -138,3 +138,18 @@ def test_serving_pending_space_and_admission():
         assert e.value.status == native.GPZ_E_BUSY
         st = c.serve_stats()
         assert st["rejected"] == 1
+
+
+def test_fixed_block_mode():
+    # GPZ_FLAG_FIXED_BLOCKS: every member is the fixed-Huffman block the
+    # reference falls back to (deflate.rs:752-799), byte for byte
+    import gzip
+    items = [W.text(300_000, seed=81).tobytes(), W.binary(131_072, seed=82).tobytes(), b"", b"q",
+             W.logs(70_001, seed=83).tobytes()]
+    with native.Context(flags=native.GPZ_FLAG_FIXED_BLOCKS) as c:
+        for it in items:
+            got = c.compress_chunk(it)
+            assert got == O.gzip_chunk_fixed(it, 131072)
+            assert gzip.decompress(got) == it
+        for it, g in zip(items, c.compress_batch(items)):
+            assert g == O.gzip_chunk_fixed(it, 131072)

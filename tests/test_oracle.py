@@ -186,3 +186,16 @@ def test_cpu_baseline_gzip_chunks():
     data = (b"abc def ghi " * 300000) + rng.integers(0, 256, size=5000, dtype=np.uint8).tobytes()
     gz = O.cpu_gzip_chunks(data, 2 << 20, 5, threads=4)
     assert inflate_all(gz) == data
+
+
+def test_fixed_block_matches_python_restatement():
+    # write_fixed_block_fast (deflate.rs:763-799): the C oracle's fixed block
+    # equals the pure-Python restatement's and inflates back
+    import gzip
+    from gpzip_b200 import workloads as W
+    for i, kind in enumerate(("text", "logs", "binary")):
+        data = W.GENERATORS[kind](12_000, seed=70 + i).tobytes()
+        toks = O.tokens(data)
+        assert O.encode_block_fixed(toks) == P._encode_fixed([int(t) for t in toks])
+        assert gzip.decompress(O.gzip_chunk_fixed(data)) == data
+    assert gzip.decompress(O.gzip_chunk_fixed(b"")) == b""
