@@ -39,7 +39,7 @@ namespace {
 
 constexpr size_t kDefaultMember = 131072;
 constexpr size_t kMaxMember = 2u << 20;
-constexpr size_t kDefaultBatch = 32u << 20;
+constexpr size_t kDefaultBatch = 64u << 20;
 constexpr size_t kDefaultPool = 40ull << 30;
 constexpr int kBuckets = 5;
 constexpr size_t kDescHeader = 64;  // batch dimensions at the start of a descriptor block

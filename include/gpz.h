@@ -55,7 +55,7 @@ typedef struct gpz_config {
     size_t member_bytes;   /* input bytes per gzip member: 131072 (default, the reference's
                               sub-chunk) up to 2097152 (whole-chunk mode); multiple of 4096 */
     size_t pool_bytes;     /* device pool cap in bytes (0: 40 GiB) */
-    size_t batch_bytes;    /* input bytes per device pass (0: 32 MiB); larger calls are split into
+    size_t batch_bytes;    /* input bytes per device pass (0: 64 MiB); larger calls are split into
                               passes that overlap upload, compute and download */
     int streams;           /* reserved (0) */
     int flags;             /* GPZ_FLAG_* */
