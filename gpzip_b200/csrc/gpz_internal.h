@@ -89,6 +89,8 @@ enum {
     GPZ_CNT_HUFF = 3,
     GPZ_CNT_EMIT = 4,
     GPZ_CNT_SEGSORT = 5,
+    GPZ_CNT_EXIT_DONE = 6,  // CTAs of k_walk_exit that finished (the last one chains)
+    GPZ_CNT_HUFF_DONE = 7,  // CTAs of k_huff that finished (the last one places)
     GPZ_NCOUNTERS = 8
 };
 

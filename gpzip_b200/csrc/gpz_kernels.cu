@@ -13,13 +13,12 @@
 //                one packed token per position (pp).
 //   k_walk_exit  per tile: exit offset for each of the 258 entry offsets of
 //                the lazy walk (lz77.rs:260-284), by pointer jumping.
-//   k_chain      per member: the entry offset of every tile.
+//                (its last CTA: the entry offset of every tile, by member)
 //   k_walk_mark  per tile: walked tokens in order and the tile's symbol
 //                histogram.
 //   k_huff       per member: CRC-32, length-limited codes (huffman.rs:26-152),
 //                dynamic block header (deflate.rs:830-932), exact bit plan
-//                per tile.
-//   k_place      one CTA: byte offset of every gzip member (scan).
+//                per tile (its last CTA: every member's output offset).
 //   k_frame      per member: gzip header words, shared boundary words, EOB.
 //   k_emit       per tile: per-token codes and bit packing
 //                (deflate.rs:934-958) into the batch's gzip stream.
@@ -473,8 +472,9 @@ __global__ void __launch_bounds__(T, 1) k_lookup(BatchParams bp) {
 // The lazy walk of lz77.rs:260-284 visits p, next(p), next(next(p)), ...
 // where next(p) depends only on pp[p] and pp[p+1].  Each 4 KiB tile is walked
 // on its own: k_walk_exit computes, for every position a walk can enter the
-// tile at (its first 258), where it leaves; k_chain strings the tiles of a
-// member together (entry of tile b+1 = exit of tile b at its entry);
+// tile at (its first 258), where it leaves, and its last CTA strings the
+// tiles of a member together (entry of tile b+1 = exit of tile b at its
+// entry);
 // k_walk_mark walks from the known entry and emits the visited tokens in
 // order with the tile's symbol histogram.  Two forms with identical output:
 //   warp  one warp per tile, 32 positions at a time, links inside a window
@@ -485,6 +485,14 @@ __global__ void __launch_bounds__(T, 1) k_lookup(BatchParams bp) {
 //         small batches, where a tile's latency is the batch's.
 
 constexpr uint32_t kFull = 0xFFFFFFFFu;
+
+// Defined below: the per-member tile chaining run by the last CTA of
+// k_walk_exit, the member placement run by the last CTA of k_huff, and the
+// last-CTA test itself.
+__device__ void chain_members(const BatchParams& bp);
+template <int T>
+__device__ void place_members(const BatchParams& bp, unsigned long long* wsum, unsigned long long& carry);
+__device__ bool last_cta_done(uint32_t* counter);
 
 // next(p) (lz77.rs:266-282): a literal advances by one; a match advances by
 // its length unless pp[p+1] is a longer match (lazy demotion to a literal).
@@ -553,6 +561,8 @@ __global__ void __launch_bounds__(T) k_walk_exit_warp(BatchParams bp) {
         for (int e = lane; e < GPZ_EXITS; e += 32) bp.tile_exit[(size_t)t * GPZ_EXITS + e] = ex[e];
         __syncwarp();
     }
+    // the last CTA strings every member's tiles together
+    if (last_cta_done(&bp.counters[GPZ_CNT_EXIT_DONE])) chain_members(bp);
 }
 
 // ---- block form: one CTA per tile
@@ -620,18 +630,21 @@ __global__ void __launch_bounds__(T) k_walk_exit_blk(BatchParams bp) {
         for (int e = tid; e < GPZ_EXITS; e += T)
             bp.tile_exit[(size_t)t * GPZ_EXITS + e] = (uint16_t)(w.J[cur][e] - cnt);
     }
+    // the last CTA strings every member's tiles together
+    if (last_cta_done(&bp.counters[GPZ_CNT_EXIT_DONE])) chain_members(bp);
 }
 
-// Entry offset of every tile: one thread per member follows the exit tables.
-__global__ void k_chain(BatchParams bp) {
+// Entry offset of every tile: one thread per member follows the exit tables
+// (written by other CTAs: read past L1).  Run by the last CTA of k_walk_exit.
+__device__ void chain_members(const BatchParams& bp) {
     const uint32_t nmembers = bp.dims[1];
-    for (uint32_t m = blockIdx.x * blockDim.x + threadIdx.x; m < nmembers; m += gridDim.x * blockDim.x) {
+    for (uint32_t m = threadIdx.x; m < nmembers; m += blockDim.x) {
         const MemberDesc md = bp.members[m];
         uint32_t e = 0;
         for (uint32_t b = 0; b < md.ntiles; b++) {
             const uint32_t t = md.tile_base + b;
             bp.tile_entry[t] = e;
-            if (b + 1u < md.ntiles) e = bp.tile_exit[(size_t)t * GPZ_EXITS + min(e, (uint32_t)GPZ_EXITS - 1u)];
+            if (b + 1u < md.ntiles) e = __ldcg(&bp.tile_exit[(size_t)t * GPZ_EXITS + min(e, (uint32_t)GPZ_EXITS - 1u)]);
         }
     }
 }
@@ -1348,6 +1361,7 @@ __device__ void block_code_lengths(Smem& sm, int tid, Sync sync) {
 // DEFLATE size and its CRC-32.  Members are independent: no waiting.
 __global__ void __launch_bounds__(kHuffThreads) k_huff(BatchParams bp) {
     __shared__ HuffSmem sm;
+    __shared__ unsigned long long s_wsum[32], s_carry;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     // threads [0, 256): code construction, header and bit plan (named
     // barrier 1); threads [256, 512): the member's CRC-32 (named barrier 2).
@@ -1574,24 +1588,26 @@ __global__ void __launch_bounds__(kHuffThreads) k_huff(BatchParams bp) {
         for (int q = tid; q < GPZ_NSYM; q += kHuffThreads) bp.member_codes[(size_t)m * GPZ_NSYM + q] = sm.codes[q];
         for (int q = tid; q < GPZ_HDR_WORDS; q += kHuffThreads) bp.member_hdr[(size_t)m * GPZ_HDR_WORDS + q] = sm.hdr[q];
     }
+    // the last CTA places every member in the batch output (a scan of sizes)
+    if (last_cta_done(&bp.counters[GPZ_CNT_HUFF_DONE])) place_members<kHuffThreads>(bp, s_wsum, s_carry);
 }
 
-// ================================================================= k_place
+// ========================================================== member placement
 
 // Byte offset of every gzip member in the batch output: exclusive scan of
 // (18 + DEFLATE bytes) in member order, one CTA.
-constexpr int kPlaceThreads = 1024;
 
-__global__ void __launch_bounds__(kPlaceThreads) k_place(BatchParams bp) {
-    __shared__ unsigned long long wsum[32];
-    __shared__ unsigned long long carry;
+template <int T>
+__device__ void place_members(const BatchParams& bp, unsigned long long* wsum, unsigned long long& carry) {
+    constexpr int NW = T / 32;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t nmembers = bp.dims[1];
     if (tid == 0) carry = bp.out_base;
     __syncthreads();
-    for (uint32_t base = 0; base < nmembers; base += kPlaceThreads) {
+    for (uint32_t base = 0; base < nmembers; base += T) {
         const uint32_t m = base + tid;
-        const unsigned long long v = m < nmembers ? 18ull + bp.member_out[m].deflate_bytes : 0ull;
+        // written by other CTAs of the producing kernel: read past L1
+        const unsigned long long v = m < nmembers ? 18ull + __ldcg(&bp.member_out[m].deflate_bytes) : 0ull;
         unsigned long long x = v;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -1601,21 +1617,33 @@ __global__ void __launch_bounds__(kPlaceThreads) k_place(BatchParams bp) {
         if (lane == 31) wsum[warp] = x;
         __syncthreads();
         if (warp == 0) {
-            unsigned long long s = wsum[lane];
+            unsigned long long s = lane < NW ? wsum[lane] : 0ull;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
                 const unsigned long long y = __shfl_up_sync(0xFFFFFFFFu, s, o);
                 if (lane >= o) s += y;
             }
-            wsum[lane] = s;
+            if (lane < NW) wsum[lane] = s;
         }
         __syncthreads();
         const unsigned long long excl = carry + (warp ? wsum[warp - 1] : 0ull) + x - v;
         if (m < nmembers) bp.member_out[m].gz_off = excl;
         __syncthreads();
-        if (tid == 0) carry += wsum[31];
+        if (tid == 0) carry += wsum[NW - 1];
         __syncthreads();
     }
+}
+
+// True in the last CTA of the grid to get here: every CTA's global writes
+// are fenced before it counts itself, so the last one sees them all.
+__device__ bool last_cta_done(uint32_t* counter) {
+    __shared__ bool s_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = atomicAdd(counter, 1u) == gridDim.x - 1u;
+    __syncthreads();
+    if (s_last) __threadfence();
+    return s_last;
 }
 
 // ================================================================= k_frame
@@ -1908,28 +1936,23 @@ int gpz_launch_batch(const BatchParams& bp, const LaunchShape& ls, void* stream,
     // walk form: 1024 selects the block form (512 threads per tile CTA);
     // 256 / 512 the warp form with that many threads per CTA
     const int gw = grid_of(ls.walk_grid, bp.ntiles);
-    const int gc = ls.huff_grid > 0 ? ls.huff_grid : (nm + 127) / 128;
     switch (ls.walk_threads) {
         case 1024:
             k_walk_exit_blk<512><<<gw, 512, 0, s>>>(bp);
-            k_chain<<<gc, 128, 0, s>>>(bp);
             k_walk_mark_blk<512><<<gw, 512, 0, s>>>(bp);
             break;
         case 256:
             k_walk_exit_warp<256><<<gw, 256, 0, s>>>(bp);
-            k_chain<<<gc, 128, 0, s>>>(bp);
             k_walk_mark_warp<256><<<gw, 256, 0, s>>>(bp);
             break;
         default:
             k_walk_exit_warp<512><<<gw, 512, 0, s>>>(bp);
-            k_chain<<<gc, 128, 0, s>>>(bp);
             k_walk_mark_warp<512><<<gw, 512, 0, s>>>(bp);
             break;
     }
     mark(3);
     const int gh = grid_of(ls.huff_grid, bp.nmembers);
     k_huff<<<gh, kHuffThreads, 0, s>>>(bp);
-    k_place<<<1, kPlaceThreads, 0, s>>>(bp);
     k_frame<<<gh, kFrameThreads, 0, s>>>(bp);
     mark(4);
     const int ge = grid_of(ls.emit_grid, bp.ntiles);

@@ -43,9 +43,9 @@ constexpr size_t kDefaultBatch = 64u << 20;
 constexpr size_t kDefaultPool = 40ull << 30;
 constexpr int kBuckets = 5;
 constexpr size_t kDescHeader = 64;  // batch dimensions at the start of a descriptor block
-// kernels of one batch without k_fetch / k_drain: segtab, lookup, walk exit,
-// chain, walk mark, huff, place, frame, emit
-constexpr uint64_t kStageKernels = 9;
+// kernels of one batch without k_fetch / k_drain: segtab, lookup, walk exit
+// (+ chaining), walk mark, huff (+ placement), frame, emit
+constexpr uint64_t kStageKernels = 7;
 
 size_t round_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
