@@ -4,6 +4,7 @@ answer without touching a device (no compute calls here)."""
 import ctypes
 import os
 import re
+import shutil
 import subprocess
 
 import pytest
@@ -107,3 +108,31 @@ def test_create_fails_loudly_without_a_gpu(lib):
     assert not h.value
     with pytest.raises(native.GpzError):
         native.Context()
+
+
+def test_c_program_compiles_against_the_header(tmp_path):
+    # a plain C caller builds against include/gpz.h and links libgpz.so
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if not cc:
+        pytest.skip("no C compiler")
+    exe = tmp_path / "abi_roundtrip"
+    r = subprocess.run([cc, "-O1", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+                        os.path.join(ROOT, "tests", "c", "abi_roundtrip.c"), "-o", str(exe),
+                        "-L", os.path.dirname(native.LIB_PATH), "-lgpz", "-lz",
+                        "-Wl,-rpath," + os.path.dirname(native.LIB_PATH)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+
+
+@pytest.mark.gpu
+def test_c_program_round_trip(tmp_path):
+    # the same program run on the GPU: chunk and batch calls inflate back
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if not cc:
+        pytest.skip("no C compiler")
+    build.build()
+    exe = tmp_path / "abi_roundtrip"
+    subprocess.run([cc, "-O1", "-I", os.path.join(ROOT, "include"), os.path.join(ROOT, "tests", "c", "abi_roundtrip.c"),
+                    "-o", str(exe), "-L", os.path.dirname(native.LIB_PATH), "-lgpz", "-lz",
+                    "-Wl,-rpath," + os.path.dirname(native.LIB_PATH)], check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout + r.stderr

@@ -4,7 +4,6 @@ oracle; the 64 MiB logs tar and the 272 MiB mixed binary stream through
 size-independent properties (every member inflates back to its chunk, the
 streams are exactly the concatenation of valid gzip members, sampled chunks
 equal the oracle's)."""
-import gzip
 import zlib
 
 import numpy as np
@@ -25,9 +24,10 @@ def chunks_of(data):
 def members(stream: bytes):
     """Splits a concatenation of gzip members; every member must be valid."""
     out, pos = [], 0
+    view = memoryview(stream)
     while pos < len(stream):
         d = zlib.decompressobj(31)
-        body = d.decompress(stream[pos:])
+        body = d.decompress(view[pos:])
         assert d.eof, "truncated member"
         used = len(stream) - pos - len(d.unused_data)
         out.append(body)
@@ -56,4 +56,3 @@ def test_full_config_properties(ctx, name):
         assert b"".join(ms) == it.tobytes()
         if k in sample:
             assert g == O.gzip_chunk(it.tobytes(), 131072, threads=8)
-    assert gzip.decompress(b"".join(bytes(g) for g in got)) == data.tobytes()
