@@ -37,6 +37,26 @@ def test_batch_plain_oracle_uneven(ctx):
         assert g == O.gzip_chunk(it, 131072, threads=8)
 
 
+def test_page_locked_inputs_upload_directly(ctx):
+    # inputs in page-locked memory skip the staging copy; the bytes are the
+    # same as from pageable inputs, including ragged and empty items and
+    # items that start at odd offsets inside the pinned buffer
+    import torch
+    items = uneven_items(count=12, seed=8)
+    total = sum(len(x) for x in items) + 3 * len(items)
+    pinned = torch.empty(total, dtype=torch.uint8, pin_memory=True).numpy()
+    views, off = [], 1
+    for it in items:
+        pinned[off:off + len(it)] = np.frombuffer(it, dtype=np.uint8) if it else []
+        views.append(pinned[off:off + len(it)])
+        off += len(it) + 3
+    got = ctx.compress_batch(views)
+    want = ctx.compress_batch(items)
+    assert got == want
+    for it, g in zip(items, got):
+        assert g == O.gzip_chunk(it, 131072, threads=8)
+
+
 def test_graph_reuse_across_batch_sizes(ctx):
     # same size bucket, different member/tile counts: the captured graph reads
     # the batch dimensions from device memory
