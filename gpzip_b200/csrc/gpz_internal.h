@@ -137,6 +137,8 @@ struct FetchSource {
 // fetch: NULL, or the mapped sources k_fetch copies in before the first stage.
 int gpz_launch_batch(const BatchParams& bp, const LaunchShape& ls, void* stream, void* const* events,
                      const DrainTarget* drain, const FetchSource* fetch = nullptr);
+// k_drain alone, for a batch whose stage kernels ran on another stream.
+int gpz_launch_drain(const BatchParams& bp, const DrainTarget& drain, void* stream);
 // Persistent grid sizes (SMs x resident CTAs) for the shape's thread counts.
 int gpz_occupancy(LaunchShape* persistent);
 int gpz_kernel_smem_setup();

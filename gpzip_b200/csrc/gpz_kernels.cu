@@ -1965,6 +1965,11 @@ int gpz_launch_batch(const BatchParams& bp, const LaunchShape& ls, void* stream,
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
+int gpz_launch_drain(const BatchParams& bp, const DrainTarget& drain, void* stream) {
+    k_drain<<<drain.grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(bp, drain.h_out, drain.h_mout, drain.h_err);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
 int gpz_occupancy(LaunchShape* persistent) {
     int dev = 0, sms = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)

@@ -701,6 +701,9 @@ int submit_slot(gpz_ctx* c, Slot& sl, const gpz_desc* d, size_t count, const Lau
         if ((rc = upload_desc(c, sl, s))) return rc;
     }
     CU(c, cudaEventRecord(sl.tv[1], s));
+    // with a separate kernel stream, the drain runs on the slot's stream:
+    // the next pass's kernels need not wait for it
+    const bool split_drain = ks && ks != s && !pol.fetch;
     if (ks && ks != s) {
         CU(c, cudaStreamWaitEvent(ks, sl.tv[1], 0));
         c->last_upload = sl.tv[1];
@@ -714,7 +717,7 @@ int submit_slot(gpz_ctx* c, Slot& sl, const gpz_desc* d, size_t count, const Lau
     if (pol.exact) {
         // one launch per kernel, grids sized to this batch, no graph
         const LaunchShape exact{1024, 0, 1024, 0, 512, 0, 0, 0};
-        rc = launch(c, sl, bp, exact, false, &dt, timing, s);
+        rc = launch(c, sl, bp, exact, false, split_drain ? nullptr : &dt, timing, s);
     } else {
         bool tuned;
         {
@@ -731,11 +734,18 @@ int submit_slot(gpz_ctx* c, Slot& sl, const gpz_desc* d, size_t count, const Lau
                            &shape.huff_grid})
                 *g = std::max(1, *g * pol.grid_pct / 100);
         }
-        rc = launch(c, sl, bp, shape, graphs, &dt, timing, s, pol.fetch ? &fs : nullptr);
+        rc = launch(c, sl, bp, shape, graphs, split_drain ? nullptr : &dt, timing, s, pol.fetch ? &fs : nullptr);
     }
     if (rc) return rc;
     CU(c, cudaEventRecord(sl.tv[2], s));
-    CU(c, cudaEventRecord(sl.done, s));
+    if (split_drain) {
+        CU(c, cudaStreamWaitEvent(sl.stream, sl.tv[2], 0));
+        if (gpz_launch_drain(bp, dt, sl.stream) != 0) return fail(c, GPZ_E_CUDA, "drain launch", cudaGetLastError());
+        c->launches++;
+        CU(c, cudaEventRecord(sl.done, sl.stream));
+    } else {
+        CU(c, cudaEventRecord(sl.done, s));
+    }
     sl.busy = true;
     add_time(c, 2, now_ms() - t0);
     {
@@ -1368,8 +1378,12 @@ int gpz_create(const gpz_config* cfg, gpz_ctx** out) {
     }
     cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, c->device);
     default_shapes(c);
+    // slot streams carry the uploads and the drains: the highest priority,
+    // so a drain's CTAs are placed ahead of the next pass's waiting CTAs
+    int least = 0, greatest = 0;
+    cudaDeviceGetStreamPriorityRange(&least, &greatest);
     for (auto& s : c->slots)
-        if (init_slot(c, s) != GPZ_OK) {
+        if (init_slot(c, s, greatest) != GPZ_OK) {
             gpz_destroy(c);
             return GPZ_E_CUDA;
         }
