@@ -320,6 +320,48 @@ struct LookupSmem {
     static constexpr size_t kBytes = kOwnTab + kSlots * 4;
 };
 
+// The join's loads for one back segment (tile ts, ns distinct keys): this
+// thread's keys j = tid + u * T, u < GPZ_SEG / T, each guarded by j < ns <=
+// 4096, inside segment ts's arrays.  Absent keys read as kEmpty.
+template <int T>
+__device__ __forceinline__ void join_load(const BatchParams& bp, uint32_t ts, uint32_t ns,
+                                          uint32_t (&hk)[GPZ_SEG / T], uint32_t (&ov)[GPZ_SEG / T]) {
+    const uint16_t* gk = bp.seg_keys + (size_t)ts * GPZ_SEG;
+    const uint32_t* go = bp.seg_on + (size_t)ts * GPZ_SEG;
+#pragma unroll
+    for (int u = 0; u < (int)(GPZ_SEG / T); u++) {
+        const uint32_t j = threadIdx.x + (uint32_t)u * T;
+        hk[u] = kEmpty;
+        ov[u] = 0u;
+        if (j < ns) {
+            hk[u] = gk[j];
+            ov[u] = go[j];
+        }
+    }
+}
+
+// Probes the loaded keys into the tile's table; a key found there writes
+// its segment's newest | oldest into the key's candidate row.
+template <int T>
+__device__ __forceinline__ void join_probe(const uint32_t* owntab, uint32_t* cb, const uint32_t (&hk)[GPZ_SEG / T],
+                                           const uint32_t (&ov)[GPZ_SEG / T]) {
+#pragma unroll
+    for (int u = 0; u < (int)(GPZ_SEG / T); u++) {
+        const uint32_t h = hk[u];
+        if (h == kEmpty) continue;
+        uint32_t sl = slot_of(h);
+        for (int probe = 0; probe < kSlots; probe++) {
+            const uint32_t wv = owntab[sl];
+            if (wv == kEmpty) break;
+            if ((wv & 0xFFFFu) == h) {
+                cb[(wv >> 16) & (GPZ_SEG - 1)] = ov[u];
+                break;
+            }
+            sl = (sl + 1u) & (kSlots - 1);
+        }
+    }
+}
+
 // One CTA per 4 KiB tile S of a member (persistent over tiles).  The window
 // [S-8, S] plus 320 bytes of lookahead is staged in shared memory.  The
 // tile's distinct hashes go into a shared-memory table; the distinct hashes
@@ -359,6 +401,7 @@ __global__ void __launch_bounds__(T, 1) k_lookup(BatchParams bp) {
         const uint32_t pl0 = start - w0;
         const uint32_t nback = min(S, 8u);
         const uint32_t nown = min(bp.seg_nkeys[t], GPZ_SEG);
+        uint32_t hk[PER], ov[PER];  // join keys of the next back segment
 
         // ---- stage the window [w0, w0 + wvalid) (16-byte vectors; members
         // are 16-byte aligned and padded in the batch input); own-segment
@@ -371,6 +414,9 @@ __global__ void __launch_bounds__(T, 1) k_lookup(BatchParams bp) {
             const uint32_t* go = bp.seg_on + (size_t)t * GPZ_SEG;
             // key counts of the segments the join reads, all loaded at once
             if (tid < nback) s_nback_keys[tid] = bp.seg_nkeys[t - 1u - tid];
+            // the keys of segment S-1 are loaded now, while the window is
+            // staged and the tile's table is built
+            if (nback) join_load<T>(bp, t - 1u, min(bp.seg_nkeys[t - 1u], GPZ_SEG), hk, ov);
             for (uint32_t i = tid; i < nown; i += T) cand[i] = go[i];
             for (uint32_t i = tid; i < nback * GPZ_SEG; i += T) cand[GPZ_SEG + i] = kEmpty;
             for (int i = tid; i < kSlots; i += T) owntab[i] = kEmpty;
@@ -397,44 +443,21 @@ __global__ void __launch_bounds__(T, 1) k_lookup(BatchParams bp) {
         __syncthreads();
 
         // ---- join: the distinct hashes of segments S-1 .. S-8 probe the
-        // tile's table (each segment writes its own candidate row)
+        // tile's table (each segment writes its own candidate row).  The
+        // keys of segment S-back-1 are loaded before S-back's are probed.
         for (uint32_t back = 1; back <= nback; back++) {
-            const uint32_t ts = t - back;  // a member's tiles are consecutive
-            const uint32_t ns = min(s_nback_keys[back - 1], GPZ_SEG);
-            const uint16_t* gk = bp.seg_keys + (size_t)ts * GPZ_SEG;
-            const uint32_t* go = bp.seg_on + (size_t)ts * GPZ_SEG;
-            uint32_t* cb = cand + back * GPZ_SEG;
-            // up to kJoinBatch keys per thread in flight: all loads first
-            // (each guarded by j < ns <= 4096, inside segment ts's arrays),
-            // then the probes
-            constexpr int kJoinBatch = 4;
-            for (uint32_t j0 = tid; j0 < ns; j0 += kJoinBatch * T) {
-                uint32_t hk[kJoinBatch], ov[kJoinBatch];
+            uint32_t hn[PER], on[PER];
+            if (back < nback) {
+                join_load<T>(bp, t - back - 1u, min(s_nback_keys[back], GPZ_SEG), hn, on);
+            } else {
 #pragma unroll
-                for (int u = 0; u < kJoinBatch; u++) {
-                    const uint32_t j = j0 + (uint32_t)u * T;
-                    hk[u] = kEmpty;
-                    ov[u] = 0u;
-                    if (j < ns) {
-                        hk[u] = gk[j];
-                        ov[u] = go[j];
-                    }
-                }
+                for (int u = 0; u < PER; u++) hn[u] = on[u] = kEmpty;
+            }
+            join_probe<T>(owntab, cand + back * GPZ_SEG, hk, ov);
 #pragma unroll
-                for (int u = 0; u < kJoinBatch; u++) {
-                    const uint32_t h = hk[u];
-                    if (h == kEmpty) continue;
-                    uint32_t sl = slot_of(h);
-                    for (int probe = 0; probe < kSlots; probe++) {
-                        const uint32_t wv = owntab[sl];
-                        if (wv == kEmpty) break;
-                        if ((wv & 0xFFFFu) == h) {
-                            cb[(wv >> 16) & (GPZ_SEG - 1)] = ov[u];
-                            break;
-                        }
-                        sl = (sl + 1u) & (kSlots - 1);
-                    }
-                }
+            for (int u = 0; u < PER; u++) {
+                hk[u] = hn[u];
+                ov[u] = on[u];
             }
         }
         __syncthreads();
