@@ -25,6 +25,7 @@ Multi-GPU (torchrun): every rank compresses its own copy of the workload
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -212,6 +213,51 @@ def run_uneven(ctx, args, stream):
             "plain_gbs": round(plain, 4), "batched_over_plain": round(batched / plain, 3),
             "batched_ms": round(min(times), 3), "outputs_identical": same, "host_ms_per_step": host,
             "ratio": round(sum(len(o) for o in outs) / total, 5)}
+
+
+def chunk_fn_rate(ctx, chunks, threads: int = 16, rounds: int = 3):
+    """The ChunkFn drop-in as ParallelChunkedWriter drives it: `threads`
+    workers (max_in_flight for the gpu backend, gpu.rs:160-166) each call
+    gpz_compress_chunk on their share of the chunks, concurrently; input GB/s
+    over the whole set, best of `rounds` after one warm-up round."""
+    import threading
+    import time as _t
+    L = ctx.L
+    outs = [np.empty(ctx.bound(len(x)), dtype=np.uint8) for x in chunks]
+    lens = [ctypes.c_size_t() for _ in chunks]
+    failed = []
+
+    def one_round():
+        go = threading.Barrier(threads + 1)
+
+        def worker(k):
+            go.wait()
+            for i in range(k, len(chunks), threads):
+                a = chunks[i]
+                rc = L.gpz_compress_chunk(ctx._h, a.ctypes.data, a.size, 5, outs[i].ctypes.data, outs[i].size,
+                                          ctypes.byref(lens[i]))
+                if rc:
+                    failed.append(rc)
+
+        th = [threading.Thread(target=worker, args=(k,)) for k in range(threads)]
+        for t in th:
+            t.start()
+        go.wait()
+        t0 = _t.perf_counter()
+        for t in th:
+            t.join()
+        return _t.perf_counter() - t0
+
+    one_round()
+    ctx.host_times(reset=True)
+    best = min(one_round() for _ in range(rounds))
+    passes = ctx.host_times()["passes"] / rounds
+    nbytes = sum(int(x.size) for x in chunks)
+    if failed:
+        return {"failed": sorted(set(failed))}
+    return {"value": round(nbytes / best / 1e9, 4), "unit": "GB/s", "threads": threads, "calls": len(chunks),
+            "passes_per_round": round(passes, 2), "out_bytes": int(sum(x.value for x in lens)),
+            "what": "gpz_compress_chunk from concurrent caller threads (the ChunkFn drop-in), wall clock"}
 
 
 def run_serving(device: int, seconds: float, rates, warm_seconds: float = 0.3):
@@ -473,6 +519,8 @@ def main():
         dist.all_reduce(et, op=dist.ReduceOp.MAX)
     e2e_value = data.size * len(e_times) * world / (float(et.item()) / 1e3) / 1e9
     e2e_host = {k: round(v / max(1, len(e_times)), 3) for k, v in ectx.host_times().items()}
+    # pageable chunks, as a writer hands them over
+    chunk_fn = None if args.device_only else chunk_fn_rate(ectx, [np.ascontiguousarray(data[o:o + n]) for o, n in spans])
 
     stage_ms = stages / args.steps
     names = native.STAGE_NAMES
@@ -530,6 +578,7 @@ def main():
             "e2e": {"value": round(e2e_value, 4), "unit": "GB/s", "h2d_bytes_per_step": int(data.size),
                     "d2h_bytes_per_step": int(e2e_out), "api": "gpz_compress_batch (host buffers; inputs page-locked)",
                     "host_ms_per_step": e2e_host},
+            "chunk_fn": chunk_fn,
             "gpu_launches": int(launches),
             "clocks": clk,
             "ratio": round(ratio, 5),

@@ -257,6 +257,17 @@ struct gpz_ctx {
     int flags = 0;
     int sms = 0;
     std::mutex mu;  // the synchronous entry points (and their slots)
+    // gpz_compress_chunk callers waiting to be batched (see there)
+    struct ChunkCall {
+        gpz_desc d;
+        gpz_out o;
+        int rc = GPZ_OK;
+        bool done = false;
+    };
+    std::mutex comb_mu;
+    std::condition_variable comb_cv;
+    std::deque<ChunkCall*> comb_q;
+    bool comb_busy = false;
     std::string last_err;
     std::atomic<uint64_t> launches{0};
     std::atomic<size_t> pool_used{0};
@@ -1422,16 +1433,60 @@ size_t gpz_bound_ctx(const gpz_ctx* c, size_t n) {
     return nm * member_bound(c->member_bytes);
 }
 
+// Concurrent callers are combined into one batch: each call queues itself;
+// whichever caller finds no batch running takes everything queued (up to
+// batch_bytes), runs it as one gpz_compress_batch and hands every caller
+// its result.  A lone caller runs its chunk at once.  This takes the place
+// of BatchedLz77's submitter thread (batch.rs:48-141), which batches the
+// chunks that ParallelChunkedWriter's workers submit concurrently.
 int gpz_compress_chunk(gpz_ctx* c, const uint8_t* in, size_t n, int level, uint8_t* out, size_t out_cap,
                        size_t* out_len) {
     if (!c || (!in && n) || !out_len) return GPZ_E_ARG;
-    std::lock_guard<std::mutex> lk(c->mu);
-    cudaSetDevice(c->device);
-    gpz_desc d{in, n, level};
-    gpz_out o{out, out_cap, 0, 0};
-    const int rc = run_host_items(c, &d, 1, &o, false);
-    *out_len = o.out_len;
-    return rc != GPZ_OK ? rc : o.status;
+    constexpr int kNotRun = -1000;
+    gpz_ctx::ChunkCall me;
+    me.d = gpz_desc{in, n, level};
+    me.o = gpz_out{out, out_cap, 0, 0};
+    std::unique_lock<std::mutex> q(c->comb_mu);
+    c->comb_q.push_back(&me);
+    while (!me.done) {
+        if (c->comb_busy) {
+            c->comb_cv.wait(q);
+            continue;
+        }
+        c->comb_busy = true;
+        std::vector<gpz_ctx::ChunkCall*> batch;
+        size_t bytes = 0;
+        while (!c->comb_q.empty() && (batch.empty() || bytes + c->comb_q.front()->d.n <= c->batch_bytes)) {
+            batch.push_back(c->comb_q.front());
+            bytes += c->comb_q.front()->d.n;
+            c->comb_q.pop_front();
+        }
+        q.unlock();
+        std::vector<gpz_desc> ds(batch.size());
+        std::vector<gpz_out> os(batch.size());
+        for (size_t i = 0; i < batch.size(); i++) {
+            ds[i] = batch[i]->d;
+            os[i] = batch[i]->o;
+            os[i].status = kNotRun;
+        }
+        int rc;
+        {
+            std::lock_guard<std::mutex> lk(c->mu);
+            cudaSetDevice(c->device);
+            rc = run_host_items(c, ds.data(), ds.size(), os.data(), false);
+        }
+        q.lock();
+        for (size_t i = 0; i < batch.size(); i++) {
+            batch[i]->o = os[i];
+            // an item the batch never reached takes the batch's failure
+            batch[i]->rc = os[i].status != kNotRun ? os[i].status : (rc != GPZ_OK ? rc : GPZ_E_INTERNAL);
+            batch[i]->done = true;
+        }
+        c->comb_busy = false;
+        c->comb_cv.notify_all();
+    }
+    *out_len = me.o.out_len;
+    return me.rc;
 }
 
 int gpz_compress_batch(gpz_ctx* c, const gpz_desc* d, size_t count, gpz_out* outs) {

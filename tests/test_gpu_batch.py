@@ -112,6 +112,47 @@ def test_short_output_buffer_is_reported(ctx):
     assert ctx.compress_chunk(data) == O.gzip_chunk(data.tobytes(), 131072)  # context still usable
 
 
+def test_concurrent_chunk_calls_are_batched():
+    # ParallelChunkedWriter's workers call the ChunkFn concurrently: the
+    # calls are combined into shared passes, and every caller gets exactly
+    # the bytes of a lone call, also with one short output buffer in the mix
+    items = [W.GENERATORS[["text", "logs", "binary"][i % 3]](int(n), seed=500 + i).tobytes()
+             for i, n in enumerate(np.random.default_rng(6).integers(1, 3 << 20, size=48))]
+    items[5] = b""
+    with native.Context() as c:
+        want = [bytes(x) for x in c.compress_batch(items)]
+        c.host_times(reset=True)
+        got = [None] * len(items)
+        errs = []
+        start = threading.Barrier(16)
+        L = c.L
+
+        def worker(k):
+            start.wait()
+            for i in range(k, len(items), 16):
+                if i == 7:
+                    a = np.frombuffer(items[i], dtype=np.uint8)
+                    small = np.zeros(8, dtype=np.uint8)
+                    n = ctypes.c_size_t()
+                    rc = L.gpz_compress_chunk(c._h, a.ctypes.data, a.size, 5, small.ctypes.data, 8, ctypes.byref(n))
+                    if rc != 6 or n.value != len(want[i]):
+                        errs.append((i, rc, n.value))
+                try:
+                    got[i] = c.compress_chunk(items[i])
+                except Exception as e:  # noqa: BLE001
+                    errs.append((i, e))
+
+        th = [threading.Thread(target=worker, args=(k,)) for k in range(16)]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        passes = c.host_times()["passes"]
+    assert not errs, errs
+    assert got == want
+    assert passes < len(items) + 1  # at least two calls shared a pass
+
+
 def test_whole_chunk_member_mode():
     data = W.logs(3 << 20, seed=21).tobytes()
     with native.Context(member_bytes=2 << 20) as c2:
