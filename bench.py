@@ -215,6 +215,53 @@ def run_uneven(ctx, args, stream):
             "ratio": round(sum(len(o) for o in outs) / total, 5)}
 
 
+def inflate_rates(ctx, gz: bytes, want_len: int, steps: int = 5):
+    """Decompression of the workload's gzip stream (the `gpzip x` path):
+    gpz_inflate from page-locked host buffers, copies included (e2e), the
+    device time of its kernels, and the gpzip-cpu equivalent, zlib inflate of
+    the members on all host threads as parallel_decompress does with flate2."""
+    import time as _t
+    from concurrent.futures import ThreadPoolExecutor
+    import zlib as _z
+
+    import torch
+    src = torch.empty(len(gz), dtype=torch.uint8, pin_memory=True).numpy()
+    src[:] = np.frombuffer(gz, dtype=np.uint8)
+    dst = torch.empty(max(want_len, 1), dtype=torch.uint8, pin_memory=True).numpy()
+    for _ in range(2):
+        ctx.inflate(src, out=dst)
+    ts, dev = [], []
+    for _ in range(steps):
+        t0 = _t.perf_counter()
+        n = len(ctx.inflate(src, out=dst))
+        ts.append(_t.perf_counter() - t0)
+        dev.append(ctx.inflate_device_ms())
+    assert n == want_len
+    hdr = bytes([0x1F, 0x8B, 0x08, 0, 0, 0, 0, 0, 0, 0xFF])
+    starts, p = [], 0
+    while True:
+        q = gz.find(hdr, p)
+        if q < 0:
+            break
+        starts.append(q)
+        p = q + 10
+    members = [gz[a:b] for a, b in zip(starts, starts[1:] + [len(gz)])]
+    threads = os.cpu_count() or 1
+    with ThreadPoolExecutor(threads) as ex:
+        list(ex.map(lambda m: _z.decompress(m, 31), members))
+        t0 = _t.perf_counter()
+        out_n = sum(len(x) for x in ex.map(lambda m: _z.decompress(m, 31), members))
+        tc = _t.perf_counter() - t0
+    assert out_n == want_len
+    dms = statistics.median(dev)
+    return {"value": round(want_len / min(ts) / 1e9, 4), "unit": "GB/s of output",
+            "members": len(members), "in_bytes": len(gz), "out_bytes": want_len,
+            "device_ms": round(dms, 4), "device_gbs": round(want_len / (dms / 1e3) / 1e9, 4),
+            "cpu_zlib": {"value": round(want_len / tc / 1e9, 4), "threads": threads,
+                         "what": "zlib inflate per member on a thread pool (parallel_decompress equivalent)"},
+            "what": "gpz_inflate: page-locked host buffers, copies inside the timed region, wall clock"}
+
+
 def chunk_fn_rate(ctx, chunks, threads: int = 16, rounds: int = 3):
     """The ChunkFn drop-in as ParallelChunkedWriter drives it: `threads`
     workers (max_in_flight for the gpu backend, gpu.rs:160-166) each call
@@ -519,6 +566,10 @@ def main():
         dist.all_reduce(et, op=dist.ReduceOp.MAX)
     e2e_value = data.size * len(e_times) * world / (float(et.item()) / 1e3) / 1e9
     e2e_host = {k: round(v / max(1, len(e_times)), 3) for k, v in ectx.host_times().items()}
+    inflate = None
+    if not args.device_only:
+        gz_all = b"".join(bytes(x) for x in outs)
+        inflate = inflate_rates(ectx, gz_all, data.size)
     # pageable chunks, as a writer hands them over
     chunk_fn = None if args.device_only else chunk_fn_rate(ectx, [np.ascontiguousarray(data[o:o + n]) for o, n in spans])
 
@@ -579,6 +630,7 @@ def main():
                     "d2h_bytes_per_step": int(e2e_out), "api": "gpz_compress_batch (host buffers; inputs page-locked)",
                     "host_ms_per_step": e2e_host},
             "chunk_fn": chunk_fn,
+            "inflate": inflate,
             "gpu_launches": int(launches),
             "clocks": clk,
             "ratio": round(ratio, 5),

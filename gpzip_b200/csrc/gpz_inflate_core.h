@@ -1,0 +1,517 @@
+// gpz_inflate_core.h -- RFC 1951 decoder for one gzip member, written once
+// for two builds:
+//   * CUDA (NL = 32): one warp decodes one member.  Every lane runs the same
+//     decode on the same data (lane-uniform control flow), and the lanes
+//     share the wide work: staging input, filling lookup tables, copying
+//     matches and flushing output.
+//   * host C++ (NL = 1): the same code on one thread, which the CPU tests
+//     check against zlib.
+//
+// It replaces, for gpzip-written archives, the per-member GzDecoder of
+// crates/gpzip-codec-cpu/src/parallel_decompress.rs:63-113 (flate2).  The
+// decoder follows RFC 1951 directly: block types 0 (stored), 1 (fixed) and
+// 2 (dynamic), canonical Huffman codes (RFC 1951 3.2.2), the code-length
+// alphabet and its repeat codes 16/17/18 (3.2.7), and the length / distance
+// tables of 3.2.5.  It checks what zlib's inflate checks and reports, never
+// writes outside the member's output range, and never reads outside its
+// input range: every failure is a status code.
+#pragma once
+
+#include <stdint.h>
+
+#if defined(__CUDACC__)
+#define GPZI_FN __host__ __device__ __forceinline__
+#else
+#define GPZI_FN inline
+#endif
+
+namespace gpzi {
+
+constexpr uint32_t kRing = 32768;   // window ring of the last 32 KiB of output
+constexpr uint32_t kStage = 4096;   // input bytes staged at a time
+constexpr uint32_t kFlush = 4096;   // output flushed to its destination in steps of this
+constexpr int kFastBits = 9;        // first-level table index width
+
+// status codes of one member
+enum : uint32_t {
+    kOk = 0,
+    kErrBlockType = 1,   // block type 3
+    kErrStoredLen = 2,   // LEN != ~NLEN
+    kErrCodeLens = 3,    // bad code-length code or repeat
+    kErrCodeSet = 4,     // over-subscribed or incomplete code
+    kErrSymbol = 5,      // a code that no symbol has, or litlen 286/287, dist 30/31
+    kErrDistance = 6,    // distance beyond the start of the member
+    kErrOutput = 7,      // output longer than ISIZE
+    kErrInput = 8,       // ran past the end of the member's deflate bytes
+    kErrLength = 9,      // output shorter than ISIZE
+    kErrTrailing = 10,   // deflate data ends before the trailer
+    kErrCrc = 11,        // CRC-32 differs from the trailer (set by the CRC pass)
+    kErrEmptyLen = 12,   // a table without any code is used
+};
+
+// Decoded entries carry what the decoder needs next, so it never maps a
+// symbol again: bits 0-3 code length (fast table; 0 = not in the fast
+// table), bits 4-5 kind, then per table kind
+//   litlen:  kind 0 literal (byte in bits 8-15), 1 length (base in bits
+//            8-16, extra bits in 17-19), 2 end of block, 3 invalid (286, 287)
+//   dist:    kind 0 (base in bits 8-22, extra bits in 24-27), 3 invalid (30, 31)
+//   meta:    kind 0, the code-length symbol in bits 8-15
+enum : uint32_t { kTabMeta = 0, kTabLit = 1, kTabDist = 2 };
+struct Table {
+    uint32_t fast[1 << kFastBits];  // entries of codes of <= kFastBits bits, 0 otherwise
+    uint16_t count[16];             // codes of each length
+    uint16_t sym[320];              // symbols ordered by (length, value)
+};
+
+struct Shared {
+    uint8_t ring[kRing];
+    alignas(4) uint8_t stage[kStage + 16];
+    Table lit, dist;
+    uint8_t lens[320];
+    uint32_t bcast;  // a value lane 0 computed, for every lane
+};
+
+GPZI_FN void lane_sync() {
+#if defined(__CUDA_ARCH__)
+    __syncwarp();
+#endif
+}
+
+// Lane-uniform bit reader over the member's deflate bytes src[0, len).
+// Input is staged kStage + 16 bytes at a time by all lanes (zeros past
+// len).  Bits of buf at and above cnt are always the stream's next bits (or
+// zero), so a refill may OR the next eight bytes in at cnt (libdeflate's
+// branch-free refill).  Reading past the end yields zeros; the loops stop
+// once pos is more than 8 bytes past len, and the exact check at the end
+// catches a smaller overrun.
+template <int NL>
+struct Bits {
+    const uint8_t* src;
+    uint32_t len;
+    uint32_t pos;   // next input byte not yet counted in cnt
+    uint64_t buf;
+    uint32_t cnt;   // valid bits in buf
+    uint32_t lane;
+    uint32_t base;  // input offset of s.stage[0], a multiple of 4
+
+    GPZI_FN void restage(Shared& s, uint32_t p) {
+        lane_sync();  // every lane is done with the old stage
+        base = p & ~3u;
+        for (uint32_t k = lane; k < kStage + 16; k += NL)
+            s.stage[k] = base + k < len ? src[base + k] : (uint8_t)0;
+        lane_sync();
+    }
+    // afterwards at least 56 bits are valid
+    GPZI_FN void refill(Shared& s) {
+        if (pos - base > kStage) restage(s, pos);
+        const uint32_t off = pos - base, i = off >> 2, sh = (off & 3u) * 8u;
+        const uint32_t* w = reinterpret_cast<const uint32_t*>(s.stage);
+        uint64_t v = ((uint64_t)w[i + 1] << 32 | w[i]) >> sh;
+        if (sh) v |= (uint64_t)w[i + 2] << (64u - sh);
+        buf |= v << cnt;
+        const uint32_t nb = (63u - cnt) >> 3;
+        pos += nb;
+        cnt += nb * 8u;
+    }
+    GPZI_FN uint32_t peek(uint32_t n) const { return (uint32_t)(buf & ((1ull << n) - 1ull)); }
+    GPZI_FN void drop(uint32_t n) {
+        buf >>= n;
+        cnt -= n;
+    }
+    GPZI_FN uint32_t take(Shared& s, uint32_t n) {  // n <= 32
+        if (cnt < n) refill(s);
+        const uint32_t v = peek(n);
+        drop(n);
+        return v;
+    }
+    // bits consumed so far, padding included
+    GPZI_FN uint64_t consumed() const { return 8ull * pos - cnt; }
+    GPZI_FN bool overrun() const { return consumed() > 8ull * len; }
+    GPZI_FN bool far_past_end() const { return pos > len + 8u; }
+};
+
+struct LenDist {
+    uint32_t base;
+    uint32_t extra;
+};
+// RFC 1951 3.2.5 by arithmetic (no tables): length symbol 257 + i
+GPZI_FN LenDist len_row(uint32_t i) {
+    if (i >= 28u) return LenDist{258u, 0u};
+    if (i < 8u) return LenDist{i + 3u, 0u};
+    const uint32_t e = (i >> 2) - 1u;
+    return LenDist{((4u + (i & 3u)) << e) + 3u, e};
+}
+// distance code i (0..29)
+GPZI_FN LenDist dist_row(uint32_t i) {
+    if (i < 4u) return LenDist{i + 1u, 0u};
+    const uint32_t e = (i >> 1) - 1u;
+    return LenDist{((2u + (i & 1u)) << e) + 1u, e};
+}
+// position i of the code-length code lengths: 16, 17, 18, 0, 8, 7, 9, 6, ...
+GPZI_FN uint32_t meta_order(uint32_t i) {
+    if (i < 3u) return 16u + i;
+    if (i == 3u) return 0u;
+    const uint32_t k = i - 4u;
+    return (k & 1u) ? 7u - (k >> 1) : 8u + (k >> 1);
+}
+
+GPZI_FN uint32_t pack_entry(uint32_t kind, uint32_t sym, uint32_t l) {
+    if (kind == kTabLit) {
+        if (sym < 256u) return l | (sym << 8);
+        if (sym == 256u) return l | (2u << 4);
+        if (sym > 285u) return l | (3u << 4);
+        const LenDist r = len_row(sym - 257u);
+        return l | (1u << 4) | (r.base << 8) | (r.extra << 17);
+    }
+    if (kind == kTabDist) {
+        if (sym > 29u) return l | (3u << 4);
+        const LenDist r = dist_row(sym);
+        return l | (r.base << 8) | (r.extra << 24);
+    }
+    return l | (sym << 8);
+}
+
+// Builds t from code lengths lens[0, n): counts, the symbols in canonical
+// order (lane 0), then the first-level table (all lanes).  As zlib's
+// inflate_table: an over-subscribed code is an error, and so is an
+// incomplete one, except for a single code of length 1 in the litlen and
+// distance codes (meta = false); a code with no symbols at all is accepted
+// (empty = true) and fails only when used.
+template <int NL>
+GPZI_FN uint32_t build_table(Shared& s, Table& t, uint32_t kind, const uint8_t* lens, uint32_t n, uint32_t lane,
+                             bool& empty) {
+    const bool meta = kind == kTabMeta;
+    if (lane == 0) {
+        uint32_t st = kOk;
+        uint16_t offs[16];
+        for (int i = 0; i < 16; i++) t.count[i] = 0;
+        for (uint32_t i = 0; i < n; i++) t.count[lens[i]]++;
+        int left = 1, maxlen = 0;  // codes of the current length still unassigned
+        for (int l = 1; l < 16; l++) {
+            if (t.count[l]) maxlen = l;
+            if (left < 0) continue;
+            left = 2 * left - t.count[l];
+            if (left < 0) st = kErrCodeSet;
+        }
+        if (st == kOk && left > 0 && maxlen > 0 && (meta || maxlen > 1)) st = kErrCodeSet;
+        offs[1] = 0;
+        for (int l = 1; l < 15; l++) offs[l + 1] = (uint16_t)(offs[l] + t.count[l]);
+        if (st == kOk)
+            for (uint32_t i = 0; i < n; i++)
+                if (lens[i]) t.sym[offs[lens[i]]++] = (uint16_t)i;
+        t.count[0] = 0;
+        s.bcast = st;
+    }
+    lane_sync();
+    const uint32_t st = s.bcast;
+    uint32_t total = 0;
+    for (int l = 1; l < 16; l++) total += t.count[l];
+    empty = total == 0;
+    if (st != kOk) {
+        lane_sync();
+        return st;
+    }
+    // first-level entries: index = the next kFastBits stream bits (first
+    // stream bit in bit 0); canonical walk over at most kFastBits lengths
+    for (uint32_t idx = lane; idx < (1u << kFastBits); idx += NL) {
+        uint32_t code = 0, first = 0, index = 0, e = 0;
+        for (uint32_t l = 1; l <= (uint32_t)kFastBits; l++) {
+            code |= (idx >> (l - 1)) & 1u;
+            const uint32_t c = t.count[l];
+            if (code - first < c) {
+                e = pack_entry(kind, t.sym[index + code - first], l);
+                break;
+            }
+            index += c;
+            first += c;
+            first <<= 1;
+            code <<= 1;
+        }
+        t.fast[idx] = e;
+    }
+    lane_sync();
+    return kOk;
+}
+
+// One code's entry (see Table); refills so that at least 15 bits are
+// available.  Codes longer than kFastBits are walked length by length
+// (RFC 1951 3.2.2).
+template <int NL>
+GPZI_FN uint32_t decode_entry(Shared& s, Bits<NL>& b, const Table& t, uint32_t kind, uint32_t& err) {
+    if (b.cnt < 15) b.refill(s);
+    const uint32_t e = t.fast[b.peek(kFastBits)];
+    if (e) {
+        b.drop(e & 15u);
+        return e;
+    }
+    uint32_t code = 0, first = 0, index = 0;
+    for (uint32_t l = 1; l < 16; l++) {
+        code |= (uint32_t)(b.buf >> (l - 1)) & 1u;
+        const uint32_t c = t.count[l];
+        if (code - first < c) {
+            b.drop(l);
+            return pack_entry(kind, t.sym[index + code - first], 0u);
+        }
+        index += c;
+        first += c;
+        first <<= 1;
+        code <<= 1;
+    }
+    err = kErrSymbol;
+    return 0;
+}
+
+
+// Output state: bytes [0, o) of the member are produced, [0, flushed) of
+// them already copied to dst; the ring holds the last kRing bytes.
+template <int NL>
+struct Out {
+    uint8_t* dst;
+    uint32_t cap;  // ISIZE
+    uint32_t o;
+    uint32_t flushed;
+    uint32_t lane;
+
+    GPZI_FN void flush(Shared& s, uint32_t upto) {
+        lane_sync();
+        for (uint32_t k = flushed + lane; k < upto; k += NL) dst[k] = s.ring[k & (kRing - 1)];
+        flushed = upto;
+    }
+    GPZI_FN void maybe_flush(Shared& s) {
+        if (o - flushed >= kFlush) flush(s, flushed + kFlush);
+    }
+};
+
+// Decodes one member's deflate data src[0, len) into dst[0, isize).
+// Returns a status code; on kOk exactly isize bytes were written and the
+// data ended exactly at len.
+template <int NL>
+GPZI_FN uint32_t inflate_member(Shared& s, uint32_t lane, const uint8_t* src, uint32_t len, uint8_t* dst,
+                                uint32_t isize) {
+    Bits<NL> b{src, len, 0u, 0ull, 0u, lane, 0u};
+    Out<NL> out{dst, isize, 0u, 0u, lane};
+    b.restage(s, 0);
+    uint32_t err = kOk;
+    bool last = false;
+    // every block consumes at least 3 bits and every symbol at least 1, and
+    // past the end of the input the reader yields zero bits and the
+    // overrun checks stop the loops
+    while (!last && err == kOk) {
+        if (b.far_past_end()) {
+            err = kErrInput;
+            break;
+        }
+        last = b.take(s, 1) != 0;
+        const uint32_t type = b.take(s, 2);
+        if (type == 0) {
+            // stored: to a byte boundary, LEN, NLEN, then LEN raw bytes
+            b.drop(b.cnt & 7u);
+            const uint32_t ln = b.take(s, 16), nl = b.take(s, 16);
+            if ((ln ^ 0xFFFFu) != nl) {
+                err = kErrStoredLen;
+                break;
+            }
+            if (out.o + ln > out.cap) {
+                err = kErrOutput;
+                break;
+            }
+            // whole bytes still in the bit buffer come first
+            uint32_t k = 0;
+            for (; k < ln && b.cnt >= 8; k++) {
+                if (lane == 0) s.ring[(out.o + k) & (kRing - 1)] = (uint8_t)b.peek(8);
+                b.drop(8);
+            }
+            out.o += k;
+            // then straight from the input, at most kFlush / 2 bytes a round
+            // so that the unflushed part always fits the ring; the bit
+            // buffer is empty and its look-ahead stale from here
+            if (k < ln) b.buf = 0;
+            while (k < ln) {
+                const uint32_t step = ln - k < kFlush / 2 ? ln - k : kFlush / 2;
+                lane_sync();
+                for (uint32_t q = lane; q < step; q += NL) {
+                    const uint32_t p = b.pos + q;
+                    s.ring[(out.o + q) & (kRing - 1)] = p < len ? src[p] : (uint8_t)0;
+                }
+                b.pos += step;
+                k += step;
+                out.o += step;
+                out.maybe_flush(s);
+            }
+            if (b.overrun()) err = kErrInput;
+            out.maybe_flush(s);
+            continue;
+        }
+        if (type == 3) {
+            err = kErrBlockType;
+            break;
+        }
+        bool lit_empty = false, dist_empty = false;
+        if (type == 1) {
+            lane_sync();
+            if (lane == 0) {
+                for (int i = 0; i < 144; i++) s.lens[i] = 8;
+                for (int i = 144; i < 256; i++) s.lens[i] = 9;
+                for (int i = 256; i < 280; i++) s.lens[i] = 7;
+                for (int i = 280; i < 288; i++) s.lens[i] = 8;
+                for (int i = 288; i < 320; i++) s.lens[i] = 5;
+            }
+            lane_sync();
+            build_table<NL>(s, s.lit, kTabLit, s.lens, 288, lane, lit_empty);
+            build_table<NL>(s, s.dist, kTabDist, s.lens + 288, 32, lane, dist_empty);
+        } else {
+            const uint32_t hlit = b.take(s, 5) + 257, hdist = b.take(s, 5) + 1, hclen = b.take(s, 4) + 4;
+            lane_sync();
+            if (lane == 0)
+                for (int i = 0; i < 19; i++) s.lens[i] = 0;
+            for (uint32_t i = 0; i < hclen; i++) {
+                const uint32_t v = b.take(s, 3);
+                if (lane == 0) s.lens[meta_order(i)] = (uint8_t)v;
+            }
+            lane_sync();
+            if (hlit > 286 || hdist > 30) {
+                err = kErrCodeLens;
+                break;
+            }
+            bool cl_empty = false;
+            if (build_table<NL>(s, s.lit, kTabMeta, s.lens, 19, lane, cl_empty) != kOk || cl_empty) {
+                err = kErrCodeLens;
+                break;
+            }
+            // the litlen and distance code lengths as one sequence (3.2.7)
+            uint32_t i = 0, prev = 0;
+            const uint32_t nl = hlit + hdist;
+            while (i < nl) {
+                const uint32_t sym = (decode_entry<NL>(s, b, s.lit, kTabMeta, err) >> 8) & 255u;
+                if (err) break;
+                uint32_t rep = 1, val = sym;
+                if (sym == 16) {
+                    if (i == 0) {
+                        err = kErrCodeLens;
+                        break;
+                    }
+                    val = prev;
+                    rep = 3 + b.take(s, 2);
+                } else if (sym == 17) {
+                    val = 0;
+                    rep = 3 + b.take(s, 3);
+                } else if (sym == 18) {
+                    val = 0;
+                    rep = 11 + b.take(s, 7);
+                }
+                if (i + rep > nl) {
+                    err = kErrCodeLens;
+                    break;
+                }
+                lane_sync();
+                if (lane == 0)
+                    for (uint32_t r = 0; r < rep; r++) s.lens[i + r] = (uint8_t)val;
+                lane_sync();
+                prev = val;
+                i += rep;
+            }
+            if (err) break;
+            if (b.far_past_end()) {
+                err = kErrInput;
+                break;
+            }
+            if (s.lens[256] == 0) {  // no end-of-block code
+                err = kErrCodeLens;
+                break;
+            }
+            // distance lengths moved to s.lens[288, 318) (from the top down:
+            // the ranges may overlap and the target lies above), litlen
+            // lengths stay in s.lens[0, hlit)
+            if (lane == 0) {
+                for (uint32_t q = 30; q-- > 0;) s.lens[288 + q] = q < hdist ? s.lens[hlit + q] : (uint8_t)0;
+                s.lens[318] = s.lens[319] = 0;
+            }
+            lane_sync();
+            if (build_table<NL>(s, s.lit, kTabLit, s.lens, hlit, lane, lit_empty) != kOk ||
+                build_table<NL>(s, s.dist, kTabDist, s.lens + 288, 30, lane, dist_empty) != kOk) {
+                err = kErrCodeSet;
+                break;
+            }
+        }
+        // symbols up to the end of the block
+        for (;;) {
+            if (b.far_past_end()) {
+                err = kErrInput;
+                break;
+            }
+            const uint32_t e = decode_entry<NL>(s, b, s.lit, kTabLit, err);
+            if (err) break;
+            const uint32_t kind = (e >> 4) & 3u;
+            if (kind == 0u) {
+                if (out.o >= out.cap) {
+                    err = kErrOutput;
+                    break;
+                }
+                s.ring[out.o & (kRing - 1)] = (uint8_t)(e >> 8);  // every lane, the same byte
+                out.o++;
+                out.maybe_flush(s);
+                continue;
+            }
+            if (kind == 2u) break;
+            if (kind == 3u) {
+                err = kErrSymbol;
+                break;
+            }
+            const uint32_t lx = (e >> 17) & 7u;
+            const uint32_t mlen = ((e >> 8) & 511u) + (lx ? b.take(s, lx) : 0u);
+            if (dist_empty) {
+                err = kErrEmptyLen;
+                break;
+            }
+            const uint32_t de = decode_entry<NL>(s, b, s.dist, kTabDist, err);
+            if (err) break;
+            if (((de >> 4) & 3u) == 3u) {
+                err = kErrSymbol;
+                break;
+            }
+            const uint32_t dx = (de >> 24) & 15u;
+            const uint32_t d = ((de >> 8) & 0x7FFFu) + (dx ? b.take(s, dx) : 0u);
+            if (d > out.o) {
+                err = kErrDistance;
+                break;
+            }
+            if (out.o + mlen > out.cap) {
+                err = kErrOutput;
+                break;
+            }
+            if (d >= NL && d <= kRing - NL) {
+                // byte o + k = byte o + k - d, which precedes this step of
+                // NL bytes, and no write of a step hits a slot that the same
+                // step reads
+                for (uint32_t k0 = 0; k0 < mlen; k0 += NL) {
+                    const uint32_t k = k0 + lane;
+                    lane_sync();
+                    if (k < mlen) s.ring[(out.o + k) & (kRing - 1)] = s.ring[(out.o + k - d) & (kRing - 1)];
+                }
+            } else {
+                // byte o + k = byte o - d + (k mod d), which precedes o; each
+                // step reads before any lane writes
+                for (uint32_t k0 = 0; k0 < mlen; k0 += NL) {
+                    const uint32_t k = k0 + lane;
+                    lane_sync();
+                    uint8_t v = 0;
+                    if (k < mlen) v = s.ring[(out.o - d + (d >= mlen ? k : k % d)) & (kRing - 1)];
+                    lane_sync();
+                    if (k < mlen) s.ring[(out.o + k) & (kRing - 1)] = v;
+                }
+            }
+            out.o += mlen;
+            out.maybe_flush(s);
+        }
+    }
+    if (err == kOk) {
+        if (b.overrun()) err = kErrInput;
+        else if (out.o != out.cap) err = kErrLength;
+        else if ((b.consumed() + 7u) / 8u != len) err = kErrTrailing;
+    }
+    if (err == kOk) out.flush(s, out.o);
+    lane_sync();
+    return err;
+}
+
+}  // namespace gpzi

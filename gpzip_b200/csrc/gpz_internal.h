@@ -139,6 +139,21 @@ int gpz_launch_batch(const BatchParams& bp, const LaunchShape& ls, void* stream,
                      const DrainTarget* drain, const FetchSource* fetch = nullptr);
 // k_drain alone, for a batch whose stage kernels ran on another stream.
 int gpz_launch_drain(const BatchParams& bp, const DrainTarget& drain, void* stream);
+// One gzip member of a stream to decompress (gpz_inflate).
+struct InflateMember {
+    uint64_t in_off;   // first DEFLATE byte (after the 10-byte header)
+    uint64_t out_off;  // first output byte
+    uint32_t in_len;   // DEFLATE bytes (member bytes - 18)
+    uint32_t isize;    // ISIZE of the trailer
+    uint32_t crc;      // CRC-32 of the trailer
+    uint32_t pad;
+};
+// k_inflate (one warp per member) then k_inflate_crc (gpz_inflate.cu);
+// status[m] = 0 or the member's gpzi status code.  events: NULL or two
+// cudaEvent_t recorded before and after.
+int gpz_launch_inflate(const uint8_t* in, uint8_t* out, const InflateMember* members, uint32_t* status,
+                       uint32_t count, void* stream, void* const* events);
+size_t gpz_inflate_smem_bytes();
 // Persistent grid sizes (SMs x resident CTAs) for the shape's thread counts.
 int gpz_occupancy(LaunchShape* persistent);
 int gpz_kernel_smem_setup();

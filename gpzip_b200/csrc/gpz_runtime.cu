@@ -38,6 +38,7 @@
 #include <vector>
 
 #include "../../include/gpz.h"
+#include "gpz_inflate_core.h"
 #include "gpz_internal.h"
 
 namespace {
@@ -264,6 +265,11 @@ struct gpz_ctx {
         int rc = GPZ_OK;
         bool done = false;
     };
+    // gpz_inflate's device buffers (d_in, d_out, d_members: the member
+    // descriptors, d_cnt: their statuses) and pinned staging
+    Slot inf;
+    cudaEvent_t inf_ev[2] = {nullptr, nullptr};
+    float inf_ms = 0;
     std::mutex comb_mu;
     std::condition_variable comb_cv;
     std::deque<ChunkCall*> comb_q;
@@ -1418,6 +1424,9 @@ void gpz_destroy(gpz_ctx* c) {
     }
     if (c->kstream) cudaStreamSynchronize(c->kstream);
     for (auto& s : c->slots) free_slot(c, s);
+    free_slot(c, c->inf);
+    for (auto& e : c->inf_ev)
+        if (e) cudaEventDestroy(e);
     if (c->kstream) cudaStreamDestroy(c->kstream);
     delete c;
 }
@@ -1541,6 +1550,147 @@ int gpz_compress_device(gpz_ctx* c, const void* d_in, const uint64_t* in_off, co
     for (size_t i = 0; i < count; i++) out_off[i] = c->mout[sl.spans[i].first_member].gz_off;
     const MemberOut& l = c->mout.back();
     out_off[count] = l.gz_off + 18 + l.deflate_bytes;
+    return GPZ_OK;
+}
+
+namespace {
+
+const uint8_t kGzipHeader[10] = {0x1f, 0x8b, 0x08, 0x00, 0x00, 0x00, 0x00, 0x00, 0x00, 0xff};
+
+uint32_t le32(const uint8_t* p) { return p[0] | (uint32_t)p[1] << 8 | (uint32_t)p[2] << 16 | (uint32_t)p[3] << 24; }
+
+// Member boundaries as find_member_starts (parallel_decompress.rs:36-58):
+// every occurrence of the header, scanning on 10 bytes past each one.
+int split_members(const uint8_t* in, size_t n, std::vector<InflateMember>* ms, size_t* total, std::string* why) {
+    if (ms) ms->clear();
+    *total = 0;
+    if (n == 0) return GPZ_OK;
+    if (n < 18 || std::memcmp(in, kGzipHeader, 10) != 0) {
+        *why = "the stream does not start with gpzip's gzip header";
+        return GPZ_E_DATA;
+    }
+    std::vector<size_t> starts{0};
+    for (size_t p = 10; p + 10 <= n;) {
+        const void* q = memmem(in + p, n - p, kGzipHeader, 10);
+        if (!q) break;
+        const size_t at = static_cast<const uint8_t*>(q) - in;
+        starts.push_back(at);
+        p = at + 10;
+    }
+    uint64_t out = 0;
+    for (size_t i = 0; i < starts.size(); i++) {
+        const size_t b = starts[i], e = i + 1 < starts.size() ? starts[i + 1] : n;
+        if (e - b < 18 || e - b - 18 > 0xFFFFFFFFull) {
+            *why = "member " + std::to_string(i) + " at byte " + std::to_string(b) + " has an impossible length";
+            return GPZ_E_DATA;
+        }
+        InflateMember m{};
+        m.in_off = b + 10;
+        m.in_len = (uint32_t)(e - b - 18);
+        m.crc = le32(in + e - 8);
+        m.isize = le32(in + e - 4);
+        // DEFLATE expands at most 1032:1 (a 258-byte match in 2 bits)
+        if (m.isize > 1032ull * (m.in_len + 1ull)) {
+            *why = "member " + std::to_string(i) + " at byte " + std::to_string(b) + " claims more output than its data can hold";
+            return GPZ_E_DATA;
+        }
+        m.out_off = out;
+        out += m.isize;
+        if (ms) ms->push_back(m);
+    }
+    *total = out;
+    return GPZ_OK;
+}
+
+const char* inflate_reason(uint32_t st) {
+    switch (st) {
+        case gpzi::kErrBlockType: return "invalid block type";
+        case gpzi::kErrStoredLen: return "stored block length check";
+        case gpzi::kErrCodeLens: return "invalid code lengths";
+        case gpzi::kErrCodeSet: return "over-subscribed or incomplete code";
+        case gpzi::kErrSymbol: return "invalid code";
+        case gpzi::kErrDistance: return "distance too far back";
+        case gpzi::kErrOutput: return "output longer than ISIZE";
+        case gpzi::kErrInput: return "ran past the end of the member";
+        case gpzi::kErrLength: return "output shorter than ISIZE";
+        case gpzi::kErrTrailing: return "data between the last block and the trailer";
+        case gpzi::kErrCrc: return "CRC-32 mismatch";
+        case gpzi::kErrEmptyLen: return "distance code used but none defined";
+        default: return "decode error";
+    }
+}
+
+}  // namespace
+
+int gpz_inflate_size(const uint8_t* in, size_t n, size_t* members, size_t* out_bytes) {
+    if ((!in && n) || !out_bytes) return GPZ_E_ARG;
+    std::vector<InflateMember> ms;
+    std::string why;
+    size_t total = 0;
+    const int rc = split_members(in, n, &ms, &total, &why);
+    if (members) *members = rc == GPZ_OK ? ms.size() : 0;
+    *out_bytes = rc == GPZ_OK ? total : 0;
+    return rc;
+}
+
+float gpz_inflate_device_ms(const gpz_ctx* c) { return c ? c->inf_ms : 0.0f; }
+
+int gpz_inflate(gpz_ctx* c, const uint8_t* in, size_t n, uint8_t* out, size_t out_cap, size_t* out_len) {
+    if (!c || (!in && n) || !out_len) return GPZ_E_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    cudaSetDevice(c->device);
+    std::vector<InflateMember> ms;
+    std::string why;
+    size_t total = 0;
+    int rc = split_members(in, n, &ms, &total, &why);
+    *out_len = total;
+    if (rc) return fail(c, rc, why.c_str());
+    if (total > out_cap || (!out && total)) return fail(c, GPZ_E_SPACE, "output buffer too small");
+    if (ms.empty()) return GPZ_OK;
+    Slot& sl = c->inf;
+    const size_t nm = ms.size();
+    if ((rc = ensure_dev(c, sl, sl.d_in, n + 16)) || (rc = ensure_dev(c, sl, sl.d_out, total + 16)) ||
+        (rc = ensure_dev(c, sl, sl.d_members, nm * sizeof(InflateMember))) ||
+        (rc = ensure_dev(c, sl, sl.d_cnt, nm * 4)))
+        return rc;
+    for (auto& e : c->inf_ev)
+        if (!e) CU(c, cudaEventCreate(&e));
+    cudaStream_t s = c->kstream;
+    cudaPointerAttributes a{};
+    const bool in_locked = cudaPointerGetAttributes(&a, in) == cudaSuccess && a.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+    if (in_locked) {
+        CU(c, cudaMemcpyAsync(sl.d_in.p, in, n, cudaMemcpyHostToDevice, s));
+    } else {
+        if ((rc = ensure_host(c, sl, sl.h_in, sl.h_in_cap, n, false))) return rc;
+        copy_pool().run({CopyPool::Copy{sl.h_in, in, n}}, true);
+        CU(c, cudaMemcpyAsync(sl.d_in.p, sl.h_in, n, cudaMemcpyHostToDevice, s));
+    }
+    CU(c, cudaMemcpyAsync(sl.d_members.p, ms.data(), nm * sizeof(InflateMember), cudaMemcpyHostToDevice, s));
+    if (gpz_launch_inflate(static_cast<const uint8_t*>(sl.d_in.p), static_cast<uint8_t*>(sl.d_out.p),
+                           static_cast<const InflateMember*>(sl.d_members.p), static_cast<uint32_t*>(sl.d_cnt.p),
+                           (uint32_t)nm, s, reinterpret_cast<void* const*>(c->inf_ev)) != 0)
+        return fail(c, GPZ_E_CUDA, "inflate launch", cudaGetLastError());
+    const bool out_locked = cudaPointerGetAttributes(&a, out) == cudaSuccess && a.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+    std::vector<uint32_t> status(nm);
+    CU(c, cudaMemcpyAsync(status.data(), sl.d_cnt.p, nm * 4, cudaMemcpyDeviceToHost, s));
+    if (out_locked) {
+        CU(c, cudaMemcpyAsync(out, sl.d_out.p, total, cudaMemcpyDeviceToHost, s));
+        CU(c, cudaStreamSynchronize(s));
+    } else {
+        if ((rc = ensure_host(c, sl, sl.h_out, sl.h_out_cap, total, false))) return rc;
+        CU(c, cudaMemcpyAsync(sl.h_out, sl.d_out.p, total, cudaMemcpyDeviceToHost, s));
+        CU(c, cudaStreamSynchronize(s));
+    }
+    cudaEventElapsedTime(&c->inf_ms, c->inf_ev[0], c->inf_ev[1]);
+    for (size_t i = 0; i < nm; i++)
+        if (status[i] != gpzi::kOk) {
+            why = "member " + std::to_string(i) + " at byte " + std::to_string(ms[i].in_off - 10) + ": " +
+                  inflate_reason(status[i]);
+            return fail(c, GPZ_E_DATA, why.c_str());
+        }
+    if (!out_locked) copy_pool().run({CopyPool::Copy{out, sl.h_out, total}});
     return GPZ_OK;
 }
 
@@ -1687,6 +1837,7 @@ const char* gpz_strerror(int s) {
         case GPZ_E_INTERNAL: return "device self-check failed";
         case GPZ_E_BUSY: return "serving queue full";
         case GPZ_E_PENDING: return "result not ready";
+        case GPZ_E_DATA: return "gzip data this path cannot split or decode";
         default: return "unknown status";
     }
 }

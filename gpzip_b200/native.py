@@ -15,7 +15,9 @@ LIB_PATH = os.path.join(HERE, "libgpz.so")
 
 GPZ_OK = 0
 STATUS = {0: "GPZ_OK", 1: "GPZ_E_NOMEM", 2: "GPZ_E_ADMISSION", 3: "GPZ_E_TIMEOUT", 4: "GPZ_E_CUDA",
-          5: "GPZ_E_ARG", 6: "GPZ_E_SPACE", 7: "GPZ_E_INTERNAL", 8: "GPZ_E_BUSY", 9: "GPZ_E_PENDING"}
+          5: "GPZ_E_ARG", 6: "GPZ_E_SPACE", 7: "GPZ_E_INTERNAL", 8: "GPZ_E_BUSY", 9: "GPZ_E_PENDING",
+          10: "GPZ_E_DATA"}
+GPZ_E_DATA = 10
 GPZ_E_PENDING = 9
 GPZ_E_BUSY = 8
 GPZ_FLAG_NO_GRAPHS = 1
@@ -33,6 +35,7 @@ EXPORTS = [
     "gpz_debug_chunk", "gpz_submit", "gpz_poll", "gpz_serve_stats_get", "gpz_strerror", "gpz_last_error",
     "gpz_get_shape", "gpz_set_shape", "gpz_last_launches", "gpz_stage_times", "gpz_compress_member_static",
     "gpz_serve_reset_stats", "gpz_submit_ref", "gpz_host_times", "gpz_serve_lane_stats",
+    "gpz_inflate_size", "gpz_inflate", "gpz_inflate_device_ms",
 ]
 
 
@@ -125,6 +128,12 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.gpz_serve_lane_stats.restype = ctypes.c_int
     L.gpz_host_times.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.c_int]
     L.gpz_host_times.restype = ctypes.c_int
+    L.gpz_inflate_size.argtypes = [vp, sz, ctypes.POINTER(sz), ctypes.POINTER(sz)]
+    L.gpz_inflate_size.restype = ctypes.c_int
+    L.gpz_inflate.argtypes = [vp, vp, sz, vp, sz, ctypes.POINTER(sz)]
+    L.gpz_inflate.restype = ctypes.c_int
+    L.gpz_inflate_device_ms.argtypes = [vp]
+    L.gpz_inflate_device_ms.restype = ctypes.c_float
     L.gpz_strerror.argtypes = [ctypes.c_int]
     L.gpz_strerror.restype = ctypes.c_char_p
     L.gpz_last_error.argtypes = [vp]
@@ -147,6 +156,19 @@ def _u8(data) -> np.ndarray:
     if isinstance(data, np.ndarray):
         return np.ascontiguousarray(data, dtype=np.uint8).reshape(-1)
     return np.frombuffer(bytes(data), dtype=np.uint8)
+
+
+def inflate_size(data):
+    """(members, output bytes) of a gzip stream written by gpzip, from its
+    headers and ISIZE trailers (host only).  Raises GpzError (GPZ_E_DATA)
+    when the stream does not start with gpzip's header."""
+    L = load()
+    a = _u8(data)
+    m, t = ctypes.c_size_t(), ctypes.c_size_t()
+    rc = L.gpz_inflate_size(_p(a), a.size, ctypes.byref(m), ctypes.byref(t))
+    if rc:
+        raise GpzError(rc, "gpz_inflate_size")
+    return m.value, t.value
 
 
 def _p(a: np.ndarray):
@@ -309,6 +331,24 @@ class Context:
             rc = self.L.gpz_poll(self._h, ticket, ctypes.byref(o), wait_ms)
         self._check(rc, "gpz_poll")
         return buf[:o.out_len].tobytes()
+
+    def inflate(self, data, out=None):
+        """Decompresses a gzip stream written by gpzip on the device (one warp
+        per member).  `out`: optional reusable uint8 array of at least the
+        output size; the result is a view into it.  Raises GpzError with
+        GPZ_E_DATA when the stream cannot be split or a member fails."""
+        a = _u8(data)
+        if out is None:
+            _, total = inflate_size(a)
+            out = np.empty(max(total, 1), dtype=np.uint8)
+        elif out.dtype != np.uint8 or not out.flags.c_contiguous:
+            raise ValueError("out must be a contiguous uint8 array")
+        n = ctypes.c_size_t()
+        self._check(self.L.gpz_inflate(self._h, _p(a), a.size, _p(out), out.size, ctypes.byref(n)), "gpz_inflate")
+        return memoryview(out)[:n.value]
+
+    def inflate_device_ms(self) -> float:
+        return float(self.L.gpz_inflate_device_ms(self._h))
 
     def host_times(self, reset: bool = False) -> dict:
         a = (ctypes.c_double * 6)()

@@ -47,6 +47,7 @@ extern "C" {
 #define GPZ_E_INTERNAL 7    /* device self-check failed (bit plan mismatch) */
 #define GPZ_E_BUSY 8        /* serving queue full, retry later */
 #define GPZ_E_PENDING 9     /* ticket not finished yet */
+#define GPZ_E_DATA 10       /* gzip input this path cannot split or decode (use a serial decoder) */
 
 typedef struct gpz_ctx gpz_ctx;
 
@@ -199,6 +200,32 @@ GPZ_API int gpz_set_shape(gpz_ctx* ctx, const gpz_shape* s);
 
 /* Number of kernel launches the last compress call issued. */
 GPZ_API uint64_t gpz_last_launches(gpz_ctx* ctx);
+
+/* ---- Decompression of gpzip-written archives (the `gpzip x` path) ----
+ *
+ * The GPU counterpart of parallel_decompress
+ * (crates/gpzip-codec-cpu/src/parallel_decompress.rs:63-113): the stream is
+ * cut into members at every occurrence of the fixed 10-byte header that
+ * gpzip writes (1f 8b 08 00 00 00 00 00 00 ff, parallel_decompress.rs:29-58),
+ * and every member is decoded on the device, one warp each, into its place
+ * in the output (offsets from the members' ISIZE trailers).
+ *
+ * gpz_inflate_size: host only, no context.  Scans in[0, n) and returns the
+ * member count and the total output size.  GPZ_E_DATA when the stream does
+ * not start with the header or a member is shorter than 18 bytes.
+ *
+ * gpz_inflate: *out_len receives the total output size; GPZ_E_SPACE when
+ * out_cap is smaller (out may then be NULL).  GPZ_E_DATA when the stream
+ * cannot be cut as above, or when any member fails to decode, does not end
+ * exactly at its trailer, or does not match its CRC-32 or ISIZE: the caller
+ * then decodes serially, as parallel_decompress falls back to
+ * MultiGzDecoder.  gpz_last_error names the member and the reason.  An
+ * empty input gives an empty output. */
+GPZ_API int gpz_inflate_size(const uint8_t* in, size_t n, size_t* members, size_t* out_bytes);
+GPZ_API int gpz_inflate(gpz_ctx* ctx, const uint8_t* in, size_t n, uint8_t* out, size_t out_cap,
+                        size_t* out_len);
+/* Device time of the last gpz_inflate's kernels (decode and CRC), in ms. */
+GPZ_API float gpz_inflate_device_ms(const gpz_ctx* ctx);
 
 /* Largest input gpz_compress_member_static accepts (one 128 KiB member). */
 #define GPZ_STATIC_MAX_BYTES 131072
