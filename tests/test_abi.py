@@ -92,6 +92,10 @@ def test_argument_checks_without_a_device(lib):
     assert lib.gpz_last_launches(None) == 0
     assert lib.gpz_last_error(None) == b"no context"
     lib.gpz_destroy(None)
+    assert lib.gpz_inflate(None, None, 0, None, 0, ctypes.byref(n)) == 5
+    assert lib.gpz_inflate_size(None, 10, None, ctypes.byref(n)) == 5
+    assert lib.gpz_inflate_size(None, 0, None, None) == 5
+    assert lib.gpz_inflate_device_ms(None) == 0.0
     # the allocation-free entry point checks its arguments before any CUDA call
     assert lib.gpz_compress_member_static(vp(16), 131073, vp(16), 1 << 20, ctypes.byref(n), None) == 5
     assert lib.gpz_compress_member_static(None, 10, vp(16), 1 << 20, ctypes.byref(n), None) == 5
