@@ -262,6 +262,34 @@ def inflate_rates(ctx, gz: bytes, want_len: int, steps: int = 5):
             "what": "gpz_inflate: page-locked host buffers, copies inside the timed region, wall clock"}
 
 
+def writer_rate(ctx, data, rounds: int = 3):
+    """The streaming writer (gpz_writer_*, ParallelChunkedWriter) as pack_tar
+    drives it: the workload written in 1 MiB pieces, cut into 2 MiB chunks,
+    16 in flight; input GB/s, best of `rounds` after one warm-up round."""
+    import time as _t
+    from gpzip_b200 import native
+
+    class Count:
+        n = 0
+
+        def write(self, b):
+            Count.n += len(b)
+
+    view = np.ascontiguousarray(data)
+    best = None
+    for r in range(rounds + 1):
+        Count.n = 0
+        t0 = _t.perf_counter()
+        with native.Writer(Count(), ctx=ctx, chunk_size=2 << 20, max_in_flight=16) as w:
+            for i in range(0, len(view), 1 << 20):
+                w.write(view[i:i + (1 << 20)])
+        t = _t.perf_counter() - t0
+        if r:
+            best = t if best is None else min(best, t)
+    return {"value": round(len(view) / best / 1e9, 4), "unit": "GB/s", "out_bytes": Count.n,
+            "what": "gpz_writer: 1 MiB writes, 2 MiB chunks, 16 in flight, wall clock"}
+
+
 def chunk_fn_rate(ctx, chunks, threads: int = 16, rounds: int = 3):
     """The ChunkFn drop-in as ParallelChunkedWriter drives it: `threads`
     workers (max_in_flight for the gpu backend, gpu.rs:160-166) each call
@@ -567,6 +595,7 @@ def main():
     e2e_value = data.size * len(e_times) * world / (float(et.item()) / 1e3) / 1e9
     e2e_host = {k: round(v / max(1, len(e_times)), 3) for k, v in ectx.host_times().items()}
     inflate = None
+    writer = None if args.device_only else writer_rate(ectx, data)
     if not args.device_only:
         gz_all = b"".join(bytes(x) for x in outs)
         inflate = inflate_rates(ectx, gz_all, data.size)
@@ -631,6 +660,7 @@ def main():
                     "host_ms_per_step": e2e_host},
             "chunk_fn": chunk_fn,
             "inflate": inflate,
+            "writer": writer,
             "gpu_launches": int(launches),
             "clocks": clk,
             "ratio": round(ratio, 5),

@@ -1838,6 +1838,7 @@ const char* gpz_strerror(int s) {
         case GPZ_E_BUSY: return "serving queue full";
         case GPZ_E_PENDING: return "result not ready";
         case GPZ_E_DATA: return "gzip data this path cannot split or decode";
+        case GPZ_E_SINK: return "the writer's sink or chunk function failed";
         default: return "unknown status";
     }
 }

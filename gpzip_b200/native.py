@@ -16,8 +16,13 @@ LIB_PATH = os.path.join(HERE, "libgpz.so")
 GPZ_OK = 0
 STATUS = {0: "GPZ_OK", 1: "GPZ_E_NOMEM", 2: "GPZ_E_ADMISSION", 3: "GPZ_E_TIMEOUT", 4: "GPZ_E_CUDA",
           5: "GPZ_E_ARG", 6: "GPZ_E_SPACE", 7: "GPZ_E_INTERNAL", 8: "GPZ_E_BUSY", 9: "GPZ_E_PENDING",
-          10: "GPZ_E_DATA"}
+          10: "GPZ_E_DATA", 11: "GPZ_E_SINK"}
 GPZ_E_DATA = 10
+GPZ_E_SINK = 11
+# gpz_sink_fn / gpz_chunk_fn
+SINK_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint8), ctypes.c_size_t)
+CHUNK_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint8), ctypes.c_size_t,
+                            ctypes.POINTER(ctypes.c_uint8), ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t))
 GPZ_E_PENDING = 9
 GPZ_E_BUSY = 8
 GPZ_FLAG_NO_GRAPHS = 1
@@ -36,6 +41,8 @@ EXPORTS = [
     "gpz_get_shape", "gpz_set_shape", "gpz_last_launches", "gpz_stage_times", "gpz_compress_member_static",
     "gpz_serve_reset_stats", "gpz_submit_ref", "gpz_host_times", "gpz_serve_lane_stats",
     "gpz_inflate_size", "gpz_inflate", "gpz_inflate_device_ms",
+    "gpz_writer_open", "gpz_writer_open_fn", "gpz_writer_write", "gpz_writer_flush", "gpz_writer_finish",
+    "gpz_writer_close",
 ]
 
 
@@ -134,6 +141,17 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.gpz_inflate.restype = ctypes.c_int
     L.gpz_inflate_device_ms.argtypes = [vp]
     L.gpz_inflate_device_ms.restype = ctypes.c_float
+    L.gpz_writer_open.argtypes = [vp, sz, sz, SINK_FN, vp, ctypes.POINTER(vp)]
+    L.gpz_writer_open.restype = ctypes.c_int
+    L.gpz_writer_open_fn.argtypes = [CHUNK_FN, vp, sz, sz, SINK_FN, vp, ctypes.POINTER(vp)]
+    L.gpz_writer_open_fn.restype = ctypes.c_int
+    L.gpz_writer_write.argtypes = [vp, vp, sz]
+    L.gpz_writer_write.restype = ctypes.c_int
+    for f in (L.gpz_writer_flush, L.gpz_writer_finish):
+        f.argtypes = [vp]
+        f.restype = ctypes.c_int
+    L.gpz_writer_close.argtypes = [vp]
+    L.gpz_writer_close.restype = None
     L.gpz_strerror.argtypes = [ctypes.c_int]
     L.gpz_strerror.restype = ctypes.c_char_p
     L.gpz_last_error.argtypes = [vp]
@@ -373,3 +391,78 @@ class Context:
         s = ServeStats()
         self._check(self.L.gpz_serve_stats_get(self._h, ctypes.byref(s)), "gpz_serve_stats_get")
         return {f: getattr(s, f) for f, _ in ServeStats._fields_}
+
+
+class Writer:
+    """ParallelChunkedWriter over the library (gpz_writer_*): a file-like
+    object whose bytes are cut into `chunk_size` chunks, compressed `max_in_flight`
+    at a time on the writer's thread, and written as gzip members, in order,
+    to `dst` (anything with a write method).  With `ctx` the chunks go
+    through the device; with `chunk_fn` (bytes -> gzip bytes) through that
+    function instead, as the reference's writer takes any ChunkFn.
+    flush() does not cut a chunk; close() writes the last partial chunk and
+    raises the first error the writer met."""
+
+    def __init__(self, dst, ctx: "Context" = None, chunk_fn=None, chunk_size: int = 2 << 20, max_in_flight: int = 16):
+        self.L = load()
+        self._dst = dst
+        self._err = None
+        self._chunk_fn = chunk_fn
+
+        def sink(_user, buf, n):
+            try:
+                self._dst.write(ctypes.string_at(buf, n))
+                return 0
+            except Exception as e:  # noqa: BLE001 -- reported by close()
+                self._err = self._err or e
+                return 1
+
+        def chunk(_user, buf, n, out, cap, out_len):
+            try:
+                g = bytes(self._chunk_fn(ctypes.string_at(buf, n)))
+                if len(g) > cap:
+                    return 1
+                ctypes.memmove(out, g, len(g))
+                out_len[0] = len(g)
+                return 0
+            except Exception as e:  # noqa: BLE001 -- reported by close()
+                self._err = self._err or e
+                return 1
+
+        self._sink = SINK_FN(sink)  # kept alive with the writer
+        self._chunk = CHUNK_FN(chunk)
+        h = ctypes.c_void_p()
+        if ctx is not None:
+            rc = self.L.gpz_writer_open(ctx._h, chunk_size, max_in_flight, self._sink, None, ctypes.byref(h))
+        else:
+            rc = self.L.gpz_writer_open_fn(self._chunk, None, chunk_size, max_in_flight, self._sink, None,
+                                           ctypes.byref(h))
+        if rc:
+            raise GpzError(rc, "gpz_writer_open")
+        self._h = h
+
+    def _check(self, rc, what):
+        if rc:
+            raise GpzError(rc, f"{what}: {self._err!r}" if self._err else what)
+
+    def write(self, data) -> int:
+        a = _u8(data)
+        self._check(self.L.gpz_writer_write(self._h, _p(a), a.size), "gpz_writer_write")
+        return a.size
+
+    def flush(self):
+        self._check(self.L.gpz_writer_flush(self._h), "gpz_writer_flush")
+
+    def close(self):
+        if self._h:
+            rc = self.L.gpz_writer_finish(self._h)
+            self.L.gpz_writer_close(self._h)
+            self._h = None
+            self._check(rc, "gpz_writer_finish")
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+

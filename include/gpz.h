@@ -48,6 +48,7 @@ extern "C" {
 #define GPZ_E_BUSY 8        /* serving queue full, retry later */
 #define GPZ_E_PENDING 9     /* ticket not finished yet */
 #define GPZ_E_DATA 10       /* gzip input this path cannot split or decode (use a serial decoder) */
+#define GPZ_E_SINK 11       /* a writer's sink or chunk function reported an error */
 
 typedef struct gpz_ctx gpz_ctx;
 
@@ -258,11 +259,48 @@ GPZ_API int gpz_compress_member_static(const uint8_t* d_in, size_t n, uint8_t* d
 GPZ_API int gpz_host_times(gpz_ctx* ctx, double* ms6, int reset);
 
 /* Device time of each stage of the last device pass, in ms, GPZ_STAGES
- * values: segment summaries (k_segtab), lookup (k_lookup), walk (k_walk_exit,
- * k_chain, k_walk_mark), Huffman plan and placement (k_huff, k_place,
- * k_frame), emit (k_emit).  Needs GPZ_FLAG_STAGE_TIMING at gpz_create. */
+ * values: segment summaries (k_segtab), lookup (k_lookup), walk (k_walk_exit
+ * with the member chaining in its last CTA, k_walk_mark), Huffman plan and
+ * placement (k_huff with the placement in its last CTA, k_frame), emit
+ * (k_emit).  Needs GPZ_FLAG_STAGE_TIMING at gpz_create. */
 #define GPZ_STAGES 5
 GPZ_API int gpz_stage_times(gpz_ctx* ctx, float* ms);
+
+/* ---- Streaming chunked writer (ParallelChunkedWriter) ----
+ *
+ * The caller of ChunkFn in the reference, ParallelChunkedWriter
+ * (crates/gpzip-codec-cpu/src/parallel.rs:28-229), which pack_tar wraps
+ * around the archive file (crates/gpzip-core/src/archive/pack.rs:144-176):
+ * bytes written are cut into chunk_size chunks, the chunks are compressed
+ * into independent gzip members, and the members reach `sink` in input
+ * order.  Up to max_in_flight chunks are compressed together as one batch
+ * on an internal thread while the caller fills the next batch.
+ *
+ *  - sink(user, buf, n) returns 0 on success; it is called from the
+ *    internal thread, never concurrently, and with members in order.
+ *  - gpz_writer_flush does not cut the current partial chunk (tar calls
+ *    flush between entries; parallel.rs:207-213) and waits for nothing.
+ *  - gpz_writer_finish compresses the partial chunk, waits for every batch
+ *    and returns the first error of the writer's life; errors are sticky,
+ *    as in the reference (parallel.rs:70-89).  It may be called again.
+ *  - gpz_writer_close finishes (if not yet) and frees the writer.
+ *
+ * gpz_writer_open compresses with ctx (gpz_compress_batch).
+ * gpz_writer_open_fn compresses each chunk with fn(fn_user, in, n, out,
+ * out_cap, &out_len) instead (out_cap = gpz_bound(n); nonzero return is an
+ * error): a caller-supplied ChunkFn, as the reference's writer takes any. */
+typedef struct gpz_writer gpz_writer;
+typedef int (*gpz_sink_fn)(void* user, const uint8_t* buf, size_t n);
+typedef int (*gpz_chunk_fn)(void* user, const uint8_t* in, size_t n, uint8_t* out, size_t out_cap,
+                            size_t* out_len);
+GPZ_API int gpz_writer_open(gpz_ctx* ctx, size_t chunk_size, size_t max_in_flight, gpz_sink_fn sink,
+                            void* sink_user, gpz_writer** out);
+GPZ_API int gpz_writer_open_fn(gpz_chunk_fn fn, void* fn_user, size_t chunk_size, size_t max_in_flight,
+                               gpz_sink_fn sink, void* sink_user, gpz_writer** out);
+GPZ_API int gpz_writer_write(gpz_writer* w, const uint8_t* buf, size_t n);
+GPZ_API int gpz_writer_flush(gpz_writer* w);
+GPZ_API int gpz_writer_finish(gpz_writer* w);
+GPZ_API void gpz_writer_close(gpz_writer* w);
 
 #ifdef __cplusplus
 }

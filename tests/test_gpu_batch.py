@@ -214,3 +214,17 @@ def test_fixed_block_mode():
             assert gzip.decompress(got) == it
         for it, g in zip(items, c.compress_batch(items)):
             assert g == O.gzip_chunk_fixed(it, 131072)
+
+
+def test_device_writer_matches_the_oracle(ctx):
+    # the streaming writer over the device path: 2 MiB chunks, 16 in flight,
+    # members in order; bytes equal the oracle's per-chunk gzip streams
+    import io
+    data = W.logs((9 << 20) + 4321, seed=30).tobytes()
+    out = io.BytesIO()
+    with native.Writer(out, ctx=ctx, chunk_size=2 << 20, max_in_flight=3) as w:
+        for i in range(0, len(data), 700_000):
+            w.write(data[i:i + 700_000])
+    want = b"".join(O.gzip_chunk(data[i:i + (2 << 20)], 131072, threads=8) for i in range(0, len(data), 2 << 20))
+    assert out.getvalue() == want
+    assert bytes(ctx.inflate(out.getvalue())) == data
