@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <condition_variable>
 #include <deque>
+#include <memory>
 #include <mutex>
 #include <new>
 #include <thread>
@@ -22,6 +23,64 @@
 
 using Chunk = std::vector<uint8_t>;
 using Batch = std::vector<Chunk>;
+
+namespace {
+
+// Chunk buffers outlive their writer here, so that a new writer does not
+// page-fault its way through fresh memory (a 64 MiB stream would otherwise
+// take 16 K page faults).  Bounded: at most kPoolChunks buffers are kept.
+constexpr size_t kPoolChunks = 64;
+std::mutex g_pool_mu;
+std::vector<Chunk> g_pool;
+
+bool pool_take(size_t chunk_size, Chunk& into) {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    for (size_t i = g_pool.size(); i-- > 0;)
+        if (g_pool[i].capacity() == chunk_size) {
+            into = std::move(g_pool[i]);
+            g_pool.erase(g_pool.begin() + (std::ptrdiff_t)i);
+            return true;
+        }
+    return false;
+}
+
+// Output buffers, kept across writers for the same reason: the first
+// touch of a fresh 64 MiB buffer (page faults, huge-page compaction) cost a
+// writer's first batch 50-260 ms instead of 4 ms.
+constexpr size_t kPoolOuts = 4;
+std::vector<std::pair<std::unique_ptr<uint8_t[]>, size_t>> g_outs;
+
+std::pair<std::unique_ptr<uint8_t[]>, size_t> out_take(size_t cap) {
+    {
+        std::lock_guard<std::mutex> lk(g_pool_mu);
+        for (size_t i = 0; i < g_outs.size(); i++)
+            if (g_outs[i].second >= cap) {
+                auto o = std::move(g_outs[i]);
+                g_outs.erase(g_outs.begin() + (std::ptrdiff_t)i);
+                return o;
+            }
+    }
+    return {std::unique_ptr<uint8_t[]>(new (std::nothrow) uint8_t[cap]), cap};
+}
+
+void out_give(std::unique_ptr<uint8_t[]>& p, size_t cap) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (g_outs.size() < kPoolOuts) g_outs.emplace_back(std::move(p), cap);
+    p.reset();
+}
+
+void pool_give(std::vector<Chunk>& chunks) {
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    for (Chunk& ch : chunks)
+        if (g_pool.size() < kPoolChunks && ch.capacity()) {
+            ch.clear();
+            g_pool.push_back(std::move(ch));
+        }
+    chunks.clear();
+}
+
+}  // namespace
 
 struct gpz_writer {
     gpz_ctx* ctx = nullptr;
@@ -41,18 +100,25 @@ struct gpz_writer {
     bool stop = false;
     int sticky = GPZ_OK;
     std::thread worker;
-    std::vector<uint8_t> out;  // the thread's output buffer, reused
+    std::unique_ptr<uint8_t[]> out;  // the thread's output buffer, from and back to the pool
+    size_t out_cap = 0;
     std::vector<Chunk> spare;  // chunk buffers of finished batches, reused (no page faults)
 
     int compress(Batch& b) {
         size_t cap = 0;
         for (const Chunk& ch : b) cap += ctx ? gpz_bound_ctx(ctx, ch.size()) : gpz_bound(ch.size());
-        if (out.size() < cap) out.resize(cap);
+        if (out_cap < cap) {
+            out_give(out, out_cap);
+            auto o = out_take(cap);
+            out = std::move(o.first);
+            out_cap = out ? o.second : 0;
+            if (!out) return GPZ_E_NOMEM;
+        }
         std::vector<gpz_out> outs(b.size());
         size_t off = 0;
         for (size_t i = 0; i < b.size(); i++) {
             const size_t c = ctx ? gpz_bound_ctx(ctx, b[i].size()) : gpz_bound(b[i].size());
-            outs[i] = gpz_out{out.data() + off, c, 0, 0};
+            outs[i] = gpz_out{out.get() + off, c, 0, 0};
             off += c;
         }
         if (ctx) {
@@ -127,6 +193,7 @@ struct gpz_writer {
                 return;
             }
         }
+        if (pool_take(chunk_size, current)) return;
         current = Chunk{};
         current.reserve(chunk_size);
     }
@@ -219,5 +286,7 @@ void gpz_writer_close(gpz_writer* w) {
     }
     w->cv.notify_all();
     w->worker.join();
+    pool_give(w->spare);
+    out_give(w->out, w->out_cap);
     delete w;
 }
