@@ -120,9 +120,13 @@ class CopyPool {
         size_t n;
     };
 
+    // Half the host's cores (at most 8 copiers with the caller): the copies
+    // are memory-bound, and the other half stays free for the application.
+    // With every core taken, a copier that the scheduler preempted held up
+    // its whole batch of pieces while the application kept running.
     CopyPool() {
         const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-        const unsigned nw = std::min(hw, 16u) - 1;
+        const unsigned nw = std::max(1u, std::min(hw / 2, 8u)) - 1;
         for (unsigned i = 0; i < nw; i++) th_.emplace_back([this] { work(); });
     }
     ~CopyPool() {
