@@ -284,6 +284,8 @@ GPZ_API int gpz_stage_times(gpz_ctx* ctx, float* ms);
  *    and returns the first error of the writer's life; errors are sticky,
  *    as in the reference (parallel.rs:70-89).  It may be called again.
  *  - gpz_writer_close finishes (if not yet) and frees the writer.
+ *  - One writer is driven by one caller thread at a time (like the
+ *    reference's &mut self methods); separate writers are independent.
  *
  * gpz_writer_open compresses with ctx (gpz_compress_batch).
  * gpz_writer_open_fn compresses each chunk with fn(fn_user, in, n, out,
