@@ -19,6 +19,10 @@
 
 #include <stdint.h>
 
+#if defined(GPZI_HOST_LANES)
+#include <barrier>
+#endif
+
 #if defined(__CUDACC__)
 #define GPZI_FN __host__ __device__ __forceinline__
 #else
@@ -71,9 +75,17 @@ struct Shared {
     uint32_t bcast;  // a value lane 0 computed, for every lane
 };
 
+#if defined(GPZI_HOST_LANES)
+// Host test build with NL host threads standing in for the lanes of a warp
+// (tests/c/inflate_lanes.cpp): lane_sync is a barrier across them.
+inline std::barrier<>* g_lanes = nullptr;
+#endif
+
 GPZI_FN void lane_sync() {
 #if defined(__CUDA_ARCH__)
     __syncwarp();
+#elif defined(GPZI_HOST_LANES)
+    g_lanes->arrive_and_wait();
 #endif
 }
 

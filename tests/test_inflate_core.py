@@ -179,3 +179,46 @@ def test_member_split_and_sizes_on_the_host():
     forged[-4:] = struct.pack("<I", 1 << 30)
     with pytest.raises(native.GpzError):
         native.inflate_size(bytes(forged))
+
+
+@pytest.fixture(scope="module")
+def lanes_decoder(tmp_path_factory):
+    cxx = shutil.which("g++")
+    if not cxx:
+        pytest.skip("no C++ compiler")
+    exe = str(tmp_path_factory.mktemp("infl32") / "inflate_lanes")
+    src = [os.path.join(ROOT, "tests", "c", "inflate_lanes.cpp"), "-I", os.path.join(ROOT, "gpzip_b200", "csrc")]
+    r = subprocess.run([cxx, "-O2", "-std=c++20", "-pthread", "-Wall", "-Wextra", "-Werror", *src, "-o", exe],
+                       capture_output=True, text=True)
+    if r.returncode != 0 and "barrier" in r.stderr:
+        pytest.skip("no std::barrier")
+    assert r.returncode == 0, r.stderr
+    return exe
+
+
+def test_32_lane_build_matches_zlib(lanes_decoder, tmp_path):
+    # the device build's lane-cooperative paths (NL = 32) on 32 host threads:
+    # strided staging and table fills, copies with distances below 32 (the
+    # modulo path the one-lane build never takes), flushes; every lane must
+    # return the same status
+    from oracle import oracle as O
+    rng = np.random.default_rng(21)
+    runs = b"ab" * 3000 + b"\0" * 5000 + bytes(rng.integers(0, 4, 3000, dtype=np.uint8)) + b"xyz" * 2000
+    cases, want = [], []
+    for data in (runs, W.text(40_000, seed=22).tobytes(), W.binary(50_000, seed=23).tobytes(), b"", b"q"):
+        for level, strat in ((0, 0), (1, zlib.Z_DEFAULT_STRATEGY), (9, zlib.Z_RLE), (6, zlib.Z_FIXED)):
+            cases.append((raw_deflate(data, level, strat), len(data)))
+            want.append(data)
+    data = W.logs(131_072, seed=24).tobytes()
+    member = O.gzip_chunk(data, 131072)
+    cases.append((member[10:-8], len(data)))
+    want.append(data)
+    d = raw_deflate(runs, 6)
+    cases += [(d[:len(d) // 2], len(runs)), (d, len(runs) - 5)]
+    want += [None, None]
+    got = run(lanes_decoder, tmp_path, cases)
+    for (st, out), w in zip(got, want):
+        if w is None:
+            assert st != 0
+        else:
+            assert st == 0 and out == w
