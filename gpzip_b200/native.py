@@ -404,10 +404,13 @@ class Writer:
     raises the first error the writer met."""
 
     def __init__(self, dst, ctx: "Context" = None, chunk_fn=None, chunk_size: int = 2 << 20, max_in_flight: int = 16):
+        if (ctx is None) == (chunk_fn is None):
+            raise ValueError("give exactly one of ctx and chunk_fn")
         self.L = load()
         self._dst = dst
         self._err = None
         self._chunk_fn = chunk_fn
+        self._h = None
 
         def sink(_user, buf, n):
             try:

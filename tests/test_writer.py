@@ -88,6 +88,8 @@ def test_errors_are_sticky():
 
 
 def test_bad_arguments():
+    with pytest.raises(ValueError):
+        native.Writer(io.BytesIO())
     with pytest.raises(native.GpzError):
         native.Writer(io.BytesIO(), chunk_fn=oracle_fn, chunk_size=0)
     with pytest.raises(native.GpzError):
