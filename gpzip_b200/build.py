@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgpz.so")
-SOURCES = ["gpz_kernels.cu", "gpz_runtime.cu", "gpz_serve.cu", "gpz_static.cu", "gpz_inflate.cu", "gpz_writer.cu"]
+SOURCES = ["gpz_kernels.cu", "gpz_runtime.cu", "gpz_static.cu", "gpz_inflate.cu", "gpz_writer.cu"]
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -44,7 +44,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
     tmp = LIB + ".tmp"
     cmd = [nvcc(), *GENCODE, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
            "-Xcompiler", "-fvisibility=hidden", "-I", os.path.join(ROOT, "include"), "-o", tmp, *sources(),
-           "-lpthread"]
+           "-lpthread", "-lz"]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
     r = subprocess.run(cmd, capture_output=True, text=True)

@@ -21,7 +21,6 @@
 #define GPZ_HDR_WORDS 144                   // dynamic block header <= 4498 bits, + slack
 
 // Error bits reported through BatchParams::err.
-#define GPZ_ERRBIT_SPIN 1u      // a bounded wait expired
 #define GPZ_ERRBIT_BITS 2u      // emitted bit count disagreed with the plan
 #define GPZ_ERRBIT_HUFF 4u      // code construction failed (never expected)
 #define GPZ_ERRBIT_DESC 8u      // a fetched descriptor block exceeded the arenas
@@ -59,9 +58,8 @@ struct BatchParams {
     const MemberDesc* members;
     const TileDesc* tiles;
     uint32_t* pp;             // per-position packed tokens, indexed like `in`
-    uint16_t* seg_keys;       // [tile][4096] distinct hashes of the segment, ascending
+    uint16_t* seg_keys;       // [tile][4096] distinct hashes of the segment, ascending (id = rank)
     uint32_t* seg_on;         // [tile][4096] newest offset | oldest offset << 16, per distinct hash
-    uint16_t* seg_posid;      // [tile][4096] rank of each position's hash (0xFFFF: none)
     uint32_t* seg_nkeys;      // [tile] distinct hashes in the segment
     uint32_t* tok;            // walked tokens, tile-sparse, indexed like `in`
     uint32_t* out_words;      // gzip stream of the batch, as 32-bit words

@@ -129,22 +129,18 @@ __device__ __forceinline__ Head load_head(const uint32_t* w, uint32_t b) {
                 __funnelshift_r(b3, b4, sb)};
 }
 
-// try_candidate (lz77_hash_lookup.wgsl:99-121) on packed best = len<<16|dist.
-// A candidate that cannot beat the current best is dropped early: it must
+// try_candidate (lz77_hash_lookup.wgsl:45-67) on packed best = len<<16|dist,
+// for a candidate already known to be valid: it lies before p and at most
+// 32768 bytes back (the caller checks what its segment does not imply).
+// `a` and `b` are the window offsets of the candidate and of p.  A
+// candidate that cannot beat the current best is dropped early: it must
 // agree with p at offset best_len, and best_len must be below the cap.  The
 // first 16 bytes are compared with p's Head; only a candidate that agrees on
 // all of them continues in match_len.
-__device__ __forceinline__ void try_cand(const uint8_t* win, const uint32_t* w32, const Head& hp, uint32_t raw,
-                                         uint32_t p, uint32_t n, uint32_t w0, uint32_t& best) {
-    if (raw == 0u || raw == kEmpty) return;
-    const uint32_t cand = raw - 1u;
-    if (cand >= p) return;
-    const uint32_t dist = p - cand;
-    if (dist > GPZ_WINDOW) return;
-    const uint32_t limit = min(GPZ_MAX_MATCH, n - p);
+__device__ __forceinline__ void try_win(const uint8_t* win, const uint32_t* w32, const Head& hp, uint32_t a,
+                                        uint32_t b, uint32_t dist, uint32_t limit, uint32_t& best) {
     const uint32_t bl = best >> 16;
     if (bl >= limit) return;
-    const uint32_t a = cand - w0, b = p - w0;
     if (bl >= 3u && win[a + bl] != win[b + bl]) return;
     const uint32_t sa = (a & 3u) * 8u, ia = a >> 2;
     const uint32_t a0 = w32[ia], a1 = w32[ia + 1], a2 = w32[ia + 2], a3 = w32[ia + 3], a4 = w32[ia + 4];
@@ -195,23 +191,42 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* warp_s
 
 // The reference's dense seg_oldest / seg_newest tables (65536 x num_segs,
 // lz77_hash_build.wgsl:45-54) are never materialised.  Instead every 4 KiB
-// segment is summarised once: its distinct hashes, each with its oldest and
-// newest offset -- exactly the two values the reference's atomicMin /
-// atomicMax leave in table[h][seg] -- and, for every position, the dense id
-// of its hash.  Built in shared memory with an open-addressed table.
-// Positions with p + 2 >= n have no hash, as in the reference build.
-constexpr int kSlots = 8192;
-constexpr size_t kSegtabSmem = 3 * kSlots * 4;
+// segment is summarised once: its distinct hashes in ascending order, each
+// with its oldest and newest offset -- exactly the two values the
+// reference's atomicMin / atomicMax leave in table[h][seg].  A hash's index
+// in that order (its id) is its rank in the segment's set of hashes.  The
+// set is a 65536-bit bitmap in shared memory, and the rank is the number of
+// set bits before it: a prefix count per 32-bit word plus a popcount inside
+// the word.  k_lookup rebuilds the same bitmap from the keys, so both
+// kernels give a hash the same id without probing a table.  Positions with
+// p + 2 >= n have no hash, as in the reference build.
+constexpr int kBmWords = 65536 / 32;
 
-__device__ __forceinline__ uint32_t slot_of(uint32_t h) { return (h * 0x85EBCA6Bu) >> 19; }
+struct SegtabSmem {
+    static constexpr size_t kBitmap = 0;                       // u32[2048] the segment's hash set
+    static constexpr size_t kPrefix = kBitmap + kBmWords * 4;  // u32[2048] set bits before each word
+    static constexpr size_t kOld = kPrefix + kBmWords * 4;     // u32[4096] oldest offset per id
+    static constexpr size_t kNew = kOld + GPZ_SEG * 4;         // u32[4096] newest offset per id
+    static constexpr size_t kKey = kNew + GPZ_SEG * 4;         // u16[4096] hash of each id
+    static constexpr size_t kBytes = kKey + GPZ_SEG * 2;
+};
+
+// hash3 of the bytes s[0..2] (lz77_hash_build.wgsl:36-43)
+__device__ __forceinline__ uint32_t hash3_at(const uint8_t* s) {
+    const uint32_t x = ((uint32_t)s[0] << 16) | ((uint32_t)s[1] << 8) | (uint32_t)s[2];
+    return (x * 0x9E3779B1u) >> 16;
+}
 
 template <int T>
-__global__ void __launch_bounds__(T, 2) k_segtab(BatchParams bp) {
+__global__ void __launch_bounds__(T, 3) k_segtab(BatchParams bp) {
     constexpr int PER = GPZ_SEG / T;
+    constexpr int WPT = kBmWords / T;
     extern __shared__ __align__(16) uint8_t smem[];
-    uint32_t* keyt = reinterpret_cast<uint32_t*>(smem);
-    uint32_t* oldt = keyt + kSlots;
-    uint32_t* newt = oldt + kSlots;
+    uint32_t* bm = reinterpret_cast<uint32_t*>(smem + SegtabSmem::kBitmap);
+    uint32_t* pre = reinterpret_cast<uint32_t*>(smem + SegtabSmem::kPrefix);
+    uint32_t* oldt = reinterpret_cast<uint32_t*>(smem + SegtabSmem::kOld);
+    uint32_t* newt = reinterpret_cast<uint32_t*>(smem + SegtabSmem::kNew);
+    uint16_t* keyof = reinterpret_cast<uint16_t*>(smem + SegtabSmem::kKey);
     __shared__ uint32_t wsum[32];
     __shared__ uint32_t s_tile;
     const int tid = threadIdx.x, lane = tid & 31;
@@ -227,85 +242,62 @@ __global__ void __launch_bounds__(T, 2) k_segtab(BatchParams bp) {
         const uint32_t n = md.len, start = td.seg << GPZ_SEG_LOG2;
         const uint32_t cnt = min(GPZ_SEG, n - start);
         const uint8_t* src = bp.in + md.in_off + start;
-        for (int i = tid; i < kSlots; i += T) {
-            keyt[i] = kEmpty;
+        for (int i = tid; i < kBmWords; i += T) bm[i] = 0u;
+        for (int i = tid; i < (int)GPZ_SEG; i += T) {
             oldt[i] = kEmpty;
             newt[i] = 0u;
         }
         __syncthreads();
-        uint32_t slot[PER];
+        // the segment's hash set; lanes of a warp hold consecutive positions
+        uint32_t hv[PER];
 #pragma unroll
         for (int k = 0; k < PER; k++) {
-            const uint32_t i = tid + k * T;
-            slot[k] = kEmpty;
+            const uint32_t i = (uint32_t)(k * T + tid);
+            hv[k] = kEmpty;
             if (i < cnt && start + i + 2u < n) {
-                const uint32_t x = ((uint32_t)src[i] << 16) | ((uint32_t)src[i + 1] << 8) | (uint32_t)src[i + 2];
-                const uint32_t h = (x * 0x9E3779B1u) >> 16;  // hash3, lz77_hash_build.wgsl:36-43
-                uint32_t sl = slot_of(h);
-                for (int probe = 0; probe < kSlots; probe++) {
-                    const uint32_t old = atomicCAS(&keyt[sl], kEmpty, h);
-                    if (old == kEmpty || old == h) break;
-                    sl = (sl + 1u) & (kSlots - 1);
-                }
-                slot[k] = sl;
-            }
-            // lanes of a warp hold consecutive positions: one atomic per run
-            // of equal slots for the oldest (its first lane), one for the
-            // newest (its last lane)
-            const uint32_t prev = __shfl_up_sync(0xFFFFFFFFu, slot[k], 1);
-            const uint32_t next = __shfl_down_sync(0xFFFFFFFFu, slot[k], 1);
-            if (slot[k] != kEmpty) {
-                if (lane == 0 || prev != slot[k]) atomicMin(&oldt[slot[k]], i);
-                if (lane == 31 || next != slot[k]) atomicMax(&newt[slot[k]], i);
+                hv[k] = hash3_at(src + i);
+                atomicOr(&bm[hv[k] >> 5], 1u << (hv[k] & 31u));
             }
         }
         __syncthreads();
-        // dense ids of the occupied slots, in slot order: warp w owns slots
-        // [w * SW, (w + 1) * SW), read 32 at a time; ballots give each
-        // occupied slot its rank, a scan over the warps' counts the base
-        constexpr int NWARP = T / 32, SW = kSlots / NWARP, KW = SW / 32;
-        const int warp = tid >> 5;
-        const uint32_t lt = (1u << lane) - 1u;
-        uint32_t kv[KW];
-        uint32_t wcount = 0;
+        // exclusive prefix count of set bits over the bitmap words
+        uint32_t c[WPT], sum = 0, nkeys = 0;
 #pragma unroll
-        for (int k = 0; k < KW; k++) {
-            kv[k] = keyt[warp * SW + k * 32 + lane];
-            wcount += __popc(__ballot_sync(0xFFFFFFFFu, kv[k] != kEmpty));
+        for (int j = 0; j < WPT; j++) {
+            c[j] = __popc(bm[tid * WPT + j]);
+            sum += c[j];
         }
-        if (lane == 0) wsum[warp] = wcount;
+        uint32_t run = block_excl_scan<T>(sum, wsum, &nkeys);
+#pragma unroll
+        for (int j = 0; j < WPT; j++) {
+            pre[tid * WPT + j] = run;
+            run += c[j];
+        }
         __syncthreads();
-        uint32_t wbase = 0, nkeys = 0;
-        {
-            const uint32_t c = lane < NWARP ? wsum[lane] : 0u;
-            uint32_t x = c;
+        // oldest / newest per id: one atomic per run of equal ids in a warp,
+        // its first lane for the oldest and its last lane for the newest
 #pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
-                if (lane >= o) x += y;
+        for (int k = 0; k < PER; k++) {
+            const uint32_t i = (uint32_t)(k * T + tid), h = hv[k];
+            uint32_t id = kEmpty;
+            if (h != kEmpty) {
+                const uint32_t w = h >> 5;
+                id = pre[w] + __popc(bm[w] & ((1u << (h & 31u)) - 1u));
+                keyof[id] = (uint16_t)h;
             }
-            wbase = __shfl_sync(0xFFFFFFFFu, x - c, warp);
-            nkeys = __shfl_sync(0xFFFFFFFFu, x, NWARP - 1);
+            const uint32_t prev = __shfl_up_sync(0xFFFFFFFFu, id, 1);
+            const uint32_t next = __shfl_down_sync(0xFFFFFFFFu, id, 1);
+            if (id != kEmpty) {
+                if (lane == 0 || prev != id) atomicMin(&oldt[id], i);
+                if (lane == 31 || next != id) atomicMax(&newt[id], i);
+            }
         }
+        __syncthreads();
         uint16_t* keys = bp.seg_keys + (size_t)t * GPZ_SEG;
         uint32_t* on = bp.seg_on + (size_t)t * GPZ_SEG;
-#pragma unroll
-        for (int k = 0; k < KW; k++) {
-            const uint32_t m = __ballot_sync(0xFFFFFFFFu, kv[k] != kEmpty);
-            if (kv[k] != kEmpty) {
-                const uint32_t sl = warp * SW + k * 32 + lane, id = wbase + __popc(m & lt);
-                keys[id] = (uint16_t)kv[k];
-                on[id] = newt[sl] | (oldt[sl] << 16);
-                oldt[sl] = id;  // slot -> id from here on
-            }
-            wbase += __popc(m);
-        }
-        __syncthreads();
-        uint16_t* pos_id = bp.seg_posid + (size_t)t * GPZ_SEG;
-#pragma unroll
-        for (int k = 0; k < PER; k++) {
-            const uint32_t i = tid + k * T;
-            if (i < cnt) pos_id[i] = slot[k] == kEmpty ? (uint16_t)0xFFFFu : (uint16_t)oldt[slot[k]];
+        for (uint32_t id = tid; id < nkeys; id += T) {
+            keys[id] = keyof[id];
+            on[id] = newt[id] | (oldt[id] << 16);
         }
         if (tid == 0) bp.seg_nkeys[t] = nkeys;
     }
@@ -313,76 +305,51 @@ __global__ void __launch_bounds__(T, 2) k_segtab(BatchParams bp) {
 
 // ================================================================ k_lookup
 
+// Candidate rows: [id][bpp] entries newest | oldest << 16, one per back
+// segment of the current pass (kEmpty: the hash does not occur there).  A
+// tile with at most 1280 distinct hashes joins all 8 back segments in one
+// pass, up to 2560 in two passes of 4, more in four passes of 2.
+constexpr uint32_t kRowEntries = 10240;
+
 struct LookupSmem {
-    static constexpr size_t kWin = 0;
-    static constexpr size_t kCand = kWin + GPZ_WIN_BYTES;  // [9][4096] newest | oldest << 16
-    static constexpr size_t kOwnTab = kCand + 9 * GPZ_SEG * 4;
-    static constexpr size_t kBytes = kOwnTab + kSlots * 4;
+    static constexpr size_t kWin = 0;                          // the window's bytes
+    static constexpr size_t kBitmap = kWin + GPZ_WIN_BYTES;    // u32[2048] the tile's hash set
+    static constexpr size_t kPrefix = kBitmap + kBmWords * 4;  // u16[2048] ids before each word
+    static constexpr size_t kOwnOld = kPrefix + kBmWords * 2;  // u16[4096] oldest offset per id
+    static constexpr size_t kBest = kOwnOld + GPZ_SEG * 2;     // u32[4096] best so far per position
+    static constexpr size_t kRows = kBest + GPZ_SEG * 4;       // u32[kRowEntries]
+    static constexpr size_t kBytes = kRows + kRowEntries * 4;
 };
+static_assert(LookupSmem::kRows % 16 == 0, "candidate rows are cleared with 16-byte stores");
+static_assert(kRowEntries % 4 == 0 && kRowEntries / 2 >= GPZ_SEG, "four passes must hold any tile");
 
-// The join's loads for one back segment (tile ts, ns distinct keys): this
-// thread's keys j = tid + u * T, u < GPZ_SEG / T, each guarded by j < ns <=
-// 4096, inside segment ts's arrays.  Absent keys read as kEmpty.
+// One CTA per 4 KiB tile S of a member (persistent over tiles); two CTAs
+// share an SM, so one's barriers and loads overlap the other's candidate
+// evaluation.  The window [S-8, S] plus 320 bytes of lookahead is staged in
+// shared memory, and the tile's hash set is rebuilt from its keys.  The
+// keys of segments S-1 .. S-8 are looked up in that set, which gives, for
+// every hash of the tile, the newest and oldest position in each of those
+// segments: the reference's table[h][seg] entries, for exactly the hashes
+// this tile queries.  Segments more than 8 back are never reachable: their
+// nearest position is more than 32768 bytes from any p in S, which
+// try_candidate rejects.  Then every position runs the reference's
+// candidate sequence (lz77_hash_lookup.wgsl:69-119): own segment (its
+// newest is always >= p, so only the oldest), then S-1 .. S-8, newest, then
+// oldest while best < 16.  When the rows of all 8 back segments do not fit,
+// the back segments are joined and evaluated a few at a time, in order,
+// with each position's best carried between passes.
 template <int T>
-__device__ __forceinline__ void join_load(const BatchParams& bp, uint32_t ts, uint32_t ns,
-                                          uint32_t (&hk)[GPZ_SEG / T], uint32_t (&ov)[GPZ_SEG / T]) {
-    const uint16_t* gk = bp.seg_keys + (size_t)ts * GPZ_SEG;
-    const uint32_t* go = bp.seg_on + (size_t)ts * GPZ_SEG;
-#pragma unroll
-    for (int u = 0; u < (int)(GPZ_SEG / T); u++) {
-        const uint32_t j = threadIdx.x + (uint32_t)u * T;
-        hk[u] = kEmpty;
-        ov[u] = 0u;
-        if (j < ns) {
-            hk[u] = gk[j];
-            ov[u] = go[j];
-        }
-    }
-}
-
-// Probes the loaded keys into the tile's table; a key found there writes
-// its segment's newest | oldest into the key's candidate row.
-template <int T>
-__device__ __forceinline__ void join_probe(const uint32_t* owntab, uint32_t* cb, const uint32_t (&hk)[GPZ_SEG / T],
-                                           const uint32_t (&ov)[GPZ_SEG / T]) {
-#pragma unroll
-    for (int u = 0; u < (int)(GPZ_SEG / T); u++) {
-        const uint32_t h = hk[u];
-        if (h == kEmpty) continue;
-        uint32_t sl = slot_of(h);
-        for (int probe = 0; probe < kSlots; probe++) {
-            const uint32_t wv = owntab[sl];
-            if (wv == kEmpty) break;
-            if ((wv & 0xFFFFu) == h) {
-                cb[(wv >> 16) & (GPZ_SEG - 1)] = ov[u];
-                break;
-            }
-            sl = (sl + 1u) & (kSlots - 1);
-        }
-    }
-}
-
-// One CTA per 4 KiB tile S of a member (persistent over tiles).  The window
-// [S-8, S] plus 320 bytes of lookahead is staged in shared memory.  The
-// tile's distinct hashes go into a shared-memory table; the distinct hashes
-// of segments S-1 .. S-8 are looked up in it, which gives, for every hash of
-// the tile, the newest and oldest position in each of those segments: the
-// reference's table[h][seg] entries, for exactly the hashes this tile
-// queries.  Segments more than 8 back are never reachable: their nearest
-// position is more than 32768 bytes from any p in S, which try_candidate
-// rejects.  Then every position runs the reference's candidate sequence on
-// its own (lz77_hash_lookup.wgsl:138-166): own segment (the newest is always
-// >= p, so only the oldest), then S-1 .. S-8, newest, then oldest while
-// best < 16.
-template <int T>
-__global__ void __launch_bounds__(T, 1) k_lookup(BatchParams bp) {
-    constexpr int PER = GPZ_SEG / T;
+__global__ void __launch_bounds__(T, 1024 / T) k_lookup(BatchParams bp) {
     extern __shared__ __align__(16) uint8_t smem[];
     uint8_t* win = smem + LookupSmem::kWin;
-    uint32_t* w32 = reinterpret_cast<uint32_t*>(win);
-    uint32_t* cand = reinterpret_cast<uint32_t*>(smem + LookupSmem::kCand);
-    uint32_t* owntab = reinterpret_cast<uint32_t*>(smem + LookupSmem::kOwnTab);
-    __shared__ uint32_t s_tile, s_nback_keys[8];
+    const uint32_t* w32 = reinterpret_cast<const uint32_t*>(win);
+    uint32_t* bm = reinterpret_cast<uint32_t*>(smem + LookupSmem::kBitmap);
+    uint16_t* pre = reinterpret_cast<uint16_t*>(smem + LookupSmem::kPrefix);
+    uint16_t* own_old = reinterpret_cast<uint16_t*>(smem + LookupSmem::kOwnOld);
+    uint32_t* bestv = reinterpret_cast<uint32_t*>(smem + LookupSmem::kBest);
+    uint32_t* rows = reinterpret_cast<uint32_t*>(smem + LookupSmem::kRows);
+    constexpr int PER = GPZ_SEG / T;
+    __shared__ uint32_t s_tile;
     const int tid = threadIdx.x;
 
     const uint32_t ntiles = bp.dims[0];
@@ -401,90 +368,115 @@ __global__ void __launch_bounds__(T, 1) k_lookup(BatchParams bp) {
         const uint32_t pl0 = start - w0;
         const uint32_t nback = min(S, 8u);
         const uint32_t nown = min(bp.seg_nkeys[t], GPZ_SEG);
-        uint32_t hk[PER], ov[PER];  // join keys of the next back segment
+        const uint32_t bpp = nown <= kRowEntries / 8u ? 8u : nown <= kRowEntries / 4u ? 4u : 2u;
+        const uint32_t npass = nback ? (nback + bpp - 1u) / bpp : 1u;
 
         // ---- stage the window [w0, w0 + wvalid) (16-byte vectors; members
-        // are 16-byte aligned and padded in the batch input); own-segment
-        // entries; candidate rows cleared
+        // are 16-byte aligned and padded in the batch input); clear the set
         {
             const uint4* src = reinterpret_cast<const uint4*>(bp.in + md.in_off + w0);
             uint4* dst = reinterpret_cast<uint4*>(win);
             const uint32_t nvec = (wvalid + 15u) >> 4;
             for (uint32_t i = tid; i < nvec; i += T) dst[i] = __ldg(src + i);
-            const uint32_t* go = bp.seg_on + (size_t)t * GPZ_SEG;
-            // key counts of the segments the join reads, all loaded at once
-            if (tid < nback) s_nback_keys[tid] = bp.seg_nkeys[t - 1u - tid];
-            // the keys of segment S-1 are loaded now, while the window is
-            // staged and the tile's table is built
-            if (nback) join_load<T>(bp, t - 1u, min(bp.seg_nkeys[t - 1u], GPZ_SEG), hk, ov);
-            for (uint32_t i = tid; i < nown; i += T) cand[i] = go[i];
-            for (uint32_t i = tid; i < nback * GPZ_SEG; i += T) cand[GPZ_SEG + i] = kEmpty;
-            for (int i = tid; i < kSlots; i += T) owntab[i] = kEmpty;
+            for (uint32_t i = tid; i < (uint32_t)kBmWords; i += T) bm[i] = 0u;
+            for (uint32_t i = tid; i < cnt; i += T) bestv[i] = 0u;
             __syncthreads();
             const uint32_t zend = min((uint32_t)GPZ_WIN_BYTES, (nvec << 4) + 32u);
             for (uint32_t i = wvalid + tid; i < zend; i += T) win[i] = 0;
+            // the tile's hash set; its keys ascend, so a key's index is its
+            // rank, and the first key of each word gives the word's prefix
             const uint16_t* gk = bp.seg_keys + (size_t)t * GPZ_SEG;
+            const uint32_t* go = bp.seg_on + (size_t)t * GPZ_SEG;
             for (uint32_t i = tid; i < nown; i += T) {
                 const uint32_t h = gk[i];
-                uint32_t sl = slot_of(h);
-                for (int probe = 0; probe < kSlots; probe++) {
-                    if (atomicCAS(&owntab[sl], kEmpty, h | (i << 16)) == kEmpty) break;
-                    sl = (sl + 1u) & (kSlots - 1);
-                }
+                atomicOr(&bm[h >> 5], 1u << (h & 31u));
+                if (i == 0u || (uint32_t)(gk[i - 1u] >> 5) != (h >> 5)) pre[h >> 5] = (uint16_t)i;
+                own_old[i] = (uint16_t)(go[i] >> 16);
             }
         }
-        uint32_t myid[PER];
-        const uint16_t* gpos = bp.seg_posid + (size_t)t * GPZ_SEG;
-#pragma unroll
-        for (int k = 0; k < PER; k++) {
-            const uint32_t i = tid + k * T;
-            myid[k] = i < cnt ? (uint32_t)gpos[i] : 0xFFFFu;
-        }
-        __syncthreads();
 
-        // ---- join: the distinct hashes of segments S-1 .. S-8 probe the
-        // tile's table (each segment writes its own candidate row).  The
-        // keys of segment S-back-1 are loaded before S-back's are probed.
-        for (uint32_t back = 1; back <= nback; back++) {
-            uint32_t hn[PER], on[PER];
-            if (back < nback) {
-                join_load<T>(bp, t - back - 1u, min(s_nback_keys[back], GPZ_SEG), hn, on);
-            } else {
-#pragma unroll
-                for (int u = 0; u < PER; u++) hn[u] = on[u] = kEmpty;
+        for (uint32_t pass = 0; pass < npass; pass++) {
+            const uint32_t b0 = 1u + pass * bpp;
+            const uint32_t nb = nback >= b0 ? min(bpp, nback - b0 + 1u) : 0u;
+            // ---- this pass's rows: cleared, then the join of its back
+            // segments (their keys probe the tile's set; a key found there
+            // writes its segment's newest | oldest into the key's row)
+            __syncthreads();
+            {
+                uint4* r4 = reinterpret_cast<uint4*>(rows);
+                const uint32_t n4 = (nown * bpp + 3u) >> 2;
+                for (uint32_t r = tid; r < n4; r += T) r4[r] = make_uint4(kEmpty, kEmpty, kEmpty, kEmpty);
             }
-            join_probe<T>(owntab, cand + back * GPZ_SEG, hk, ov);
+            __syncthreads();
+            for (uint32_t j = 0; j < nb; j++) {
+                const uint32_t ts = t - (b0 + j);
+                const uint32_t ns = min(bp.seg_nkeys[ts], GPZ_SEG);
+                const uint16_t* gk = bp.seg_keys + (size_t)ts * GPZ_SEG;
+                const uint32_t* go = bp.seg_on + (size_t)ts * GPZ_SEG;
+                uint32_t hk[PER], ov[PER];
 #pragma unroll
-            for (int u = 0; u < PER; u++) {
-                hk[u] = hn[u];
-                ov[u] = on[u];
-            }
-        }
-        __syncthreads();
-
-        // ---- every position walks its candidates in the reference's order
-        uint32_t* dst = bp.pp + md.in_off + start;
-#pragma unroll
-        for (int k = 0; k < PER; k++) {
-            const uint32_t i = tid + k * T;
-            if (i >= cnt) continue;
-            const uint32_t id = myid[k], p = start + i;
-            uint32_t best = 0;
-            if (id != 0xFFFFu) {
-                const Head hp = load_head(w32, pl0 + i);
-                try_cand(win, w32, hp, start + (cand[id] >> 16) + 1u, p, n, w0, best);
-                for (uint32_t back = 1; back <= nback; back++) {
-                    const uint32_t on = cand[back * GPZ_SEG + id];
-                    if (on == kEmpty) continue;
-                    const uint32_t qb = (S - back) << GPZ_SEG_LOG2;
-                    const uint32_t rn = qb + (on & 0xFFFFu) + 1u;
-                    try_cand(win, w32, hp, rn, p, n, w0, best);
-                    if ((best >> 16) < 16u) {
-                        const uint32_t ro = qb + (on >> 16) + 1u;
-                        if (ro != rn) try_cand(win, w32, hp, ro, p, n, w0, best);
+                for (int u = 0; u < PER; u++) {
+                    const uint32_t q = tid + (uint32_t)u * T;
+                    hk[u] = kEmpty;
+                    ov[u] = 0u;
+                    if (q < ns) {
+                        hk[u] = gk[q];
+                        ov[u] = go[q];
                     }
                 }
+#pragma unroll
+                for (int u = 0; u < PER; u++) {
+                    const uint32_t h = hk[u];
+                    if (h == kEmpty) continue;
+                    const uint32_t w = h >> 5, word = bm[w], bit = 1u << (h & 31u);
+                    if (!(word & bit)) continue;
+                    const uint32_t id = pre[w] + __popc(word & (bit - 1u));
+                    if (id < nown) rows[id * bpp + j] = ov[u];
+                }
             }
+            __syncthreads();
+
+            // ---- every position tries this pass's candidates in the
+            // reference's order
+#pragma unroll 1
+            for (uint32_t i = tid; i < cnt; i += T) {
+                if (start + i + 2u >= n) continue;  // no hash: a literal
+                const uint32_t b = pl0 + i;
+                const uint32_t h = hash3_at(win + b);
+                const uint32_t w = h >> 5, word = bm[w], bit = 1u << (h & 31u);
+                const uint32_t id = pre[w] + __popc(word & (bit - 1u));
+                if (!(word & bit) || id >= nown) continue;  // never: the tile's own hash is in its set
+                const uint32_t limit = min(GPZ_MAX_MATCH, n - start - i);
+                uint32_t best = bestv[i];
+                if ((best >> 16) >= limit) continue;
+                const Head hp = load_head(w32, b);
+                if (pass == 0u) {
+                    const uint32_t oo = own_old[id];
+                    if (oo < i) try_win(win, w32, hp, pl0 + oo, b, i - oo, limit, best);
+                }
+                const uint32_t* row = rows + id * bpp;
+                for (uint32_t j = 0; j < nb; j++) {
+                    const uint32_t on = row[j];
+                    if (on == kEmpty) continue;
+                    const uint32_t back = b0 + j;
+                    const uint32_t qa = pl0 - (back << GPZ_SEG_LOG2);  // segment S - back in the window
+                    const uint32_t on_n = on & 0xFFFFu, on_o = on >> 16;
+                    // a candidate up to 7 segments back is within 32767
+                    // bytes of p; 8 back, only if p's offset is at most its own
+                    if (back < 8u || i <= on_n)
+                        try_win(win, w32, hp, qa + on_n, b, (back << GPZ_SEG_LOG2) + i - on_n, limit, best);
+                    if ((best >> 16) < 16u && on_o != on_n && (back < 8u || i <= on_o))
+                        try_win(win, w32, hp, qa + on_o, b, (back << GPZ_SEG_LOG2) + i - on_o, limit, best);
+                }
+                bestv[i] = best;
+            }
+        }
+        __syncthreads();
+
+        // ---- pp of the tile: the best match, or the literal byte
+        uint32_t* dst = bp.pp + md.in_off + start;
+        for (uint32_t i = tid; i < cnt; i += T) {
+            const uint32_t best = bestv[i];
             dst[i] = (best >> 16) ? best : (uint32_t)win[pl0 + i];
         }
     }
@@ -1925,7 +1917,7 @@ int gpz_kernel_smem_setup() {
     tab[0] = x8;
     for (int k = 1; k < 32; k++) tab[k] = mul(tab[k - 1], tab[k - 1]);
     if (cudaMemcpyToSymbol(c_x8pow2, tab, sizeof tab) != cudaSuccess) return -1;
-    if (cudaFuncSetAttribute(k_segtab<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSegtabSmem) !=
+    if (cudaFuncSetAttribute(k_segtab<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SegtabSmem::kBytes) !=
         cudaSuccess)
         return -1;
     const int smem = (int)LookupSmem::kBytes;
@@ -1949,7 +1941,7 @@ int gpz_launch_batch(const BatchParams& bp, const LaunchShape& ls, void* stream,
     mark(0);
     const int gs = grid_of(ls.segtab_grid, bp.ntiles);
     const int gl = grid_of(ls.lookup_grid, bp.ntiles);
-    k_segtab<512><<<gs, 512, kSegtabSmem, s>>>(bp);
+    k_segtab<512><<<gs, 512, SegtabSmem::kBytes, s>>>(bp);
     mark(1);
     switch (ls.lookup_threads) {
         case 512: k_lookup<512><<<gl, 512, LookupSmem::kBytes, s>>>(bp); break;
@@ -2002,7 +1994,7 @@ int gpz_occupancy(LaunchShape* persistent) {
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, f, threads, smem) != cudaSuccess || n < 1) n = 1;
         return n;
     };
-    persistent->segtab_grid = sms * occ((const void*)k_segtab<512>, 512, kSegtabSmem);
+    persistent->segtab_grid = sms * occ((const void*)k_segtab<512>, 512, SegtabSmem::kBytes);
     persistent->lookup_grid = sms * occ(persistent->lookup_threads == 512 ? (const void*)k_lookup<512>
                                                                            : (const void*)k_lookup<1024>,
                                         persistent->lookup_threads, LookupSmem::kBytes);

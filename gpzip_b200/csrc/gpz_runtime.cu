@@ -47,6 +47,7 @@ constexpr size_t kDefaultMember = 131072;
 constexpr size_t kMaxMember = 2u << 20;
 constexpr size_t kDefaultBatch = 64u << 20;
 constexpr size_t kDefaultPool = 40ull << 30;
+constexpr int kDefaultWaitMs = 60000;
 // pipeline slots of the synchronous path: while one pass computes, the
 // next two can be staged and uploaded
 constexpr int kSyncSlots = 3;
@@ -219,7 +220,7 @@ struct Span {
 };
 
 struct Slot {
-    DevArena d_in, d_pp, d_tok, d_out, d_skeys, d_son, d_sposid, d_snkeys, d_tentry, d_texit, d_thist, d_tntok,
+    DevArena d_in, d_pp, d_tok, d_out, d_skeys, d_son, d_snkeys, d_tentry, d_texit, d_thist, d_tntok,
         d_tbit, d_mcodes, d_mhdr, d_mout, d_cnt, d_members, d_tiles, d_dims;
     uint8_t* h_in = nullptr;
     size_t h_in_cap = 0;
@@ -247,6 +248,9 @@ struct Slot {
     std::vector<Span> spans;
     size_t in_bytes = 0;
     bool busy = false;
+    // a call stopped waiting for this slot's last work (GPZ_E_TIMEOUT): the
+    // work may still run, so the slot is not reused until `done` completes
+    bool stale = false;
     int bucket = 0;
 };
 
@@ -261,6 +265,8 @@ struct gpz_ctx {
     size_t batch_bytes = kDefaultBatch;
     int flags = 0;
     int sms = 0;
+    // bound of every host wait for the device in the calling thread, ms
+    std::atomic<int> wait_ms{kDefaultWaitMs};
     std::mutex mu;  // the synchronous entry points (and their slots)
     // gpz_compress_chunk callers waiting to be batched (see there)
     struct ChunkCall {
@@ -320,6 +326,28 @@ int fail(gpz_ctx* c, int code, const char* what, cudaError_t e = cudaSuccess) {
         cudaError_t _e = (call);                                          \
         if (_e != cudaSuccess) return fail((ctx), GPZ_E_CUDA, #call, _e); \
     } while (0)
+
+// Waits for event e at most the context's wait_ms (GPZ_E_TIMEOUT when that
+// passes first; a limit of 0 gives up at once unless e is already done).
+// The first 2 ms poll without sleeping, as a spinning synchronisation would;
+// after that the thread sleeps 50 us between polls.  A device error ends the
+// wait with GPZ_E_CUDA.
+int wait_event(gpz_ctx* c, cudaEvent_t e, const char* what) {
+    const double t0 = now_ms();
+    const int limit = c->wait_ms.load();
+    for (;;) {
+        const cudaError_t q = cudaEventQuery(e);
+        if (q == cudaSuccess) return GPZ_OK;
+        if (q != cudaErrorNotReady) {
+            cudaGetLastError();
+            return fail(c, GPZ_E_CUDA, what, q);
+        }
+        const double el = now_ms() - t0;
+        if (el >= (double)limit) return fail(c, GPZ_E_TIMEOUT, what);
+        if (el < 2.0) _mm_pause();
+        else std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
+}
 
 // capped: the growth counts against the context's pool cap (the serving
 // engine's fixed arenas, sized once at start, do not).
@@ -424,7 +452,6 @@ int reserve_counts(gpz_ctx* c, Slot& sl, size_t in_bytes, size_t nm, size_t nt, 
     if (own_out && (rc = ensure_dev(c, sl, sl.d_out, out_bytes + 64, capped))) return rc;
     if ((rc = ensure_dev(c, sl, sl.d_skeys, nt * GPZ_SEG * 2, capped))) return rc;
     if ((rc = ensure_dev(c, sl, sl.d_son, nt * GPZ_SEG * 4, capped))) return rc;
-    if ((rc = ensure_dev(c, sl, sl.d_sposid, nt * GPZ_SEG * 2, capped))) return rc;
     if ((rc = ensure_dev(c, sl, sl.d_snkeys, nt * 4, capped))) return rc;
     if ((rc = ensure_dev(c, sl, sl.d_tentry, nt * 4, capped))) return rc;
     if ((rc = ensure_dev(c, sl, sl.d_texit, nt * GPZ_EXITS * 2, capped))) return rc;
@@ -472,7 +499,6 @@ BatchParams params_of(const gpz_ctx* c, Slot& sl, const uint8_t* d_in, uint8_t* 
     bp.pp = static_cast<uint32_t*>(sl.d_pp.p);
     bp.seg_keys = static_cast<uint16_t*>(sl.d_skeys.p);
     bp.seg_on = static_cast<uint32_t*>(sl.d_son.p);
-    bp.seg_posid = static_cast<uint16_t*>(sl.d_sposid.p);
     bp.seg_nkeys = static_cast<uint32_t*>(sl.d_snkeys.p);
     bp.tok = static_cast<uint32_t*>(sl.d_tok.p);
     bp.out_words = reinterpret_cast<uint32_t*>(d_out);
@@ -608,7 +634,8 @@ int autotune(gpz_ctx* c, Slot& sl, const BatchParams& bp, const DrainTarget* dt,
         cudaEventRecord(a, s);
         rc = launch(c, sl, bp, cand, false, dt, false, s);
         cudaEventRecord(b, s);
-        if (cudaEventSynchronize(b) != cudaSuccess) rc = fail(c, GPZ_E_CUDA, "autotune", cudaGetLastError());
+        if (rc == GPZ_OK) rc = wait_event(c, b, "autotune");
+        if (rc == GPZ_E_TIMEOUT && cudaEventRecord(sl.done, s) == cudaSuccess) sl.stale = true;
         float ms = 0;
         cudaEventElapsedTime(&ms, a, b);
         if (rc == GPZ_OK && i >= 8 && ms < best) {
@@ -793,15 +820,15 @@ void frame_members(const MemberOut* mo, size_t first, size_t count, uint8_t* dst
 int wait_slot(gpz_ctx* c, Slot& sl) {
     sl.busy = false;
     const double t0 = now_ms();
-    CU(c, cudaEventSynchronize(sl.done));
+    const int w = wait_event(c, sl.done, "waiting for a device pass");
     add_time(c, 3, now_ms() - t0);
+    if (w == GPZ_E_TIMEOUT) sl.stale = true;
+    if (w) return w;
     cudaEventElapsedTime(&sl.last_h2d_ms, sl.tv[0], sl.tv[1]);
     cudaEventElapsedTime(&sl.last_kernel_ms, sl.tv[1], sl.tv[2]);
     if (c->flags & GPZ_FLAG_STAGE_TIMING)
         for (int i = 0; i < GPZ_STAGES; i++) cudaEventElapsedTime(&c->stage_ms[i], sl.ev[i], sl.ev[i + 1]);
-    const uint32_t err = *sl.h_err;
-    if (err & GPZ_ERRBIT_SPIN) return fail(c, GPZ_E_TIMEOUT, "bounded device wait expired");
-    if (err) return fail(c, GPZ_E_INTERNAL, "device self-check failed");
+    if (*sl.h_err) return fail(c, GPZ_E_INTERNAL, "device self-check failed");
     return GPZ_OK;
 }
 
@@ -837,9 +864,26 @@ int finish_slot(gpz_ctx* c, Slot& sl, gpz_out* outs, size_t first_item) {
     return first_bad;
 }
 
+// Before a synchronous call reuses the context's slots: the work of every
+// slot a timed-out call left behind must have finished (bounded again).
+int settle_stale(gpz_ctx* c) {
+    for (int k = 0; k <= kSyncSlots; k++) {
+        Slot* sl = k < kSyncSlots ? &c->slots[k] : &c->inf;
+        if (!sl->stale) continue;
+        const int rc = wait_event(c, sl->done, "work of an earlier call that timed out");
+        if (rc) return rc;
+        sl->stale = false;
+    }
+    return GPZ_OK;
+}
+
 // Items -> device passes of at most batch_bytes, pipelined over the slots
 // (plain: one item per pass, waited for before the next).
 int run_host_items(gpz_ctx* c, const gpz_desc* d, size_t count, gpz_out* outs, bool plain) {
+    if (const int rc = settle_stale(c)) {
+        for (size_t q = 0; q < count; q++) outs[q].status = rc;
+        return rc;
+    }
     int first_bad = GPZ_OK, fatal = GPZ_OK;
     size_t pending_first[kSyncSlots] = {};
     auto settle = [&](int k) {
@@ -900,7 +944,7 @@ void free_slot(gpz_ctx* c, Slot& sl) {
     if (sl.stream) cudaStreamSynchronize(sl.stream);
     for (auto& g : sl.graphs)
         if (g.exec) cudaGraphExecDestroy(g.exec);
-    for (DevArena* a : {&sl.d_in, &sl.d_pp, &sl.d_tok, &sl.d_out, &sl.d_skeys, &sl.d_son, &sl.d_sposid, &sl.d_snkeys,
+    for (DevArena* a : {&sl.d_in, &sl.d_pp, &sl.d_tok, &sl.d_out, &sl.d_skeys, &sl.d_son, &sl.d_snkeys,
                         &sl.d_tentry, &sl.d_texit, &sl.d_thist, &sl.d_tntok, &sl.d_tbit, &sl.d_mcodes, &sl.d_mhdr,
                         &sl.d_mout, &sl.d_cnt, &sl.d_members, &sl.d_tiles, &sl.d_dims})
         if (a->p) {
@@ -1044,12 +1088,15 @@ bool make_partitions(int device, int first, SmPartition out[2]) {
 //
 // A request completes when its last unit does; its gzip stream is its
 // units' members in order: byte for byte what gpz_compress_chunk returns for
-// it alone.  Admission: a request is rejected (GPZ_E_BUSY) while the bytes
-// queued or on the device would exceed the pool cap.
+// it alone.  Admission: a request is rejected with GPZ_E_ADMISSION while the
+// bytes queued or on the device would exceed the pool cap, and with
+// GPZ_E_BUSY while kMaxRequests requests are submitted and not yet polled.
 struct ServeEngine {
     static constexpr size_t kUnit = 2u << 20;
     static constexpr size_t kSmall = 1u << 20;
     static constexpr int kLaneSlots = 3;
+    // requests submitted and not yet polled: beyond this, submit says busy
+    static constexpr size_t kMaxRequests = 1u << 20;
 
     struct Lane {
         int nslots = 2;         // pipeline slots in use (at most kLaneSlots)
@@ -1177,6 +1224,10 @@ struct ServeEngine {
             std::lock_guard<std::mutex> lk(mu);
             if (queued_bytes + d->n > c->pool_cap) {
                 rejected++;
+                return GPZ_E_ADMISSION;
+            }
+            if (reqs.size() >= kMaxRequests) {
+                rejected++;
                 return GPZ_E_BUSY;
             }
             queued_bytes += d->n;
@@ -1303,6 +1354,13 @@ struct ServeEngine {
                 L.st.kernel_ms += L.slots[k].last_kernel_ms;
             }
             complete(L, k, rc);
+            // the batch's requests have their status; a batch that outlived
+            // the wait still runs, so its slot is reused only once it is done
+            if (L.slots[k].stale) {
+                cudaEventSynchronize(L.slots[k].done);
+                cudaGetLastError();
+                L.slots[k].stale = false;
+            }
             std::lock_guard<std::mutex> lk(mu);
             L.slot_free[k] = true;
             L.cv_work.notify_one();
@@ -1394,6 +1452,11 @@ int gpz_create(const gpz_config* cfg, gpz_ctx** out) {
     c->pool_cap = cfg->pool_bytes ? cfg->pool_bytes : kDefaultPool;
     c->batch_bytes = cfg->batch_bytes ? cfg->batch_bytes : kDefaultBatch;
     c->flags = cfg->flags;
+    if (cfg->wait_ms < 0) {
+        delete c;
+        return GPZ_E_ARG;
+    }
+    c->wait_ms = cfg->wait_ms ? cfg->wait_ms : kDefaultWaitMs;
     if (cudaSetDevice(c->device) != cudaSuccess || gpz_kernel_smem_setup() != 0) {
         cudaGetLastError();
         delete c;
@@ -1525,6 +1588,8 @@ int gpz_compress_device(gpz_ctx* c, const void* d_in, const uint64_t* in_off, co
     if (!c || !d_in || !d_out || !in_off || !in_len || !out_off || !count) return GPZ_E_ARG;
     std::lock_guard<std::mutex> lk(c->mu);
     cudaSetDevice(c->device);
+    int rc;
+    if ((rc = settle_stale(c))) return rc;
     Slot& sl = c->slots[0];
     sl.spans.assign(count, Span{});
     size_t in_end = 0;
@@ -1536,7 +1601,6 @@ int gpz_compress_device(gpz_ctx* c, const void* d_in, const uint64_t* in_off, co
     }
     plan(c, sl);
     if (out_bound_of_plan(sl) > out_cap) return fail(c, GPZ_E_SPACE, "device output buffer below bound");
-    int rc;
     if ((rc = reserve(c, sl, in_end, false, false, 0))) return rc;
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : sl.stream;
     if ((rc = upload_desc(c, sl, s))) return rc;
@@ -1546,11 +1610,15 @@ int gpz_compress_device(gpz_ctx* c, const void* d_in, const uint64_t* in_off, co
     if ((rc = launch(c, sl, bp, shape_for(c, sl.bucket), false, nullptr, timing, s))) return rc;
     CU(c, cudaMemcpyAsync(sl.h_mout, sl.d_mout.p, sl.members.size() * sizeof(MemberOut), cudaMemcpyDeviceToHost, s));
     CU(c, cudaMemcpyAsync(sl.h_err, static_cast<uint32_t*>(sl.d_cnt.p) + GPZ_NCOUNTERS, 4, cudaMemcpyDeviceToHost, s));
-    CU(c, cudaStreamSynchronize(s));
+    CU(c, cudaEventRecord(sl.done, s));
+    if ((rc = wait_event(c, sl.done, "waiting for a device pass"))) {
+        if (rc == GPZ_E_TIMEOUT) sl.stale = true;
+        return rc;
+    }
     if (timing)
         for (int i = 0; i < GPZ_STAGES; i++) cudaEventElapsedTime(&c->stage_ms[i], sl.ev[i], sl.ev[i + 1]);
     c->mout.assign(sl.h_mout, sl.h_mout + sl.members.size());
-    if (*sl.h_err) return fail(c, (*sl.h_err & GPZ_ERRBIT_SPIN) ? GPZ_E_TIMEOUT : GPZ_E_INTERNAL, "device self-check");
+    if (*sl.h_err) return fail(c, GPZ_E_INTERNAL, "device self-check");
     for (size_t i = 0; i < count; i++) out_off[i] = c->mout[sl.spans[i].first_member].gz_off;
     const MemberOut& l = c->mout.back();
     out_off[count] = l.gz_off + 18 + l.deflate_bytes;
@@ -1649,6 +1717,7 @@ int gpz_inflate(gpz_ctx* c, const uint8_t* in, size_t n, uint8_t* out, size_t ou
     int rc = split_members(in, n, &ms, &total, &why);
     *out_len = total;
     if (rc) return fail(c, rc, why.c_str());
+    if ((rc = settle_stale(c))) return rc;
     if (total > out_cap || (!out && total)) return fail(c, GPZ_E_SPACE, "output buffer too small");
     if (ms.empty()) return GPZ_OK;
     Slot& sl = c->inf;
@@ -1659,6 +1728,10 @@ int gpz_inflate(gpz_ctx* c, const uint8_t* in, size_t n, uint8_t* out, size_t ou
         return rc;
     for (auto& e : c->inf_ev)
         if (!e) CU(c, cudaEventCreate(&e));
+    if (!sl.done) CU(c, cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
+    // member statuses come back through page-locked memory, so the wait for
+    // them is the bounded event wait below
+    if ((rc = ensure_host(c, sl, sl.h_err, sl.h_err_cap, nm, false))) return rc;
     cudaStream_t s = c->kstream;
     cudaPointerAttributes a{};
     const bool in_locked = cudaPointerGetAttributes(&a, in) == cudaSuccess && a.type == cudaMemoryTypeHost;
@@ -1677,15 +1750,18 @@ int gpz_inflate(gpz_ctx* c, const uint8_t* in, size_t n, uint8_t* out, size_t ou
         return fail(c, GPZ_E_CUDA, "inflate launch", cudaGetLastError());
     const bool out_locked = cudaPointerGetAttributes(&a, out) == cudaSuccess && a.type == cudaMemoryTypeHost;
     cudaGetLastError();
-    std::vector<uint32_t> status(nm);
-    CU(c, cudaMemcpyAsync(status.data(), sl.d_cnt.p, nm * 4, cudaMemcpyDeviceToHost, s));
+    const uint32_t* status = sl.h_err;
+    CU(c, cudaMemcpyAsync(sl.h_err, sl.d_cnt.p, nm * 4, cudaMemcpyDeviceToHost, s));
     if (out_locked) {
         CU(c, cudaMemcpyAsync(out, sl.d_out.p, total, cudaMemcpyDeviceToHost, s));
-        CU(c, cudaStreamSynchronize(s));
     } else {
         if ((rc = ensure_host(c, sl, sl.h_out, sl.h_out_cap, total, false))) return rc;
         CU(c, cudaMemcpyAsync(sl.h_out, sl.d_out.p, total, cudaMemcpyDeviceToHost, s));
-        CU(c, cudaStreamSynchronize(s));
+    }
+    CU(c, cudaEventRecord(sl.done, s));
+    if ((rc = wait_event(c, sl.done, "waiting for the inflate kernels"))) {
+        if (rc == GPZ_E_TIMEOUT) sl.stale = true;
+        return rc;
     }
     cudaEventElapsedTime(&c->inf_ms, c->inf_ev[0], c->inf_ev[1]);
     for (size_t i = 0; i < nm; i++)
@@ -1695,6 +1771,12 @@ int gpz_inflate(gpz_ctx* c, const uint8_t* in, size_t n, uint8_t* out, size_t ou
             return fail(c, GPZ_E_DATA, why.c_str());
         }
     if (!out_locked) copy_pool().run({CopyPool::Copy{out, sl.h_out, total}});
+    return GPZ_OK;
+}
+
+int gpz_set_wait_ms(gpz_ctx* c, int wait_ms) {
+    if (!c || wait_ms < 0) return GPZ_E_ARG;
+    c->wait_ms = wait_ms;
     return GPZ_OK;
 }
 
@@ -1834,12 +1916,12 @@ const char* gpz_strerror(int s) {
         case GPZ_OK: return "ok";
         case GPZ_E_NOMEM: return "out of device or pinned memory";
         case GPZ_E_ADMISSION: return "request exceeds the device pool cap";
-        case GPZ_E_TIMEOUT: return "bounded device wait expired";
+        case GPZ_E_TIMEOUT: return "the device did not finish within the context's wait limit";
         case GPZ_E_CUDA: return "CUDA runtime error";
         case GPZ_E_ARG: return "invalid argument";
         case GPZ_E_SPACE: return "output buffer too small";
         case GPZ_E_INTERNAL: return "device self-check failed";
-        case GPZ_E_BUSY: return "serving queue full";
+        case GPZ_E_BUSY: return "too many requests outstanding; poll some first";
         case GPZ_E_PENDING: return "result not ready";
         case GPZ_E_DATA: return "gzip data this path cannot split or decode";
         case GPZ_E_SINK: return "the writer's sink or chunk function failed";

@@ -41,8 +41,7 @@ constexpr size_t kTok = kPp + al(kMax * 4 + 64);
 constexpr size_t kOut = kTok + al(kMax * 4 + 64);
 constexpr size_t kSkeys = kOut + al(kOutCap + 64);
 constexpr size_t kSon = kSkeys + al(kTiles * GPZ_SEG * 2);
-constexpr size_t kSposid = kSon + al(kTiles * GPZ_SEG * 4);
-constexpr size_t kSnkeys = kSposid + al(kTiles * GPZ_SEG * 2);
+constexpr size_t kSnkeys = kSon + al(kTiles * GPZ_SEG * 4);
 constexpr size_t kTentry = kSnkeys + al(kTiles * 4);
 constexpr size_t kTexit = kTentry + al(kTiles * 4);
 constexpr size_t kThist = kTexit + al(kTiles * GPZ_EXITS * 2);
@@ -127,6 +126,15 @@ __global__ void k_static_finish(const uint8_t* base, uint8_t* dst, size_t cap) {
     }
 }
 
+// A call that fails after it has queued work on s waits for that work
+// before it returns (and releases the array to the next caller), so that
+// no kernel of a failed call still uses the array when the next one starts.
+int drain_failed(cudaStream_t s) {
+    cudaStreamSynchronize(s);
+    cudaGetLastError();
+    return GPZ_E_CUDA;
+}
+
 constexpr int kMaxDevices = 64;
 std::mutex g_static_mu[kMaxDevices];
 uint8_t* g_static_addr[kMaxDevices];  // device address of the scratch array, per device
@@ -160,7 +168,11 @@ extern "C" int gpz_compress_member_static(const uint8_t* d_in, size_t n, uint8_t
     uint8_t* base = g_static_addr[dev];
     cudaStream_t s = static_cast<cudaStream_t>(stream);
 
-    if (n && cudaMemcpyAsync(base + kIn, d_in, n, cudaMemcpyDeviceToDevice, s) != cudaSuccess) return GPZ_E_CUDA;
+    if (n && cudaMemcpyAsync(base + kIn, d_in, n, cudaMemcpyDeviceToDevice, s) != cudaSuccess) {
+        // the copy may still have been queued: let it finish before the
+        // array is released to the next caller
+        return drain_failed(s);
+    }
     k_static_setup<<<1, 256, 0, s>>>(base, (uint32_t)n);
 
     BatchParams bp{};
@@ -172,7 +184,6 @@ extern "C" int gpz_compress_member_static(const uint8_t* d_in, size_t n, uint8_t
     bp.out_words = reinterpret_cast<uint32_t*>(base + kOut);
     bp.seg_keys = reinterpret_cast<uint16_t*>(base + kSkeys);
     bp.seg_on = reinterpret_cast<uint32_t*>(base + kSon);
-    bp.seg_posid = reinterpret_cast<uint16_t*>(base + kSposid);
     bp.seg_nkeys = reinterpret_cast<uint32_t*>(base + kSnkeys);
     bp.tile_entry = reinterpret_cast<uint32_t*>(base + kTentry);
     bp.tile_exit = reinterpret_cast<uint16_t*>(base + kTexit);
@@ -189,18 +200,19 @@ extern "C" int gpz_compress_member_static(const uint8_t* d_in, size_t n, uint8_t
     bp.ntiles = (uint32_t)((n + GPZ_SEG - 1) / GPZ_SEG);
     bp.out_base = 0;
     const LaunchShape shape{1024, 0, 512, 0, 512, 0, 0, 0};
-    if (gpz_launch_batch(bp, shape, s, nullptr, nullptr) != 0) return GPZ_E_CUDA;
+    // the stages launched before a failing launch still run on s
+    if (gpz_launch_batch(bp, shape, s, nullptr, nullptr) != 0) return drain_failed(s);
     k_static_finish<<<8, 256, 0, s>>>(base, d_out, out_cap);
 
     unsigned long long result[2] = {0, 0};
-    if (cudaMemcpyAsync(result, base + kResult, sizeof result, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
-        cudaStreamSynchronize(s) != cudaSuccess) {
+    if (cudaMemcpyAsync(result, base + kResult, sizeof result, cudaMemcpyDeviceToHost, s) != cudaSuccess)
+        return drain_failed(s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) {
         cudaGetLastError();
         return GPZ_E_CUDA;
     }
     *out_len = (size_t)result[0];
     if (result[1] == 0xFFFFFFFFull) return GPZ_E_SPACE;
-    if (result[1] & GPZ_ERRBIT_SPIN) return GPZ_E_TIMEOUT;
     if (result[1]) return GPZ_E_INTERNAL;
     return GPZ_OK;
 }

@@ -1,15 +1,32 @@
-// gpz_writer.cu -- the streaming chunked writer of include/gpz.h: the
-// caller of ChunkFn in the reference, ParallelChunkedWriter
-// (crates/gpzip-codec-cpu/src/parallel.rs:28-229).
+// gpz_writer.cu -- the callers of the compression path in the reference,
+// rebuilt behind the C ABI of include/gpz.h:
 //
-// Written bytes are cut into chunk_size chunks.  Full chunks collect into
-// a batch of up to max_in_flight chunks; a full batch goes to the writer's
-// thread, which compresses it (one gpz_compress_batch call, or the caller's
-// chunk function per chunk) and hands the members to the sink in input
-// order, while the caller fills the next batch.  At most one batch waits
-// behind the one being compressed, so memory stays bounded.  The first
-// error is sticky (parallel.rs:70-89): every later call returns it.
+//  * the streaming chunked writer (gpz_writer_*): ParallelChunkedWriter
+//    (crates/gpzip-codec-cpu/src/parallel.rs:28-229);
+//  * the hybrid CPU + GPU chunk function (gpz_hybrid_*): the permit
+//    scheduler of `--backend auto` (crates/gpzip-cli/src/hybrid.rs:103-147);
+//  * the CPU gzip chunk function the hybrid falls through to
+//    (GzipCompressor::chunk_fn, crates/gpzip-codec-cpu/src/compress.rs:52-59),
+//    here zlib with the same level and framing.
+//
+// Writer.  Written bytes are cut into chunk_size chunks; the first error is
+// sticky (parallel.rs:70-89): every later call returns it, and nothing after
+// the failed chunk reaches the sink.
+//  - With a device context, full chunks collect into a batch of up to
+//    max_in_flight chunks; a full batch goes to the writer's thread, which
+//    compresses it with one gpz_compress_batch call and hands the members to
+//    the sink in input order while the caller fills the next batch.  At
+//    most one batch waits behind the one being compressed.
+//  - With a chunk function, every full chunk is handed to a pool of
+//    max_in_flight worker threads at once, as the reference spawns one rayon
+//    task per chunk (parallel.rs:91-129); up to max_in_flight chunks are
+//    compressed or waiting for their turn at the sink.  The worker that
+//    finishes the oldest chunk writes it and every finished chunk behind it,
+//    in input order, one sink call at a time.
+#include <zlib.h>
+
 #include <algorithm>
+#include <atomic>
 #include <condition_variable>
 #include <deque>
 #include <memory>
@@ -46,8 +63,9 @@ bool pool_take(size_t chunk_size, Chunk& into) {
 
 // Output buffers, kept across writers for the same reason: the first
 // touch of a fresh 64 MiB buffer (page faults, huge-page compaction) cost a
-// writer's first batch 50-260 ms instead of 4 ms.
-constexpr size_t kPoolOuts = 4;
+// writer's first batch 50-260 ms instead of 4 ms.  Chunk-function writers
+// keep one per chunk in flight.
+constexpr size_t kPoolOuts = 40;
 std::vector<std::pair<std::unique_ptr<uint8_t[]>, size_t>> g_outs;
 
 std::pair<std::unique_ptr<uint8_t[]>, size_t> out_take(size_t cap) {
@@ -90,23 +108,46 @@ struct gpz_writer {
     void* sink_user = nullptr;
     size_t chunk_size = 0, max_in_flight = 0;
     Chunk current;  // the chunk being filled (caller's thread only)
-    Batch filling;  // full chunks of the open batch (caller's thread only)
+    Batch filling;  // device mode: full chunks of the open batch (caller's thread only)
     bool finished = false;
 
     std::mutex mu;
     std::condition_variable cv;
-    std::deque<Batch> queue;  // batches handed over, not yet taken
-    bool busy = false;        // the thread is compressing a batch
     bool stop = false;
     int sticky = GPZ_OK;
+    std::vector<Chunk> spare;  // chunk buffers of finished chunks, reused (no page faults)
+
+    // ---- device mode: one thread compressing whole batches
+    std::deque<Batch> queue;  // batches handed over, not yet taken
+    bool busy = false;        // the thread is compressing a batch
     std::thread worker;
     std::unique_ptr<uint8_t[]> out;  // the thread's output buffer, from and back to the pool
     size_t out_cap = 0;
-    std::vector<Chunk> spare;  // chunk buffers of finished batches, reused (no page faults)
+
+    // ---- chunk-function mode: one job per chunk, workers in a pool
+    struct Job {
+        Chunk in;
+        std::unique_ptr<uint8_t[]> out;
+        size_t out_cap = 0, out_len = 0;
+        int rc = GPZ_OK;
+        bool done = false;
+    };
+    std::deque<std::unique_ptr<Job>> jobs;  // input order; the front is the next for the sink
+    size_t started = 0;                     // jobs[0 .. started) have been taken by a worker
+    bool sinking = false;                   // a worker is writing finished jobs to the sink
+    bool broken = false;                    // a job failed or the sink did: nothing more is written
+    std::vector<std::thread> pool;
+
+    void recycle(Chunk& ch) {
+        if (spare.size() < 2 * max_in_flight && ch.capacity() == chunk_size) {
+            ch.clear();
+            spare.push_back(std::move(ch));
+        }
+    }
 
     int compress(Batch& b) {
         size_t cap = 0;
-        for (const Chunk& ch : b) cap += ctx ? gpz_bound_ctx(ctx, ch.size()) : gpz_bound(ch.size());
+        for (const Chunk& ch : b) cap += gpz_bound_ctx(ctx, ch.size());
         if (out_cap < cap) {
             out_give(out, out_cap);
             auto o = out_take(cap);
@@ -115,31 +156,22 @@ struct gpz_writer {
             if (!out) return GPZ_E_NOMEM;
         }
         std::vector<gpz_out> outs(b.size());
+        std::vector<gpz_desc> ds(b.size());
         size_t off = 0;
         for (size_t i = 0; i < b.size(); i++) {
-            const size_t c = ctx ? gpz_bound_ctx(ctx, b[i].size()) : gpz_bound(b[i].size());
+            const size_t c = gpz_bound_ctx(ctx, b[i].size());
             outs[i] = gpz_out{out.get() + off, c, 0, 0};
+            ds[i] = gpz_desc{b[i].data(), b[i].size(), 5};
             off += c;
         }
-        if (ctx) {
-            std::vector<gpz_desc> ds(b.size());
-            for (size_t i = 0; i < b.size(); i++) ds[i] = gpz_desc{b[i].data(), b[i].size(), 5};
-            const int rc = gpz_compress_batch(ctx, ds.data(), ds.size(), outs.data());
-            if (rc != GPZ_OK) return rc;
-        } else {
-            for (size_t i = 0; i < b.size(); i++) {
-                size_t n = 0;
-                if (fn(fn_user, b[i].data(), b[i].size(), outs[i].out, outs[i].out_cap, &n) != 0 || n > outs[i].out_cap)
-                    return GPZ_E_SINK;
-                outs[i].out_len = n;
-            }
-        }
+        const int rc = gpz_compress_batch(ctx, ds.data(), ds.size(), outs.data());
+        if (rc != GPZ_OK) return rc;
         for (size_t i = 0; i < b.size(); i++)
             if (sink(sink_user, outs[i].out, outs[i].out_len) != 0) return GPZ_E_SINK;
         return GPZ_OK;
     }
 
-    void run() {
+    void run_batches() {
         for (;;) {
             Batch b;
             int failed;
@@ -157,17 +189,91 @@ struct gpz_writer {
             const int rc = failed != GPZ_OK ? failed : compress(b);
             std::lock_guard<std::mutex> lk(mu);
             if (rc != GPZ_OK && sticky == GPZ_OK) sticky = rc;
-            for (Chunk& ch : b)
-                if (spare.size() < 2 * max_in_flight && ch.capacity() == chunk_size) {
-                    ch.clear();
-                    spare.push_back(std::move(ch));
-                }
+            for (Chunk& ch : b) recycle(ch);
             busy = false;
             cv.notify_all();
         }
     }
 
-    // hands the open batch to the thread once fewer than one batch waits
+    // One worker of the chunk-function pool: takes the oldest job nobody
+    // has started, compresses it, then writes every finished job at the
+    // front of the queue unless another worker is already doing so.
+    void run_jobs() {
+        std::unique_lock<std::mutex> lk(mu);
+        for (;;) {
+            cv.wait(lk, [&] { return stop || started < jobs.size(); });
+            if (started >= jobs.size()) return;
+            Job* j = jobs[started++].get();
+            const int failed = sticky;
+            lk.unlock();
+            int rc = failed;
+            if (rc == GPZ_OK) {
+                const size_t cap = gpz_bound(j->in.size());
+                if (j->out_cap < cap) {
+                    auto o = out_take(cap);
+                    j->out = std::move(o.first);
+                    j->out_cap = j->out ? o.second : 0;
+                }
+                size_t n = 0;
+                if (!j->out) rc = GPZ_E_NOMEM;
+                else if (fn(fn_user, j->in.data(), j->in.size(), j->out.get(), cap, &n) != 0 || n > cap) rc = GPZ_E_SINK;
+                j->out_len = n;
+            }
+            lk.lock();
+            j->rc = rc;
+            j->done = true;
+            if (rc != GPZ_OK && sticky == GPZ_OK) sticky = rc;
+            if (!sinking) {
+                sinking = true;
+                while (!jobs.empty() && jobs.front()->done) {
+                    std::unique_ptr<Job> f = std::move(jobs.front());
+                    jobs.pop_front();
+                    started--;
+                    // the stream ends before the first failed job (in
+                    // input order): the jobs ahead of it are written, it
+                    // and everything after it are dropped (parallel.rs:
+                    // 144-150 writes results in order up to the gap)
+                    if (f->rc != GPZ_OK) broken = true;
+                    const bool write = !broken;
+                    lk.unlock();
+                    int src = GPZ_OK;
+                    if (write && sink(sink_user, f->out.get(), f->out_len) != 0) src = GPZ_E_SINK;
+                    out_give(f->out, f->out_cap);
+                    lk.lock();
+                    if (src != GPZ_OK) {
+                        broken = true;
+                        if (sticky == GPZ_OK) sticky = src;
+                    }
+                    recycle(f->in);
+                }
+                sinking = false;
+            }
+            cv.notify_all();
+        }
+    }
+
+    // hands a full chunk over: device mode batches it, chunk-function mode
+    // queues it for the pool once fewer than max_in_flight are outstanding
+    void dispatch(Chunk&& ch) {
+        if (ctx) {
+            filling.push_back(std::move(ch));
+            if (filling.size() >= max_in_flight) submit();
+            return;
+        }
+        auto j = std::unique_ptr<Job>(new (std::nothrow) Job());
+        std::unique_lock<std::mutex> lk(mu);
+        if (!j) {
+            if (sticky == GPZ_OK) sticky = GPZ_E_NOMEM;
+            return;
+        }
+        cv.wait(lk, [&] { return jobs.size() < max_in_flight; });
+        j->in = std::move(ch);
+        jobs.push_back(std::move(j));
+        cv.notify_all();
+    }
+
+    // device mode: hands the open batch to the thread once fewer than one
+    // batch waits
     void submit() {
         if (filling.empty()) return;
         std::unique_lock<std::mutex> lk(mu);
@@ -177,12 +283,19 @@ struct gpz_writer {
         cv.notify_all();
     }
 
+    // waits until every chunk handed over has been written or dropped
+    void drain() {
+        if (ctx) submit();
+        std::unique_lock<std::mutex> lk(mu);
+        cv.wait(lk, [&] { return queue.empty() && !busy && jobs.empty(); });
+    }
+
     int status() {
         std::lock_guard<std::mutex> lk(mu);
         return sticky;
     }
 
-    // an empty chunk buffer of chunk_size capacity, from a finished batch if
+    // an empty chunk buffer of chunk_size capacity, from a finished chunk if
     // one is free
     void fresh_chunk() {
         {
@@ -205,7 +318,7 @@ int open_writer(gpz_ctx* ctx, gpz_chunk_fn fn, void* fn_user, size_t chunk_size,
                 gpz_sink_fn sink, void* sink_user, gpz_writer** out) {
     if (!out) return GPZ_E_ARG;
     *out = nullptr;
-    if ((!ctx && !fn) || !sink || chunk_size == 0 || max_in_flight == 0) return GPZ_E_ARG;
+    if ((!ctx && !fn) || !sink || chunk_size == 0 || max_in_flight == 0 || max_in_flight > 1024) return GPZ_E_ARG;
     auto* w = new (std::nothrow) gpz_writer();
     if (!w) return GPZ_E_NOMEM;
     w->ctx = ctx;
@@ -215,7 +328,22 @@ int open_writer(gpz_ctx* ctx, gpz_chunk_fn fn, void* fn_user, size_t chunk_size,
     w->sink_user = sink_user;
     w->chunk_size = chunk_size;
     w->max_in_flight = max_in_flight;
-    w->worker = std::thread([w] { w->run(); });
+    try {
+        if (ctx) {
+            w->worker = std::thread([w] { w->run_batches(); });
+        } else {
+            for (size_t i = 0; i < max_in_flight; i++) w->pool.emplace_back([w] { w->run_jobs(); });
+        }
+    } catch (...) {
+        {
+            std::lock_guard<std::mutex> lk(w->mu);
+            w->stop = true;
+        }
+        w->cv.notify_all();
+        for (auto& t : w->pool) t.join();
+        delete w;
+        return GPZ_E_NOMEM;
+    }
     *out = w;
     return GPZ_OK;
 }
@@ -251,9 +379,8 @@ int gpz_writer_write(gpz_writer* w, const uint8_t* buf, size_t n) {
         buf += take;
         n -= take;
         if (w->current.size() == w->chunk_size) {
-            w->filling.push_back(std::move(w->current));
+            w->dispatch(std::move(w->current));
             w->current = Chunk{};  // capacity 0: the next byte takes a fresh buffer
-            if (w->filling.size() >= w->max_in_flight) w->submit();
         }
     }
     return w->status();
@@ -268,11 +395,9 @@ int gpz_writer_finish(gpz_writer* w) {
     if (!w) return GPZ_E_ARG;
     if (!w->finished) {
         w->finished = true;
-        if (!w->current.empty()) w->filling.push_back(std::move(w->current));
+        if (!w->current.empty()) w->dispatch(std::move(w->current));
         w->current = Chunk{};
-        w->submit();
-        std::unique_lock<std::mutex> lk(w->mu);
-        w->cv.wait(lk, [&] { return w->queue.empty() && !w->busy; });
+        w->drain();
     }
     return w->status();
 }
@@ -285,8 +410,142 @@ void gpz_writer_close(gpz_writer* w) {
         w->stop = true;
     }
     w->cv.notify_all();
-    w->worker.join();
+    if (w->worker.joinable()) w->worker.join();
+    for (auto& t : w->pool) t.join();
     pool_give(w->spare);
     out_give(w->out, w->out_cap);
     delete w;
+}
+
+// ================================================================ hybrid
+
+// The CPU chunk function: one gzip member of the whole chunk at a zlib
+// level, as GzipCompressor::chunk_fn writes with flate2's GzEncoder
+// (compress.rs:52-59: header with no name or time, the DEFLATE stream, the
+// CRC-32 / ISIZE trailer).  zlib writes OS = 3 (Unix) where flate2 writes
+// 255 (unknown); a gzip reader ignores the byte.
+int gpz_cpu_gzip_chunk(void* level, const uint8_t* in, size_t n, uint8_t* out, size_t out_cap, size_t* out_len) {
+    if ((!in && n) || !out || !out_len) return GPZ_E_ARG;
+    const int lvl = level ? *static_cast<const int*>(level) : 5;
+    if (lvl < 0 || lvl > 9) return GPZ_E_ARG;
+    z_stream z{};
+    if (deflateInit2(&z, lvl, Z_DEFLATED, 15 + 16, 8, Z_DEFAULT_STRATEGY) != Z_OK) return GPZ_E_NOMEM;
+    z.next_out = out;
+    z.avail_out = (uInt)std::min<size_t>(out_cap, 0xFFFFFFFFu);
+    static const uint8_t kEmpty = 0;
+    z.next_in = const_cast<Bytef*>(n ? in : &kEmpty);
+    int zr = Z_OK;
+    size_t left = n;
+    while (zr == Z_OK) {
+        const uInt take = (uInt)std::min<size_t>(left, 1u << 30);
+        z.avail_in = take;
+        left -= take;
+        zr = deflate(&z, left ? Z_NO_FLUSH : Z_FINISH);
+        if (zr == Z_OK && z.avail_out == 0) break;  // out of space
+    }
+    *out_len = out_cap - z.avail_out;
+    deflateEnd(&z);
+    return zr == Z_STREAM_END ? GPZ_OK : GPZ_E_SPACE;
+}
+
+struct gpz_hybrid {
+    gpz_hybrid_config cfg{};
+    int level = 5;
+    std::atomic<size_t> permits{0};
+    std::atomic<uint64_t> counter{0}, cpu_chunks{0}, gpu_chunks{0};
+    // the device context: the caller's, or one made on the first chunk
+    // that may use the GPU (so a small input never pays for it); a context
+    // that cannot be made leaves every chunk to the CPU
+    std::once_flag once;
+    gpz_ctx* ctx = nullptr;
+    bool own_ctx = false;
+
+    gpz_ctx* gpu() {
+        std::call_once(once, [this] {
+            if (cfg.ctx) {
+                ctx = cfg.ctx;
+                return;
+            }
+            gpz_config c;
+            gpz_config_default(&c);
+            c.device = cfg.device;
+            if (gpz_create(&c, &ctx) == GPZ_OK) own_ctx = true;
+            else ctx = nullptr;
+        });
+        return ctx;
+    }
+
+    // decrement-if-positive (hybrid.rs:150-163)
+    bool try_acquire() {
+        size_t cur = permits.load(std::memory_order_acquire);
+        while (cur) {
+            if (permits.compare_exchange_weak(cur, cur - 1, std::memory_order_acq_rel, std::memory_order_acquire))
+                return true;
+        }
+        return false;
+    }
+};
+
+void gpz_hybrid_config_default(gpz_hybrid_config* cfg) {
+    if (!cfg) return;
+    *cfg = gpz_hybrid_config{};
+    cfg->ctx = nullptr;
+    cfg->device = 0;
+    cfg->level = 5;
+    cfg->gpu_permits = 1;
+    cfg->warmup_chunks = 4;
+    cfg->cpu_fn = nullptr;
+    cfg->cpu_user = nullptr;
+    cfg->gpu_fn = nullptr;
+    cfg->gpu_user = nullptr;
+}
+
+int gpz_hybrid_create(const gpz_hybrid_config* cfg, gpz_hybrid** out) {
+    if (!out) return GPZ_E_ARG;
+    *out = nullptr;
+    gpz_hybrid_config def;
+    gpz_hybrid_config_default(&def);
+    if (!cfg) cfg = &def;
+    if (cfg->level < 0 || cfg->level > 9 || cfg->gpu_permits > 4096) return GPZ_E_ARG;
+    auto* h = new (std::nothrow) gpz_hybrid();
+    if (!h) return GPZ_E_NOMEM;
+    h->cfg = *cfg;
+    h->level = cfg->level;
+    h->permits = cfg->gpu_permits;
+    *out = h;
+    return GPZ_OK;
+}
+
+int gpz_hybrid_chunk(void* hp, const uint8_t* in, size_t n, uint8_t* out, size_t out_cap, size_t* out_len) {
+    auto* h = static_cast<gpz_hybrid*>(hp);
+    if (!h || (!in && n) || !out || !out_len) return GPZ_E_ARG;
+    // the composed ChunkFn of hybrid.rs:123-138: the first warmup_chunks
+    // chunks, and every chunk while no GPU permit is free, go to the CPU
+    const uint64_t k = h->counter.fetch_add(1, std::memory_order_relaxed);
+    if (h->cfg.gpu_permits > 0 && k >= h->cfg.warmup_chunks) {
+        gpz_ctx* g = h->cfg.gpu_fn ? nullptr : h->gpu();
+        if ((g || h->cfg.gpu_fn) && h->try_acquire()) {
+            const int rc = h->cfg.gpu_fn ? h->cfg.gpu_fn(h->cfg.gpu_user, in, n, out, out_cap, out_len)
+                                         : gpz_compress_chunk(g, in, n, h->level, out, out_cap, out_len);
+            h->permits.fetch_add(1, std::memory_order_release);
+            h->gpu_chunks.fetch_add(1, std::memory_order_relaxed);
+            return rc;
+        }
+    }
+    h->cpu_chunks.fetch_add(1, std::memory_order_relaxed);
+    if (h->cfg.cpu_fn) return h->cfg.cpu_fn(h->cfg.cpu_user, in, n, out, out_cap, out_len);
+    return gpz_cpu_gzip_chunk(&h->level, in, n, out, out_cap, out_len);
+}
+
+int gpz_hybrid_stats(const gpz_hybrid* h, uint64_t* cpu_chunks, uint64_t* gpu_chunks) {
+    if (!h) return GPZ_E_ARG;
+    if (cpu_chunks) *cpu_chunks = h->cpu_chunks.load();
+    if (gpu_chunks) *gpu_chunks = h->gpu_chunks.load();
+    return GPZ_OK;
+}
+
+void gpz_hybrid_destroy(gpz_hybrid* h) {
+    if (!h) return;
+    if (h->own_ctx) gpz_destroy(h->ctx);
+    delete h;
 }

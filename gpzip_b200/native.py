@@ -25,6 +25,8 @@ CHUNK_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.POINTER(ctypes
                             ctypes.POINTER(ctypes.c_uint8), ctypes.c_size_t, ctypes.POINTER(ctypes.c_size_t))
 GPZ_E_PENDING = 9
 GPZ_E_BUSY = 8
+GPZ_E_ADMISSION = 2
+GPZ_E_TIMEOUT = 3
 GPZ_FLAG_NO_GRAPHS = 1
 GPZ_FLAG_NO_AUTOTUNE = 2
 GPZ_FLAG_STAGE_TIMING = 4
@@ -42,7 +44,8 @@ EXPORTS = [
     "gpz_serve_reset_stats", "gpz_submit_ref", "gpz_host_times", "gpz_serve_lane_stats",
     "gpz_inflate_size", "gpz_inflate", "gpz_inflate_device_ms",
     "gpz_writer_open", "gpz_writer_open_fn", "gpz_writer_write", "gpz_writer_flush", "gpz_writer_finish",
-    "gpz_writer_close",
+    "gpz_writer_close", "gpz_set_wait_ms", "gpz_hybrid_config_default", "gpz_hybrid_create", "gpz_hybrid_chunk",
+    "gpz_hybrid_stats", "gpz_hybrid_destroy", "gpz_cpu_gzip_chunk",
 ]
 
 
@@ -54,7 +57,14 @@ class GpzError(RuntimeError):
 
 class Config(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("member_bytes", ctypes.c_size_t), ("pool_bytes", ctypes.c_size_t),
-                ("batch_bytes", ctypes.c_size_t), ("streams", ctypes.c_int), ("flags", ctypes.c_int)]
+                ("batch_bytes", ctypes.c_size_t), ("streams", ctypes.c_int), ("flags", ctypes.c_int),
+                ("wait_ms", ctypes.c_int)]
+
+
+class HybridConfig(ctypes.Structure):
+    _fields_ = [("ctx", ctypes.c_void_p), ("device", ctypes.c_int), ("level", ctypes.c_int),
+                ("gpu_permits", ctypes.c_size_t), ("warmup_chunks", ctypes.c_size_t), ("cpu_fn", ctypes.c_void_p),
+                ("cpu_user", ctypes.c_void_p), ("gpu_fn", ctypes.c_void_p), ("gpu_user", ctypes.c_void_p)]
 
 
 class Desc(ctypes.Structure):
@@ -166,6 +176,20 @@ def load(path: str = LIB_PATH) -> ctypes.CDLL:
     L.gpz_stage_times.restype = ctypes.c_int
     L.gpz_compress_member_static.argtypes = [vp, sz, vp, sz, ctypes.POINTER(sz), vp]
     L.gpz_compress_member_static.restype = ctypes.c_int
+    L.gpz_set_wait_ms.argtypes = [vp, ctypes.c_int]
+    L.gpz_set_wait_ms.restype = ctypes.c_int
+    L.gpz_hybrid_config_default.argtypes = [ctypes.POINTER(HybridConfig)]
+    L.gpz_hybrid_config_default.restype = None
+    L.gpz_hybrid_create.argtypes = [ctypes.POINTER(HybridConfig), ctypes.POINTER(vp)]
+    L.gpz_hybrid_create.restype = ctypes.c_int
+    L.gpz_hybrid_chunk.argtypes = [vp, vp, sz, vp, sz, ctypes.POINTER(sz)]
+    L.gpz_hybrid_chunk.restype = ctypes.c_int
+    L.gpz_hybrid_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
+    L.gpz_hybrid_stats.restype = ctypes.c_int
+    L.gpz_hybrid_destroy.argtypes = [vp]
+    L.gpz_hybrid_destroy.restype = None
+    L.gpz_cpu_gzip_chunk.argtypes = [vp, vp, sz, vp, sz, ctypes.POINTER(sz)]
+    L.gpz_cpu_gzip_chunk.restype = ctypes.c_int
     _lib = L
     return L
 
@@ -197,12 +221,12 @@ class Context:
     """One gpz_ctx (device pool, streams, launch shapes) on one CUDA device."""
 
     def __init__(self, device: int = 0, member_bytes: int = 128 * 1024, pool_bytes: int = 0,
-                 batch_bytes: int = 0, flags: int = 0):
+                 batch_bytes: int = 0, flags: int = 0, wait_ms: int = 0):
         L = load()
         cfg = Config()
         L.gpz_config_default(ctypes.byref(cfg))
         cfg.device, cfg.member_bytes, cfg.pool_bytes = device, member_bytes, pool_bytes
-        cfg.batch_bytes, cfg.flags = batch_bytes, flags
+        cfg.batch_bytes, cfg.flags, cfg.wait_ms = batch_bytes, flags, wait_ms
         h = ctypes.c_void_p()
         rc = L.gpz_create(ctypes.byref(cfg), ctypes.byref(h))
         if rc != GPZ_OK:
@@ -234,6 +258,11 @@ class Context:
 
     def bound(self, n: int) -> int:
         return self.L.gpz_bound_ctx(self._h, n)
+
+    def set_wait_ms(self, ms: int):
+        """Bound of every wait for the device (0: give up at once unless the
+        work is done; such a call raises GpzError with GPZ_E_TIMEOUT)."""
+        self._check(self.L.gpz_set_wait_ms(self._h, ms), "gpz_set_wait_ms")
 
     def compress_chunk(self, data, level: int = 5) -> bytes:
         a = _u8(data)
@@ -393,19 +422,108 @@ class Context:
         return {f: getattr(s, f) for f, _ in ServeStats._fields_}
 
 
+def cpu_gzip_chunk(data, level: int = 5) -> bytes:
+    """gpz_cpu_gzip_chunk: one zlib gzip member of `data` at `level` (the
+    CPU chunk function of the hybrid backend)."""
+    L = load()
+    a = _u8(data)
+    cap = L.gpz_bound(a.size)
+    out = np.empty(cap, dtype=np.uint8)
+    n = ctypes.c_size_t()
+    lv = ctypes.c_int(level)
+    rc = L.gpz_cpu_gzip_chunk(ctypes.byref(lv), _p(a), a.size, _p(out), cap, ctypes.byref(n))
+    if rc:
+        raise GpzError(rc, "gpz_cpu_gzip_chunk")
+    return out[:n.value].tobytes()
+
+
+def _py_chunk_fn(f):
+    """A gpz_chunk_fn that calls f(bytes) -> bytes (a raise or a short
+    buffer is a nonzero status)."""
+    def call(_user, buf, n, out, cap, out_len):
+        try:
+            g = bytes(f(ctypes.string_at(buf, n)))
+        except Exception:  # noqa: BLE001 -- the status carries the failure
+            return 1
+        if len(g) > cap:
+            return 1
+        ctypes.memmove(out, g, len(g))
+        out_len[0] = len(g)
+        return 0
+    return CHUNK_FN(call)
+
+
+class Hybrid:
+    """gpz_hybrid: the `--backend auto` chunk function (CPU and GPU chunks by
+    permit).  `ctx`: a Context to use for GPU chunks (None: the library makes
+    one on `device` at the first GPU chunk).  `cpu_fn` / `gpu_fn`: Python
+    chunk functions (bytes -> gzip bytes) that replace either side, e.g. a
+    stand-in device in tests.  Pass it to Writer(hybrid=...)."""
+
+    def __init__(self, ctx: "Context" = None, device: int = 0, level: int = 5, gpu_permits: int = 1,
+                 warmup_chunks: int = 4, cpu_fn=None, gpu_fn=None):
+        self.L = load()
+        cfg = HybridConfig()
+        self.L.gpz_hybrid_config_default(ctypes.byref(cfg))
+        cfg.ctx = ctx._h.value if ctx is not None else None
+        cfg.device, cfg.level, cfg.gpu_permits, cfg.warmup_chunks = device, level, gpu_permits, warmup_chunks
+        self._fns = [_py_chunk_fn(f) if f is not None else None for f in (cpu_fn, gpu_fn)]  # kept alive
+        if cpu_fn is not None:
+            cfg.cpu_fn = ctypes.cast(self._fns[0], ctypes.c_void_p).value
+        if gpu_fn is not None:
+            cfg.gpu_fn = ctypes.cast(self._fns[1], ctypes.c_void_p).value
+        self._ctx = ctx  # kept alive with the hybrid
+        self.gpu_permits = gpu_permits
+        h = ctypes.c_void_p()
+        rc = self.L.gpz_hybrid_create(ctypes.byref(cfg), ctypes.byref(h))
+        if rc:
+            raise GpzError(rc, "gpz_hybrid_create")
+        self._h = h
+
+    def chunk(self, data) -> bytes:
+        a = _u8(data)
+        cap = self.L.gpz_bound(a.size)
+        out = np.empty(cap, dtype=np.uint8)
+        n = ctypes.c_size_t()
+        rc = self.L.gpz_hybrid_chunk(self._h, _p(a), a.size, _p(out), cap, ctypes.byref(n))
+        if rc:
+            raise GpzError(rc, "gpz_hybrid_chunk")
+        return out[:n.value].tobytes()
+
+    def stats(self):
+        """(chunks the CPU took, chunks the GPU took)."""
+        c, g = ctypes.c_uint64(), ctypes.c_uint64()
+        self.L.gpz_hybrid_stats(self._h, ctypes.byref(c), ctypes.byref(g))
+        return c.value, g.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.L.gpz_hybrid_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
 class Writer:
     """ParallelChunkedWriter over the library (gpz_writer_*): a file-like
-    object whose bytes are cut into `chunk_size` chunks, compressed `max_in_flight`
-    at a time on the writer's thread, and written as gzip members, in order,
-    to `dst` (anything with a write method).  With `ctx` the chunks go
-    through the device; with `chunk_fn` (bytes -> gzip bytes) through that
-    function instead, as the reference's writer takes any ChunkFn.
-    flush() does not cut a chunk; close() writes the last partial chunk and
-    raises the first error the writer met."""
+    object whose bytes are cut into `chunk_size` chunks and written as gzip
+    members, in order, to `dst` (anything with a write method).  With `ctx`
+    the chunks go through the device, `max_in_flight` at a time as one batch
+    on the writer's thread; with `chunk_fn` (bytes -> gzip bytes) through
+    that function instead, as the reference's writer takes any ChunkFn, and
+    with `hybrid` (a Hybrid) through the hybrid CPU + GPU chunk function; in
+    both, up to `max_in_flight` chunk calls run at once on the writer's
+    worker threads.  flush() does not cut a chunk; close() writes the last
+    partial chunk and raises the first error the writer met."""
 
-    def __init__(self, dst, ctx: "Context" = None, chunk_fn=None, chunk_size: int = 2 << 20, max_in_flight: int = 16):
-        if (ctx is None) == (chunk_fn is None):
-            raise ValueError("give exactly one of ctx and chunk_fn")
+    def __init__(self, dst, ctx: "Context" = None, chunk_fn=None, chunk_size: int = 2 << 20, max_in_flight: int = 16,
+                 hybrid: "Hybrid" = None):
+        if sum(x is not None for x in (ctx, chunk_fn, hybrid)) != 1:
+            raise ValueError("give exactly one of ctx, chunk_fn and hybrid")
         self.L = load()
         self._dst = dst
         self._err = None
@@ -434,9 +552,16 @@ class Writer:
 
         self._sink = SINK_FN(sink)  # kept alive with the writer
         self._chunk = CHUNK_FN(chunk)
+        self._hybrid = hybrid
         h = ctypes.c_void_p()
         if ctx is not None:
             rc = self.L.gpz_writer_open(ctx._h, chunk_size, max_in_flight, self._sink, None, ctypes.byref(h))
+        elif hybrid is not None:
+            # the library's own chunk function: no Python in the chunk calls
+            fn = CHUNK_FN(ctypes.cast(self.L.gpz_hybrid_chunk, ctypes.c_void_p).value)
+            self._chunk = fn
+            rc = self.L.gpz_writer_open_fn(fn, hybrid._h, chunk_size, max_in_flight, self._sink, None,
+                                           ctypes.byref(h))
         else:
             rc = self.L.gpz_writer_open_fn(self._chunk, None, chunk_size, max_in_flight, self._sink, None,
                                            ctypes.byref(h))

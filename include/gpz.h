@@ -39,13 +39,13 @@ extern "C" {
 /* Status codes. */
 #define GPZ_OK 0
 #define GPZ_E_NOMEM 1       /* device or pinned allocation failed */
-#define GPZ_E_ADMISSION 2   /* request does not fit the device pool cap */
-#define GPZ_E_TIMEOUT 3     /* a bounded device wait expired */
+#define GPZ_E_ADMISSION 2   /* request does not fit the device pool cap (now, or at all) */
+#define GPZ_E_TIMEOUT 3     /* the device did not finish within the context's wait limit */
 #define GPZ_E_CUDA 4        /* CUDA runtime error */
 #define GPZ_E_ARG 5         /* invalid argument */
 #define GPZ_E_SPACE 6       /* output buffer too small */
 #define GPZ_E_INTERNAL 7    /* device self-check failed (bit plan mismatch) */
-#define GPZ_E_BUSY 8        /* serving queue full, retry later */
+#define GPZ_E_BUSY 8        /* too many serving requests outstanding: poll some, then retry */
 #define GPZ_E_PENDING 9     /* ticket not finished yet */
 #define GPZ_E_DATA 10       /* gzip input this path cannot split or decode (use a serial decoder) */
 #define GPZ_E_SINK 11       /* a writer's sink or chunk function reported an error */
@@ -61,6 +61,7 @@ typedef struct gpz_config {
                               passes that overlap upload, compute and download */
     int streams;           /* reserved (0) */
     int flags;             /* GPZ_FLAG_* */
+    int wait_ms;           /* bound of every wait of a calling thread for the device, ms (0: 60000) */
 } gpz_config;
 
 #define GPZ_FLAG_NO_GRAPHS 1    /* launch kernels directly instead of per-bucket CUDA graphs */
@@ -83,6 +84,14 @@ typedef struct gpz_out {
     int status;          /* GPZ_OK or an error for this item */
 } gpz_out;
 
+/* Waits.  A call that waits for the device (every compress and inflate
+ * call, and the completion of serving batches) polls for at most the
+ * context's wait limit and then returns GPZ_E_TIMEOUT instead of blocking
+ * without end.  The work it gave up on may still run and still write the
+ * call's output buffers; the context's next call first waits (again within
+ * the limit) for that work, and only then reuses the buffers.  Serving
+ * requests of a timed-out batch complete with GPZ_E_TIMEOUT. */
+
 /* Fill *cfg with defaults (device 0, 131072-byte members). */
 GPZ_API void gpz_config_default(gpz_config* cfg);
 
@@ -90,6 +99,11 @@ GPZ_API void gpz_config_default(gpz_config* cfg);
  * GpuBackend::try_init (gpu.rs:125-167). */
 GPZ_API int gpz_create(const gpz_config* cfg, gpz_ctx** out);
 GPZ_API void gpz_destroy(gpz_ctx* ctx);
+
+/* Change the context's wait limit (ms, >= 0).  0 gives up at once unless
+ * the device has already finished: a call then returns GPZ_E_TIMEOUT
+ * whenever its work is still running when it first checks. */
+GPZ_API int gpz_set_wait_ms(gpz_ctx* ctx, int wait_ms);
 
 /* Worst-case output size of one compress call on n input bytes with
  * 131072-byte members; gpz_bound_ctx uses the context's member size. */
@@ -138,9 +152,11 @@ GPZ_API int gpz_debug_chunk(gpz_ctx* ctx, const uint8_t* in, size_t n, uint32_t*
  * arrive while others are on the device join the next batch as soon as a
  * pipeline slot frees; requests of at most 1 MiB go first.  A request whose
  * bytes would push the queued and in-flight total past the pool cap is
- * rejected with GPZ_E_BUSY.  gpz_poll returns GPZ_E_PENDING until the stream
- * is ready (wait_ms > 0 blocks up to that long), GPZ_E_SPACE (result kept)
- * if o->out_cap is short; the result is copied into o->out. */
+ * rejected with GPZ_E_ADMISSION; while 1,048,576 requests are submitted and
+ * not yet polled, gpz_submit returns GPZ_E_BUSY.  gpz_poll returns
+ * GPZ_E_PENDING until the stream is ready (wait_ms > 0 blocks up to that
+ * long), GPZ_E_SPACE (result kept) if o->out_cap is short; the result is
+ * copied into o->out. */
 GPZ_API int gpz_submit(gpz_ctx* ctx, const gpz_desc* d, uint64_t* ticket);
 /* As gpz_submit, without the copy: the caller keeps d->in unchanged and
  * alive until gpz_poll has returned the result. */
@@ -273,11 +289,13 @@ GPZ_API int gpz_stage_times(gpz_ctx* ctx, float* ms);
  * around the archive file (crates/gpzip-core/src/archive/pack.rs:144-176):
  * bytes written are cut into chunk_size chunks, the chunks are compressed
  * into independent gzip members, and the members reach `sink` in input
- * order.  Up to max_in_flight chunks are compressed together as one batch
- * on an internal thread while the caller fills the next batch.
+ * order.  With a device context, up to max_in_flight chunks are compressed
+ * together as one batch on an internal thread while the caller fills the
+ * next batch.
  *
  *  - sink(user, buf, n) returns 0 on success; it is called from the
- *    internal thread, never concurrently, and with members in order.
+ *    writer's internal threads, never concurrently, and with members in
+ *    order.
  *  - gpz_writer_flush does not cut the current partial chunk (tar calls
  *    flush between entries; parallel.rs:207-213) and waits for nothing.
  *  - gpz_writer_finish compresses the partial chunk, waits for every batch
@@ -290,7 +308,13 @@ GPZ_API int gpz_stage_times(gpz_ctx* ctx, float* ms);
  * gpz_writer_open compresses with ctx (gpz_compress_batch).
  * gpz_writer_open_fn compresses each chunk with fn(fn_user, in, n, out,
  * out_cap, &out_len) instead (out_cap = gpz_bound(n); nonzero return is an
- * error): a caller-supplied ChunkFn, as the reference's writer takes any. */
+ * error): a caller-supplied ChunkFn, as the reference's writer takes any.
+ * Each full chunk is handed at once to one of max_in_flight worker threads
+ * (at most 1024), so up to max_in_flight calls of fn run concurrently, as
+ * the reference runs one rayon task per chunk (parallel.rs:91-129); fn must
+ * be safe to call from several threads.  A failed chunk ends the stream:
+ * the chunks before it (in input order) are written, it and the chunks
+ * after it are not. */
 typedef struct gpz_writer gpz_writer;
 typedef int (*gpz_sink_fn)(void* user, const uint8_t* buf, size_t n);
 typedef int (*gpz_chunk_fn)(void* user, const uint8_t* in, size_t n, uint8_t* out, size_t out_cap,
@@ -303,6 +327,55 @@ GPZ_API int gpz_writer_write(gpz_writer* w, const uint8_t* buf, size_t n);
 GPZ_API int gpz_writer_flush(gpz_writer* w);
 GPZ_API int gpz_writer_finish(gpz_writer* w);
 GPZ_API void gpz_writer_close(gpz_writer* w);
+
+/* ---- Hybrid CPU + GPU chunk function (`--backend auto`) ----
+ *
+ * The reference's HybridGzipCompressor (crates/gpzip-cli/src/hybrid.rs:
+ * 103-147), the default backend's caller of the GPU path: a composed chunk
+ * function under which every chunk goes to whichever device is free.
+ *  - The first warmup_chunks chunks (the reference: 4) always go to the CPU,
+ *    so a small input never pays for the device context, which is made on
+ *    the first chunk that may use the GPU (unless cfg.ctx supplies one).
+ *    If it cannot be made, every chunk goes to the CPU.
+ *  - After that a chunk takes one of gpu_permits GPU permits if one is free
+ *    (decrement-if-positive, hybrid.rs:150-163) and runs gpz_compress_chunk
+ *    on the context; otherwise it runs the CPU chunk function.  A GPU
+ *    chunk's error is returned as is, with no CPU retry (hybrid.rs:131-135).
+ *  - The CPU chunk function is cfg.cpu_fn, or gpz_cpu_gzip_chunk at
+ *    cfg.level: one zlib gzip member per chunk, as GzipCompressor::chunk_fn
+ *    (crates/gpzip-codec-cpu/src/compress.rs:52-59) writes with flate2.
+ * Use gpz_hybrid_chunk as a writer's chunk function (gpz_writer_open_fn
+ * with fn_user = the gpz_hybrid), with max_in_flight = the CPU workers +
+ * gpu_permits, as the reference sizes its writer (hybrid.rs:139-146).  It is
+ * safe to call from many threads.  gpz_hybrid_stats counts the chunks each
+ * device took.  Destroy the hybrid after every writer using it is closed. */
+typedef struct gpz_hybrid gpz_hybrid;
+typedef struct gpz_hybrid_config {
+    gpz_ctx* ctx;          /* device context to use (NULL: made on the first GPU chunk on `device`) */
+    int device;
+    int level;             /* zlib level of CPU chunks, 0-9 (default 5) */
+    size_t gpu_permits;    /* concurrent GPU chunk calls (default 1, the reference's; 0: CPU only) */
+    size_t warmup_chunks;  /* leading chunks kept on the CPU (default 4) */
+    gpz_chunk_fn cpu_fn;   /* NULL: gpz_cpu_gzip_chunk at `level` */
+    void* cpu_user;
+    gpz_chunk_fn gpu_fn;   /* NULL: gpz_compress_chunk on the context; else this function runs the
+                              chunks that hold a GPU permit (no context is made) */
+    void* gpu_user;
+} gpz_hybrid_config;
+GPZ_API void gpz_hybrid_config_default(gpz_hybrid_config* cfg);
+GPZ_API int gpz_hybrid_create(const gpz_hybrid_config* cfg, gpz_hybrid** out);
+/* A gpz_chunk_fn; user is the gpz_hybrid. */
+GPZ_API int gpz_hybrid_chunk(void* user, const uint8_t* in, size_t n, uint8_t* out, size_t out_cap,
+                             size_t* out_len);
+GPZ_API int gpz_hybrid_stats(const gpz_hybrid* h, uint64_t* cpu_chunks, uint64_t* gpu_chunks);
+GPZ_API void gpz_hybrid_destroy(gpz_hybrid* h);
+
+/* The CPU chunk function: one gzip member of the whole chunk, zlib at the
+ * level *(const int*)level (NULL: 5), the gzip-cpu path of the reference
+ * (compress.rs:52-59).  GPZ_E_SPACE when out_cap is too small
+ * (gpz_bound(n) always suffices). */
+GPZ_API int gpz_cpu_gzip_chunk(void* level, const uint8_t* in, size_t n, uint8_t* out, size_t out_cap,
+                               size_t* out_len);
 
 #ifdef __cplusplus
 }

@@ -22,7 +22,7 @@
 
 /* ------------------------------------------------------------------ hash3 */
 
-/* lz77_hash_build.wgsl:36-43 (duplicated at lz77_hash_lookup.wgsl:86-93). */
+/* lz77_hash_build.wgsl:36-43 (duplicated at lz77_hash_lookup.wgsl:32-39). */
 uint32_t gpzo_hash3(const uint8_t* in, uint32_t p) {
     uint32_t x = ((uint32_t)in[p] << 16) | ((uint32_t)in[p + 1] << 8) | (uint32_t)in[p + 2];
     return (x * 0x9E3779B1u) >> (32u - HASH_BITS);
@@ -30,7 +30,7 @@ uint32_t gpzo_hash3(const uint8_t* in, uint32_t p) {
 
 /* --------------------------------------------------------- build + lookup */
 
-/* lz77_hash_lookup.wgsl:99-121 (try_candidate).  Returns the match length if
+/* lz77_hash_lookup.wgsl:45-67 (try_candidate).  Returns the match length if
  * it beats cur_best, else 0; *dist receives the distance. */
 static uint32_t try_candidate(const uint8_t* in, uint32_t n, uint32_t raw, uint32_t p,
                               uint32_t cur_best, uint32_t* dist) {
@@ -56,7 +56,7 @@ static uint32_t try_candidate(const uint8_t* in, uint32_t n, uint32_t raw, uint3
 
 /* lz77_hash.rs:306-453 (match_find) with the two shaders it dispatches:
  * the reset (lz77_hash.rs:409-415), build (lz77_hash_build.wgsl:45-54) and
- * lookup (lz77_hash_lookup.wgsl:123-173).  The dense [hash][segment] tables
+ * lookup (lz77_hash_lookup.wgsl:69-119).  The dense [hash][segment] tables
  * and the walk over every segment back to 0 are kept as the reference has
  * them; the CUDA path bounds the walk at nine segments and must agree. */
 int gpzo_match_find(const uint8_t* in, uint32_t n, uint32_t* pp) {

@@ -44,7 +44,7 @@ def hash3(b: bytes, p: int) -> int:
 def match_find(b: bytes) -> list[int]:
     """Per-position packed tokens (length<<16 | dist-or-byte).
 
-    Build: gpu/lz77_hash_build.wgsl:45-54; lookup: gpu/lz77_hash_lookup.wgsl:99-173.
+    Build: gpu/lz77_hash_build.wgsl:45-54; lookup: gpu/lz77_hash_lookup.wgsl:45-119.
     The [hash][segment] tables are dicts whose missing keys read as the
     sentinels (0xFFFFFFFF for oldest, 0 for newest), which is what the reset at
     gpu/lz77_hash.rs:584-587 leaves in the dense tables.

@@ -196,7 +196,7 @@ def test_serving_pending_space_and_admission():
     with native.Context(pool_bytes=1 << 20) as c:
         with pytest.raises(native.GpzError) as e:
             c.submit(b"z" * (2 << 20))
-        assert e.value.status == native.GPZ_E_BUSY
+        assert e.value.status == native.GPZ_E_ADMISSION
         st = c.serve_stats()
         assert st["rejected"] == 1
 
@@ -228,3 +228,59 @@ def test_device_writer_matches_the_oracle(ctx):
     want = b"".join(O.gzip_chunk(data[i:i + (2 << 20)], 131072, threads=8) for i in range(0, len(data), 2 << 20))
     assert out.getvalue() == want
     assert bytes(ctx.inflate(out.getvalue())) == data
+
+
+def test_bounded_wait_times_out_and_the_context_recovers():
+    """Every host wait for the device is bounded by the context's wait limit.
+    With a limit of 0 a call whose device work is still running gives up with
+    GPZ_E_TIMEOUT; the next call waits for that work before it reuses the
+    buffers, and its bytes are the same as ever."""
+    data = W.logs(96 << 20, seed=12)
+    items = [np.ascontiguousarray(data[i:i + (2 << 20)]) for i in range(0, data.size, 2 << 20)]
+    with native.Context() as c:
+        want = c.compress_batch(items)
+        c.set_wait_ms(0)
+        with pytest.raises(native.GpzError) as e:
+            c.compress_batch(items)
+        assert e.value.status == native.GPZ_E_TIMEOUT
+        c.set_wait_ms(60_000)
+        assert c.compress_batch(items) == want
+        assert c.compress_chunk(items[0]) == want[0]
+
+
+def test_hybrid_writer_on_the_device(ctx):
+    """The `--backend auto` composition on the device: the hybrid chunk
+    function in a writer with CPU workers + GPU permits in flight.  Every
+    chunk the GPU took equals the oracle's bytes, every CPU chunk is zlib's
+    level-5 member, the stream is in input order and gzip -t accepts it."""
+    import gzip
+    import io
+    import subprocess
+    import tempfile
+    data = W.logs(40 << 20, seed=31).tobytes()
+    chunk = 2 << 20
+    with native.Hybrid(ctx=ctx, gpu_permits=8, warmup_chunks=4) as h:
+        out = io.BytesIO()
+        with native.Writer(out, hybrid=h, chunk_size=chunk, max_in_flight=8 + 8) as w:
+            for i in range(0, len(data), 1 << 20):
+                w.write(data[i:i + (1 << 20)])
+        cpu, gpu = h.stats()
+    got = out.getvalue()
+    assert cpu >= 4 and gpu >= 1 and cpu + gpu == len(data) // chunk
+    pos, on_gpu = 0, 0
+    for i in range(0, len(data), chunk):
+        c = data[i:i + chunk]
+        a = O.gzip_chunk(c, 131072, threads=8)
+        if got.startswith(a, pos):
+            pos += len(a)
+            on_gpu += 1
+        else:
+            b = native.cpu_gzip_chunk(c, 5)
+            assert got.startswith(b, pos)
+            pos += len(b)
+    assert pos == len(got) and on_gpu == gpu
+    assert gzip.decompress(got) == data
+    with tempfile.NamedTemporaryFile(suffix=".gz") as f:
+        f.write(got)
+        f.flush()
+        subprocess.run(["gzip", "-t", f.name], check=True)

@@ -1,9 +1,24 @@
 """The named workloads at their full sizes (GPU), through the batched host
-API with 2 MiB chunks: the 8 MiB text stream byte for byte against the
-oracle; the 64 MiB logs tar and the 272 MiB mixed binary stream through
-size-independent properties (every member inflates back to its chunk, the
-streams are exactly the concatenation of valid gzip members, sampled chunks
-equal the oracle's)."""
+API with 2 MiB chunks, compared chunk by chunk with the oracle's output.
+
+The oracle's per-chunk SHA-256 digests are committed in
+tests/golden/config_digests.json (made by tests/golden/make_config_digests.py,
+which checks that every oracle chunk inflates back to its input).  Every
+chunk of every set is compared, not a sample:
+
+* text     8 MiB, 4 chunks, 128 KiB members;
+* logs     the 64 MiB log ustar stream, 33 chunks;
+* binary   272 MiB mixed binary, 136 chunks;
+* uneven   the 1,000-file mix, 1,245 chunks (each file cut on its own);
+* member2m text, logs and binary inputs of 3 x 2 MiB + 12,345 bytes with
+           2 MiB members (whole-chunk mode).
+
+Each stream must also be a concatenation of valid gzip members that inflate
+back to the chunk (zlib), a property that holds whatever the digests say.
+"""
+import hashlib
+import json
+import os
 import zlib
 
 import numpy as np
@@ -11,10 +26,10 @@ import pytest
 
 from gpzip_b200 import native
 from gpzip_b200 import workloads as W
-from oracle import oracle as O
 
-pytestmark = pytest.mark.gpu
 CHUNK = 2 << 20
+HERE = os.path.dirname(os.path.abspath(__file__))
+DIGESTS = json.load(open(os.path.join(HERE, "golden", "config_digests.json")))["sets"]
 
 
 def chunks_of(data):
@@ -35,24 +50,71 @@ def members(stream: bytes):
     return out
 
 
-def test_text_8mib_exact(ctx):
-    data = W.config_text()
-    items = chunks_of(data)
-    got = ctx.compress_batch(items)
-    for it, g in zip(items, got):
-        assert g == O.gzip_chunk(it.tobytes(), 131072, threads=8)
-
-
-@pytest.mark.parametrize("name", ["logs", "binary"])
-def test_full_config_properties(ctx, name):
-    data = W.config_logs_tar() if name == "logs" else W.config_binary()
-    items = chunks_of(data)
-    got = ctx.compress_batch(items)
-    rng = np.random.default_rng(5)
-    sample = set(int(x) for x in rng.choice(len(items), size=3, replace=False)) | {len(items) - 1}
+def check_set(got, items, want, member):
+    assert len(got) == len(items) == want["chunks"]
+    bad = []
     for k, (it, g) in enumerate(zip(items, got)):
-        ms = members(bytes(g))
-        assert len(ms) == max(1, -(-it.size // 131072))
+        g = bytes(g)
+        if hashlib.sha256(g).hexdigest() != want["chunk_sha256"][k]:
+            bad.append((k, len(g), want["gzip_len"][k]))
+        ms = members(g)
+        assert len(ms) == max(1, -(-it.size // member))
         assert b"".join(ms) == it.tobytes()
-        if k in sample:
-            assert g == O.gzip_chunk(it.tobytes(), 131072, threads=8)
+    assert not bad, f"{len(bad)} of {len(items)} chunks differ from the oracle (chunk, got len, want len): {bad[:8]}"
+
+
+def uneven_chunks():
+    items = []
+    for _, _, data in W.uneven_files(1000, seed=3):
+        items.extend(chunks_of(data))
+    return items
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["text", "logs", "binary"])
+def test_named_config_every_chunk(ctx, name):
+    data = {"text": W.config_text, "logs": W.config_logs_tar, "binary": W.config_binary}[name]()
+    want = DIGESTS[name]
+    assert W.digest(data) == want["input_sha256"], "workload generator drifted"
+    items = chunks_of(data)
+    check_set(ctx.compress_batch(items), items, want, 131072)
+
+
+@pytest.mark.gpu
+def test_uneven_mix_every_chunk(ctx):
+    items = uneven_chunks()
+    want = DIGESTS["uneven"]
+    assert hashlib.sha256(b"".join(W.digest(x).encode() for x in items)).hexdigest() == want["input_sha256"]
+    check_set(ctx.compress_batch(items), items, want, 131072)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["text", "logs", "binary"])
+def test_member2m_every_chunk(name):
+    n = 3 * CHUNK + 12_345
+    data = {"text": lambda: W.text(n, seed=7), "logs": lambda: W.logs(n, seed=8),
+            "binary": lambda: W.binary(n, seed=9)}[name]()
+    want = DIGESTS["member2m"][name]
+    assert W.digest(data) == want["input_sha256"]
+    items = chunks_of(data)
+    with native.Context(member_bytes=2 << 20) as c2:
+        check_set(c2.compress_batch(items), items, want, 2 << 20)
+
+
+def test_digest_fixture_pinned_on_cpu():
+    """The committed digests are the oracle's: the first text chunk and the
+    2 MiB-member binary tail are recomputed here (CPU, under a second)."""
+    from oracle import oracle as O
+    data = W.config_text()
+    assert W.digest(data) == DIGESTS["text"]["input_sha256"]
+    first = data[:CHUNK]
+    assert hashlib.sha256(O.gzip_chunk(first, 131072, threads=4)).hexdigest() == DIGESTS["text"]["chunk_sha256"][0]
+    n = 3 * CHUNK + 12_345
+    tail = W.binary(n, seed=9)[3 * CHUNK:]
+    assert (hashlib.sha256(O.gzip_chunk(tail, 2 << 20)).hexdigest()
+            == DIGESTS["member2m"]["binary"]["chunk_sha256"][-1])
+    for name in ("text", "logs", "binary", "uneven"):
+        s = DIGESTS[name]
+        assert len(s["chunk_sha256"]) == len(s["gzip_len"]) == s["chunks"]
+    assert DIGESTS["logs"]["chunks"] == 33 and DIGESTS["binary"]["chunks"] == 136
+    assert DIGESTS["uneven"]["chunks"] == 1245

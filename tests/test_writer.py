@@ -112,3 +112,54 @@ def test_tar_stream_packs_and_unpacks(tmp_path):
     with tarfile.open(fileobj=io.BytesIO(raw), mode="r:") as tr:
         got = {m.name: tr.extractfile(m).read() for m in tr.getmembers()}
     assert got == files
+
+
+def test_chunk_calls_run_concurrently():
+    """Up to max_in_flight chunk calls run at once (the reference spawns one
+    rayon task per chunk, parallel.rs:91-129), and the members still reach
+    the sink in input order."""
+    import threading
+    import time
+    lock = threading.Lock()
+    live = [0, 0]  # now, peak
+
+    def slow(b):
+        with lock:
+            live[0] += 1
+            live[1] = max(live[1], live[0])
+        time.sleep(0.05)  # releases the GIL: calls overlap if the writer lets them
+        with lock:
+            live[0] -= 1
+        return oracle_fn(b)
+
+    data = W.text(8 * CHUNK + 99, seed=7).tobytes()
+    out = io.BytesIO()
+    with native.Writer(out, chunk_fn=slow, chunk_size=CHUNK, max_in_flight=4) as w:
+        w.write(data)
+    assert out.getvalue() == expected(data, CHUNK)
+    assert 1 < live[1] <= 4
+
+
+def test_failed_chunk_ends_the_stream_in_input_order():
+    """With calls in flight together, the chunks before the failed one are
+    written and nothing from it on, whatever order the calls finish in."""
+    import time
+    data = W.logs(8 * CHUNK, seed=8).tobytes()
+    bad = data[3 * CHUNK:4 * CHUNK]
+
+    def fn(b):
+        if b == bad:
+            raise RuntimeError("chunk 3 failed")
+        if b == data[:CHUNK]:
+            time.sleep(0.2)  # the first chunk finishes last
+        return oracle_fn(b)
+
+    out = io.BytesIO()
+    w = native.Writer(out, chunk_fn=fn, chunk_size=CHUNK, max_in_flight=8)
+    with pytest.raises(native.GpzError) as e:
+        try:
+            w.write(data)  # may already report the failure
+        finally:
+            w.close()  # waits for the chunks in flight, then reports it
+    assert e.value.status == native.GPZ_E_SINK
+    assert out.getvalue() == expected(data[:3 * CHUNK], CHUNK)
