@@ -53,11 +53,13 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="logs", choices=["logs", "text", "binary", "uneven"])
-    ap.add_argument("--serve-seconds", type=float, default=1.5,
+    ap.add_argument("--serve-seconds", type=float, default=60.0,
                     help="seconds per arrival rate of the serving measurement (0: skip)")
     ap.add_argument("--serve-rates", default="1000,10000,50000")
     ap.add_argument("--serve-only", action="store_true", help="run only the serving measurement")
-    ap.add_argument("--cpu-sample-mib", type=int, default=8)
+    ap.add_argument("--cpu-sample-mib", type=int, default=0,
+                    help="MiB of the workload the CPU port times per step (0: all of it)")
+    ap.add_argument("--no-configs", action="store_true", help="skip the per-config (text, binary) lines")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baselines (quick runs)")
     ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-file batched vs plain measurement")
     ap.add_argument("--device-only", action="store_true",
@@ -140,6 +142,16 @@ class Clocks:
                 "samples": len(sm)}
 
 
+def chunk_parity(outs, workload: str):
+    """(chunks whose gzip stream equals the oracle's, chunks): the oracle's
+    per-chunk SHA-256 digests are committed with the tests
+    (tests/golden/config_digests.json)."""
+    import hashlib
+    want = json.load(open(os.path.join(ROOT, "tests", "golden", "config_digests.json")))["sets"][workload]
+    got = [hashlib.sha256(bytes(x)).hexdigest() for x in outs]
+    return sum(int(a == b) for a, b in zip(got, want["chunk_sha256"])), want["chunks"]
+
+
 def inflate_all(gz: bytes) -> bytes:
     import zlib
     out, rest = b"", gz
@@ -151,9 +163,10 @@ def inflate_all(gz: bytes) -> bytes:
 
 
 def cpu_port_rate(data: np.ndarray, sample_mib: int, threads: int):
-    """The CPU port of the reference GPU path (oracle) on a bounded sample."""
+    """The CPU port of the reference GPU path (oracle) on the workload, or on
+    its first sample_mib MiB when sample_mib > 0."""
     from oracle import oracle as O
-    sample = data[: min(data.size, sample_mib << 20)]
+    sample = data[: min(data.size, sample_mib << 20)] if sample_mib > 0 else data
     spans = W.chunk_spans(sample.size, CHUNK)
     t0 = time.perf_counter()
     outs = [O.gzip_chunk(sample[o:o + n], MEMBER, threads=threads) for o, n in spans]
@@ -209,7 +222,9 @@ def run_uneven(ctx, args, stream):
     e1.synchronize()
     plain = total / (e0.elapsed_time(e1) / 1e3) / 1e9
     same = all(a == b for a, b in zip(outs, plain_outs))
+    eq, tot = chunk_parity(outs, "uneven")
     return {"files": 1000, "chunks": len(items), "bytes": int(total), "batched_gbs": round(batched, 4),
+            "parity": f"ok ({eq}/{tot} chunks equal the oracle's)" if eq == tot else f"FAILED ({eq}/{tot} chunks)",
             "plain_gbs": round(plain, 4), "batched_over_plain": round(batched / plain, 3),
             "batched_ms": round(min(times), 3), "outputs_identical": same, "host_ms_per_step": host,
             "ratio": round(sum(len(o) for o in outs) / total, 5)}
@@ -425,8 +440,187 @@ def run_serving(device: int, seconds: float, rates, warm_seconds: float = 0.3):
     return results
 
 
+def gzip_check(outs, data, workload_name):
+    """Every member inflates back to its chunk; every chunk equals the
+    oracle's committed digest."""
+    gz_all = b"".join(bytes(x) for x in outs)
+    ok = inflate_all(gz_all) == data.tobytes()
+    same, total = chunk_parity(outs, workload_name)
+    return (f"ok ({same}/{total} chunks equal the oracle's; every member inflates)" if ok and same == total
+            else f"FAILED (inflate={ok}, chunks equal to the oracle's: {same}/{total})")
+
+
+def device_measure(ctx, data, workload_name, steps, warmup, stream, flush, local, rank, barrier, clocks=False,
+                   check=gzip_check):
+    """gpz_compress_device on the workload resident in HBM: one checked
+    pass, `warmup` untimed passes, then `steps` passes timed with CUDA
+    events on the launching stream, L2 flushed before each."""
+    import torch
+    from gpzip_b200 import native
+    spans = W.chunk_spans(data.size, CHUNK)
+    offs, lens, pos = [], [], 0
+    for o, n in spans:
+        offs.append(pos)
+        lens.append(n)
+        pos += (n + 15) // 16 * 16
+    packed = np.zeros(pos + 64, dtype=np.uint8)
+    for (o, n), po in zip(spans, offs):
+        packed[po:po + n] = data[o:o + n]
+    d_in = torch.from_numpy(packed).to(f"cuda:{local}")
+    del packed
+    out_cap = ctx.bound(data.size) + 64 * len(spans)
+    d_out = torch.empty(out_cap, dtype=torch.uint8, device=f"cuda:{local}")
+
+    def step():
+        return ctx.compress_device(d_in.data_ptr(), offs, lens, d_out.data_ptr(), out_cap, stream.cuda_stream)
+
+    oo = step()
+    parity = "unchecked"
+    if rank == 0:
+        host = d_out[:oo[-1]].cpu().numpy().copy()
+        ctx.frame_host(host)
+        gz_all = host.tobytes()
+        parity = check([gz_all[a:b] for a, b in zip(oo[:-1], oo[1:])], data, workload_name)
+        del host, gz_all
+    ratio = oo[-1] / data.size
+    for _ in range(warmup):
+        step()
+    barrier()
+    clk = None
+    if clocks:
+        sampler = Clocks(local)
+        sampler.start()
+    times, stages = [], np.zeros(len(native.STAGE_NAMES))
+    for _ in range(steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        e1.synchronize()
+        times.append(e0.elapsed_time(e1))
+        stages += np.array(ctx.stage_times())
+    barrier()
+    if clocks:
+        clk = sampler.stop()
+    out = {"total_ms": float(sum(times)), "stage_ms": stages / steps, "ratio": ratio, "parity": parity,
+           "launches": ctx.last_launches(), "clocks": clk}
+    del d_in, d_out
+    torch.cuda.empty_cache()
+    return out
+
+
+def e2e_measure(ectx, data, workload_name, steps, warmup, stream, local, rank, world, barrier, dist,
+                check=None):
+    """gpz_compress_batch with host buffers: the step's input in page-locked
+    host memory (the library uploads it directly), the caller's output
+    buffer reused across calls; copies inside the timed region."""
+    import torch
+    spans = W.chunk_spans(data.size, CHUNK)
+    host_in = torch.empty(data.size, dtype=torch.uint8, pin_memory=True).numpy()
+    host_in[:] = data
+    host_chunks = [host_in[o:o + n] for o, n in spans]
+    buf = np.zeros(ectx.batch_bound(host_chunks), dtype=np.uint8)
+    for _ in range(warmup):
+        ectx.compress_batch(host_chunks, out=buf)
+    barrier()
+    e_times = []
+    out_bytes = 0
+    outs = None
+    ectx.host_times(reset=True)
+    for _ in range(steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        outs = ectx.compress_batch(host_chunks, out=buf)
+        e1.record(stream)
+        e1.synchronize()
+        e_times.append(e0.elapsed_time(e1))
+        out_bytes = sum(len(x) for x in outs)
+    et = torch.tensor([sum(e_times)], device=f"cuda:{local}", dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(et, op=dist.ReduceOp.MAX)
+    value = data.size * len(e_times) * world / (float(et.item()) / 1e3) / 1e9
+    host = {k: round(v / max(1, len(e_times)), 3) for k, v in ectx.host_times().items()}
+    par = None
+    if rank == 0 and check is not None:
+        par = check(outs, data, workload_name)
+    elif rank == 0:
+        same, total = chunk_parity(outs, workload_name)
+        par = f"ok ({same}/{total} chunks)" if same == total else f"FAILED ({same}/{total} chunks)"
+    gz = b"".join(bytes(x) for x in outs)
+    return {"value": round(value, 4), "unit": "GB/s", "h2d_bytes_per_step": int(data.size),
+            "d2h_bytes_per_step": int(out_bytes), "api": "gpz_compress_batch (host buffers; inputs page-locked)",
+            "host_ms_per_step": host, "parity": par, "_gz": gz}
+
+
+def roofline_of(kernel: str, kernel_ms: float, in_bytes: int, ratio: float, clk) -> dict:
+    """The dominant stage against the measured HBM peak: algorithmic bytes
+    (1 + ratio per input byte) over its event-timed duration; its committed
+    ncu DRAM traffic and warp instructions scaled to this input; and the
+    share of the SMs' issue slots those instructions fill at the sampled
+    clock (148 SMs x 4 schedulers, one warp instruction per cycle each)."""
+    peak, peak_kind = measured_peaks()
+    algo = in_bytes * (1.0 + ratio)
+    achieved = algo / (kernel_ms / 1e3) / 1e9
+    tr = committed_traffic().get(kernel)
+    traffic = round(tr["dram_bytes_per_input_byte"] * in_bytes) if tr else None
+    r = {"bound": "hbm", "kernel": kernel, "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
+         "frac": round(achieved / peak, 5), "traffic": traffic, "peak_kind": peak_kind,
+         "algorithmic_bytes_per_launch": int(algo)}
+    if tr and tr.get("warp_inst_per_input_byte"):
+        mhz = (clk or {}).get("sm_mhz") or 1965.0
+        inst = tr["warp_inst_per_input_byte"] * in_bytes
+        r["issue_frac"] = round(inst / (148 * 4 * mhz * 1e6 * kernel_ms / 1e3), 4)
+        r["limiter"] = tr.get("limiter")
+    return r
+
+
+def hybrid_rate(ctx, data, rounds: int = 2):
+    """The `--backend auto` writer (gpz_hybrid in gpz_writer_open_fn): CPU
+    workers = host threads, 16 GPU permits on the device context, 2 MiB
+    chunks, 1 MiB writes; input GB/s, best of `rounds`, and the chunks each
+    device took."""
+    import time as _t
+    from gpzip_b200 import native
+
+    class Count:
+        n = 0
+
+        def write(self, b):
+            Count.n += len(b)
+
+    view = np.ascontiguousarray(data)
+    cpu_workers = os.cpu_count() or 1
+    best, split = None, None
+    for r in range(rounds + 1):
+        Count.n = 0
+        with native.Hybrid(ctx=ctx, gpu_permits=16, warmup_chunks=4) as h:
+            t0 = _t.perf_counter()
+            with native.Writer(Count(), hybrid=h, chunk_size=CHUNK, max_in_flight=cpu_workers + 16) as w:
+                for i in range(0, len(view), 1 << 20):
+                    w.write(view[i:i + (1 << 20)])
+            t = _t.perf_counter() - t0
+            if r and (best is None or t < best):
+                best, split = t, h.stats()
+    return {"value": round(len(view) / best / 1e9, 4), "unit": "GB/s", "out_bytes": Count.n,
+            "cpu_workers": cpu_workers, "gpu_permits": 16, "cpu_chunks": split[0], "gpu_chunks": split[1],
+            "ratio": round(Count.n / len(view), 5),
+            "what": "gpz_hybrid chunk function in the streaming writer: 1 MiB writes, 2 MiB chunks, wall clock"}
+
+
+def config_of(data, desc: str, world: int) -> dict:
+    """The bench line's config, the same for both arms."""
+    spans = W.chunk_spans(data.size, CHUNK)
+    return {"workload": desc, "bytes": int(data.size), "chunk_bytes": CHUNK, "member_bytes": MEMBER,
+            "members": sum(max(1, -(-n // MEMBER)) for _, n in spans), "level": 5,
+            "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}"}
+
+
 def run_reference(args, rank: int):
-    """--impl reference: the CPU port of the path on all host threads."""
+    """--impl reference: the CPU port of the path on all host threads, on the
+    whole workload every step (or its first --cpu-sample-mib MiB)."""
     if rank != 0:
         return
     data, desc = workload(args.workload)
@@ -445,9 +639,10 @@ def run_reference(args, rank: int):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(nbytes / (value * 1e9) * 1e3, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
         "data": "synthetic (seeded generators standing in for the reference's corpora)",
-        "config": {"workload": desc, "chunk_bytes": CHUNK, "member_bytes": MEMBER, "level": 5},
+        "config": config_of(data, desc, args.gpus),
         "cpu_baseline": {"value": round(value, 5), "unit": "GB/s", "cores": threads, "kind": "port",
-                         "sample": f"first {sample_mib} MiB of the workload per step, members on all host threads"},
+                         "sample": (f"first {sample_mib} MiB" if sample_mib > 0 else "the whole workload")
+                         + " per step, members on all host threads"},
         "e2e": {"value": round(value, 5), "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "ratio": round(ratio, 5),
     }
@@ -501,62 +696,14 @@ def main():
         return
 
     data, desc = workload(args.workload)
-    spans = W.chunk_spans(data.size, CHUNK)
-    offs, lens, pos = [], [], 0
-    for o, n in spans:
-        offs.append(pos)
-        lens.append(n)
-        pos += (n + 15) // 16 * 16
-    packed = np.zeros(pos + 64, dtype=np.uint8)
-    for (o, n), po in zip(spans, offs):
-        packed[po:po + n] = data[o:o + n]
-
-    ctx = native.Context(device=local, member_bytes=MEMBER, flags=native.GPZ_FLAG_STAGE_TIMING)
-    d_in = torch.from_numpy(packed).to(f"cuda:{local}")
-    out_cap = ctx.bound(data.size) + 64 * len(spans)
-    d_out = torch.empty(out_cap, dtype=torch.uint8, device=f"cuda:{local}")
-    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=f"cuda:{local}")
     stream = torch.cuda.current_stream()
-
-    def step():
-        return ctx.compress_device(d_in.data_ptr(), offs, lens, d_out.data_ptr(), out_cap, stream.cuda_stream)
-
-    # correctness of the device path on this workload: every member inflates
-    # back to its chunk, and one chunk is byte-compared with the oracle
-    oo = step()
-    host = d_out[:oo[-1]].cpu().numpy().copy()
-    ctx.frame_host(host)
-    parity = "unchecked"
-    if rank == 0:
-        from oracle import oracle as O
-        gz_all = host.tobytes()
-        ok = inflate_all(gz_all) == data.tobytes()
-        first = gz_all[oo[0]:oo[1]]
-        same = first == O.gzip_chunk(data[spans[0][0]:spans[0][0] + spans[0][1]], MEMBER, threads=8)
-        parity = "ok" if (ok and same) else f"FAILED (inflate={ok}, oracle_chunk0={same})"
-    ratio = oo[-1] / data.size
-
-    for _ in range(args.warmup):
-        step()
-    barrier()
-    clocks = Clocks(local)
-    clocks.start()
-    times, stages = [], np.zeros(len(native.STAGE_NAMES))
-    for _ in range(args.steps):
-        flush.zero_()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        step()
-        e1.record(stream)
-        e1.synchronize()
-        times.append(e0.elapsed_time(e1))
-        stages += np.array(ctx.stage_times())
-    barrier()
-    clk = clocks.stop()
-    launches = ctx.last_launches() * args.steps
-    total_ms = float(sum(times))
-    t = torch.tensor([total_ms], device=f"cuda:{local}", dtype=torch.float64)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=f"cuda:{local}")
+    ctx = native.Context(device=local, member_bytes=MEMBER, flags=native.GPZ_FLAG_STAGE_TIMING)
+    dev = device_measure(ctx, data, args.workload, args.steps, args.warmup, stream, flush, local, rank, barrier,
+                         clocks=True)
+    ratio, parity, clk = dev["ratio"], dev["parity"], dev["clocks"]
+    launches = dev["launches"] * args.steps
+    t = torch.tensor([dev["total_ms"]], device=f"cuda:{local}", dtype=torch.float64)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     max_ms = float(t.item())
@@ -565,53 +712,22 @@ def main():
     # end to end through the public host API (host buffers, copies inside),
     # on a context with the production settings (graphs, autotuned shapes)
     ectx = native.Context(device=local, member_bytes=MEMBER)
-    # the step's input in page-locked host memory, from which the library
-    # uploads directly (pageable inputs are staged through its own pinned
-    # buffers first)
-    host_in = torch.empty(data.size, dtype=torch.uint8, pin_memory=True).numpy()
-    host_in[:] = data
-    host_chunks = [host_in[o:o + n] for o, n in spans]
-    # the caller's output buffer, reused across calls as a writer's staging
-    # buffer would be (the library owns no host output memory)
-    e2e_buf = np.zeros(ectx.batch_bound(host_chunks), dtype=np.uint8)
-    for _ in range(0 if args.device_only else max(args.warmup, 2)):
-        ectx.compress_batch(host_chunks, out=e2e_buf)
-    barrier()
-    e_times = []
-    e2e_out = 0
-    ectx.host_times(reset=True)
-    for _ in range(1 if args.device_only else max(2, args.steps // 2)):
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        outs = ectx.compress_batch(host_chunks, out=e2e_buf)
-        e1.record(stream)
-        e1.synchronize()
-        e_times.append(e0.elapsed_time(e1))
-        e2e_out = sum(len(x) for x in outs)
-    et = torch.tensor([sum(e_times)], device=f"cuda:{local}", dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(et, op=dist.ReduceOp.MAX)
-    e2e_value = data.size * len(e_times) * world / (float(et.item()) / 1e3) / 1e9
-    e2e_host = {k: round(v / max(1, len(e_times)), 3) for k, v in ectx.host_times().items()}
+    e2e = e2e_measure(ectx, data, args.workload, 1 if args.device_only else max(2, args.steps // 2),
+                      0 if args.device_only else max(args.warmup, 2), stream, local, rank, world, barrier, dist)
+    spans = W.chunk_spans(data.size, CHUNK)
     inflate = None
     writer = None if args.device_only else writer_rate(ectx, data)
+    hybrid = None if (args.device_only or world > 1) else hybrid_rate(ectx, data)
     if not args.device_only:
-        gz_all = b"".join(bytes(x) for x in outs)
-        inflate = inflate_rates(ectx, gz_all, data.size)
+        inflate = inflate_rates(ectx, e2e.pop("_gz"), data.size)
+    e2e.pop("_gz", None)
     # pageable chunks, as a writer hands them over
     chunk_fn = None if args.device_only else chunk_fn_rate(ectx, [np.ascontiguousarray(data[o:o + n]) for o, n in spans])
 
-    stage_ms = stages / args.steps
+    stage_ms = dev["stage_ms"]
     names = native.STAGE_NAMES
     dom = int(np.argmax(stage_ms))
-    peak, peak_kind = measured_peaks()
-    algo_bytes = data.size * (1.0 + ratio)
-    achieved = algo_bytes / (stage_ms[dom] / 1e3) / 1e9
-    tr = committed_traffic().get(names[dom])
-    # ncu DRAM bytes of that kernel per input byte on this workload, scaled
-    # to this launch's input (traffic grows with the input it processes)
-    traffic = round(tr["dram_bytes_per_input_byte"] * data.size) if tr else None
+    roofline = roofline_of(names[dom], stage_ms[dom], data.size, ratio, clk)
 
     cpu = None
     zl = None
@@ -619,11 +735,36 @@ def main():
         threads = os.cpu_count() or 1
         r, cr, nb = cpu_port_rate(data, args.cpu_sample_mib, threads)
         cpu = {"value": round(r, 5), "unit": "GB/s", "cores": threads, "kind": "port",
-               "sample": f"first {args.cpu_sample_mib} MiB of the workload (CPU port of the reference GPU "
-                         f"path, members on {threads} host threads)", "ratio": round(cr, 5)}
+               "sample": (f"first {args.cpu_sample_mib} MiB of the workload" if args.cpu_sample_mib > 0
+                          else "the whole workload") + f" (CPU port of the reference GPU path, members on "
+                                                       f"{threads} host threads)", "ratio": round(cr, 5)}
         zr, zratio = cpu_zlib_rate(data, threads)
         zl = {"value": round(zr, 4), "unit": "GB/s", "cores": threads, "ratio": round(zratio, 5),
               "what": "gpzip-cpu equivalent: zlib 1.3 level 5, one gzip member per 2 MiB chunk"}
+
+    # the other single-stream configs: 8 MiB text (plain-path config) and
+    # 272 MiB mixed binary, device-resident and end to end, every chunk
+    # compared with the oracle's committed digests
+    per_config = None
+    if rank == 0 and world == 1 and not (args.device_only or args.no_configs):
+        per_config = {}
+        for name in ("text", "binary"):
+            if name == args.workload:
+                continue
+            cdata, cdesc = workload(name)
+            cd = device_measure(ctx, cdata, name, 5, 3, stream, flush, local, rank, barrier)
+            ce = e2e_measure(ectx, cdata, name, 3, 2, stream, local, rank, 1, barrier, None)
+            ce.pop("_gz", None)
+            cst = cd["stage_ms"]
+            cdom = int(np.argmax(cst))
+            per_config[name] = {
+                "workload": cdesc, "bytes": int(cdata.size),
+                "value": round(cdata.size * 5 / (cd["total_ms"] / 1e3) / 1e9, 4),
+                "unit": "GB/s", "ms_per_step": round(cd["total_ms"] / 5, 4), "ratio": round(cd["ratio"], 5),
+                "parity": cd["parity"], "e2e": ce,
+                "stage_ms": {n: round(float(x), 4) for n, x in zip(names, cst)},
+                "roofline": roofline_of(names[cdom], cst[cdom], cdata.size, cd["ratio"], clk)}
+            del cdata
 
     serving = None
     if rank == 0 and args.serve_seconds > 0 and not args.device_only:
@@ -646,25 +787,21 @@ def main():
             "warmup": args.warmup, "ms_per_step": round(max_ms / args.steps, 4), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u8",
             "data": "synthetic (seeded generators standing in for the reference's corpora)",
-            "config": {"workload": desc, "bytes": int(data.size), "chunk_bytes": CHUNK, "member_bytes": MEMBER,
-                       "members": sum(-(-n // MEMBER) for _, n in spans), "level": 5,
-                       "l2": "flushed between steps (256 MiB write)", "parallelism": f"replicas x{world}"},
-            "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": round(achieved, 2), "peak": peak,
-                         "unit": "GB/s", "frac": round(achieved / peak, 5), "traffic": traffic,
-                         "peak_kind": peak_kind, "algorithmic_bytes_per_launch": int(algo_bytes)},
+            "config": config_of(data, desc, world),
+            "roofline": roofline,
             "stage_ms": {n: round(float(x), 4) for n, x in zip(names, stage_ms)},
             "cpu_baseline": cpu,
             "gpzip_cpu_equiv": zl,
-            "e2e": {"value": round(e2e_value, 4), "unit": "GB/s", "h2d_bytes_per_step": int(data.size),
-                    "d2h_bytes_per_step": int(e2e_out), "api": "gpz_compress_batch (host buffers; inputs page-locked)",
-                    "host_ms_per_step": e2e_host},
+            "e2e": e2e,
             "chunk_fn": chunk_fn,
-            "inflate": inflate,
             "writer": writer,
+            "hybrid": hybrid,
+            "inflate": inflate,
             "gpu_launches": int(launches),
             "clocks": clk,
             "ratio": round(ratio, 5),
             "parity": parity,
+            "per_config": per_config,
             "serving": serving,
             "uneven": uneven,
         }
