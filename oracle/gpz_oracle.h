@@ -68,6 +68,14 @@ size_t gpzo_gzip_chunk(const uint8_t* in, size_t n, size_t member_bytes, uint8_t
 /* Worst-case member size bound used by the oracle for buffer sizing. */
 size_t gpzo_member_bound(size_t n);
 
+/* zstd frame of one chunk as the GPU zstd codec defines it from this
+ * path's tokens (oracle/zstd_frame.c): a 6-byte header, one block per 4 KiB
+ * tile of each member_bytes piece, raw literals, predefined FSE sequences,
+ * raw blocks where those are not smaller.  Returns bytes written, or 0 when
+ * cap < gpzo_zstd_bound or on failure. */
+size_t gpzo_zstd_chunk(const uint8_t* in, size_t n, size_t member_bytes, uint8_t* out, size_t cap);
+size_t gpzo_zstd_bound(size_t n, size_t member_bytes);
+
 /* Reference brute-force matcher used by the reference's encoder tests
  * (deflate.rs:992-1016); window given in bytes. */
 void gpzo_brute_lz77(const uint8_t* in, uint32_t n, uint32_t window, uint32_t* pp);

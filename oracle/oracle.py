@@ -60,6 +60,10 @@ def lib() -> ctypes.CDLL:
         L.gpzcpu_gzip_chunks.argtypes = [u8p, ctypes.c_size_t, ctypes.c_size_t, ctypes.c_int,
                                          ctypes.c_int, u8p, ctypes.c_size_t]
         L.gpzcpu_gzip_chunks.restype = ctypes.c_size_t
+        L.gpzo_zstd_chunk.argtypes = [u8p, ctypes.c_size_t, ctypes.c_size_t, u8p, ctypes.c_size_t]
+        L.gpzo_zstd_chunk.restype = ctypes.c_size_t
+        L.gpzo_zstd_bound.argtypes = [ctypes.c_size_t, ctypes.c_size_t]
+        L.gpzo_zstd_bound.restype = ctypes.c_size_t
         _lib = L
     return _lib
 
@@ -185,3 +189,64 @@ def cpu_gzip_chunks(data, chunk: int = 2 << 20, level: int = 5, threads: int = 1
     if k == 0:
         raise RuntimeError("cpu gzip failed")
     return out[:k].tobytes()
+
+
+def zstd_chunk(data, member_bytes: int = MEMBER_BYTES) -> bytes:
+    """The GPU zstd codec's frame for one chunk (oracle/zstd_frame.c)."""
+    a = _u8(data)
+    cap = lib().gpzo_zstd_bound(a.size, member_bytes)
+    out = np.zeros(cap, dtype=np.uint8)
+    k = lib().gpzo_zstd_chunk(_ptr(a), a.size, member_bytes, _ptr(out), cap)
+    if k == 0:
+        raise RuntimeError("oracle zstd_chunk failed")
+    return out[:k].tobytes()
+
+
+_zstd = None
+
+
+def zstd_lib():
+    """libzstd (the system's shared library, no header needed): the
+    independent decoder the zstd frames are checked with, and the CPU
+    baseline's encoder."""
+    global _zstd
+    if _zstd is None:
+        z = ctypes.CDLL("libzstd.so.1")
+        z.ZSTD_decompress.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t]
+        z.ZSTD_decompress.restype = ctypes.c_size_t
+        z.ZSTD_compress.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int]
+        z.ZSTD_compress.restype = ctypes.c_size_t
+        z.ZSTD_compressBound.argtypes = [ctypes.c_size_t]
+        z.ZSTD_compressBound.restype = ctypes.c_size_t
+        z.ZSTD_isError.argtypes = [ctypes.c_size_t]
+        z.ZSTD_isError.restype = ctypes.c_uint
+        z.ZSTD_getErrorName.argtypes = [ctypes.c_size_t]
+        z.ZSTD_getErrorName.restype = ctypes.c_char_p
+        _zstd = z
+    return _zstd
+
+
+def zstd_decompress(frames: bytes, size: int) -> bytes:
+    """libzstd's decoder over one or more concatenated frames of `size`
+    decompressed bytes in total; raises on any decoding error."""
+    z = zstd_lib()
+    src = np.frombuffer(frames, dtype=np.uint8)
+    dst = np.zeros(max(size, 1), dtype=np.uint8)
+    r = z.ZSTD_decompress(_ptr(dst), dst.size, _ptr(src), src.size)
+    if z.ZSTD_isError(r):
+        raise ValueError("libzstd: " + z.ZSTD_getErrorName(r).decode())
+    if r != size:
+        raise ValueError(f"libzstd decoded {r} bytes, expected {size}")
+    return dst[:size].tobytes()
+
+
+def zstd_compress(data, level: int = 3) -> bytes:
+    """libzstd's own encoder (one frame), the gpzip-cpu zstd path's engine."""
+    z = zstd_lib()
+    a = _u8(data)
+    cap = z.ZSTD_compressBound(a.size)
+    out = np.zeros(max(cap, 1), dtype=np.uint8)
+    r = z.ZSTD_compress(_ptr(out), cap, _ptr(a), a.size, level)
+    if z.ZSTD_isError(r):
+        raise ValueError("libzstd: " + z.ZSTD_getErrorName(r).decode())
+    return out[:r].tobytes()
