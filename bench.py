@@ -450,6 +450,59 @@ def gzip_check(outs, data, workload_name):
             else f"FAILED (inflate={ok}, chunks equal to the oracle's: {same}/{total})")
 
 
+def zstd_check(outs, data, workload_name):
+    """Every chunk's frame equals the oracle's restatement (oracle/zstd_frame.c,
+    on all host threads), and libzstd decodes the stream back to the input."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from oracle import oracle as O
+    spans = W.chunk_spans(data.size, CHUNK)
+    with ThreadPoolExecutor(os.cpu_count() or 1) as ex:
+        want = list(ex.map(lambda on: O.zstd_chunk(data[on[0]:on[0] + on[1]], MEMBER), spans))
+    same = sum(int(bytes(a) == b) for a, b in zip(outs, want))
+    try:
+        ok = O.zstd_decompress(b"".join(bytes(x) for x in outs), data.size) == data.tobytes()
+    except ValueError:
+        ok = False
+    return (f"ok ({same}/{len(spans)} frames equal the oracle's; libzstd decodes the stream)"
+            if ok and same == len(spans) else f"FAILED (libzstd={ok}, frames equal: {same}/{len(spans)})")
+
+
+def zstd_measure(data, workload_name, desc, stream, flush, local, barrier):
+    """The chunk-parallel zstd codec (GPZ_CODEC_ZSTD) on the workload:
+    device-resident rate with its stage times, end to end through
+    gpz_compress_batch, ratio, parity; beside it the gpzip-cpu zstd path,
+    libzstd level 3 (the reference's level 5 mapping, compress.rs:91-99) per
+    2 MiB chunk on all host threads."""
+    import time as _t
+    from concurrent.futures import ThreadPoolExecutor
+
+    from gpzip_b200 import native
+    from oracle import oracle as O
+    zc = native.Context(device=local, member_bytes=MEMBER, flags=native.GPZ_FLAG_STAGE_TIMING,
+                        codec=native.GPZ_CODEC_ZSTD)
+    d = device_measure(zc, data, workload_name, 5, 3, stream, flush, local, 0, barrier, check=zstd_check)
+    zc.close()
+    ze = native.Context(device=local, member_bytes=MEMBER, codec=native.GPZ_CODEC_ZSTD)
+    e = e2e_measure(ze, data, workload_name, 3, 2, stream, local, 0, 1, barrier, None, check=zstd_check)
+    e.pop("_gz", None)
+    ze.close()
+    spans = W.chunk_spans(data.size, CHUNK)
+    threads = os.cpu_count() or 1
+    with ThreadPoolExecutor(threads) as ex:
+        list(ex.map(lambda on: O.zstd_compress(data[on[0]:on[0] + min(on[1], 1 << 16)], 3), spans[:threads]))
+        t0 = _t.perf_counter()
+        cpu_out = sum(len(x) for x in ex.map(lambda on: O.zstd_compress(data[on[0]:on[0] + on[1]], 3), spans))
+        tc = _t.perf_counter() - t0
+    names = native.STAGE_NAMES_ZSTD
+    return {"workload": desc, "value": round(data.size * 5 / (d["total_ms"] / 1e3) / 1e9, 4), "unit": "GB/s",
+            "ms_per_step": round(d["total_ms"] / 5, 4), "ratio": round(d["ratio"], 5), "parity": d["parity"],
+            "stage_ms": {n: round(float(x), 4) for n, x in zip(names, d["stage_ms"])}, "e2e": e,
+            "cpu_zstd": {"value": round(data.size / tc / 1e9, 4), "unit": "GB/s", "threads": threads,
+                         "ratio": round(cpu_out / data.size, 5),
+                         "what": "libzstd level 3, one frame per 2 MiB chunk, all host threads"}}
+
+
 def device_measure(ctx, data, workload_name, steps, warmup, stream, flush, local, rank, barrier, clocks=False,
                    check=gzip_check):
     """gpz_compress_device on the workload resident in HBM: one checked
@@ -742,6 +795,10 @@ def main():
         zl = {"value": round(zr, 4), "unit": "GB/s", "cores": threads, "ratio": round(zratio, 5),
               "what": "gpzip-cpu equivalent: zlib 1.3 level 5, one gzip member per 2 MiB chunk"}
 
+    zstd = None
+    if rank == 0 and world == 1 and not (args.device_only or args.no_configs):
+        zstd = zstd_measure(data, args.workload, desc, stream, flush, local, barrier)
+
     # the other single-stream configs: 8 MiB text (plain-path config) and
     # 272 MiB mixed binary, device-resident and end to end, every chunk
     # compared with the oracle's committed digests
@@ -802,6 +859,7 @@ def main():
             "ratio": round(ratio, 5),
             "parity": parity,
             "per_config": per_config,
+            "zstd": zstd,
             "serving": serving,
             "uneven": uneven,
         }

@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgpz.so")
-SOURCES = ["gpz_kernels.cu", "gpz_runtime.cu", "gpz_static.cu", "gpz_inflate.cu", "gpz_writer.cu"]
+SOURCES = ["gpz_kernels.cu", "gpz_runtime.cu", "gpz_static.cu", "gpz_inflate.cu", "gpz_writer.cu", "gpz_zstd.cu"]
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

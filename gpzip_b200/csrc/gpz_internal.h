@@ -27,13 +27,19 @@
 
 // BatchParams.flags
 #define GPZ_BATCH_FIXED 1u      // every member as one fixed-Huffman block (RFC 1951 BTYPE 01)
+#define GPZ_BATCH_ZSTD 2u       // zstd frames (RFC 8878) instead of gzip members
+
+// MemberDesc.frame
+#define GPZ_MEMBER_FIRST 1u     // the first member of its input (a zstd frame starts here)
+#define GPZ_MEMBER_LAST 2u      // the last member of its input (its last block ends the frame)
+#define GPZ_ZSTD_FRAME_HDR 6u   // bytes of the zstd frame header
 
 struct MemberDesc {
     uint64_t in_off;     // first input byte of the member in the batch input (16-byte aligned)
     uint32_t len;        // member length in bytes
     uint32_t tile_base;  // index of the member's first tile
     uint32_t ntiles;     // ceil(len / 4096)
-    uint32_t level;      // accepted and ignored, as the reference GPU codec does (gpu.rs:223)
+    uint32_t frame;      // GPZ_MEMBER_* (the level is accepted and ignored, as gpu.rs:223 does)
     uint64_t out_slot;   // caller-visible ordinal (used by the serving queue)
 };
 
@@ -43,13 +49,13 @@ struct TileDesc {
 };
 
 struct MemberOut {
-    uint64_t gz_off;         // byte offset of this member's gzip member in the batch output
-    uint32_t deflate_bytes;  // DEFLATE payload bytes
-    uint32_t crc;            // CRC-32 of the member input
-    uint32_t total_bits;     // DEFLATE bits incl. header and EOB
+    uint64_t gz_off;         // byte offset of this member's output in the batch output
+    uint32_t deflate_bytes;  // payload bytes: the DEFLATE block (gzip), everything (zstd)
+    uint32_t crc;            // CRC-32 of the member input (gzip)
+    uint32_t total_bits;     // DEFLATE bits incl. header and EOB (gzip)
     uint32_t header_bits;
     uint32_t len;            // ISIZE (member input length)
-    uint32_t pad;
+    uint32_t frame_bytes;    // bytes around the payload: 18 (gzip header and trailer), 0 (zstd)
 };
 
 // Everything a batch launch needs; passed by value to every kernel.
@@ -65,6 +71,8 @@ struct BatchParams {
     uint32_t* out_words;      // gzip stream of the batch, as 32-bit words
     uint32_t* tile_entry;     // walk entry offset into each tile
     uint16_t* tile_exit;      // [tile][GPZ_EXITS] exit offset into the next tile
+    uint32_t* tile_zinfo;     // zstd: per tile, the block's size | compressed << 31 (in the exit tables'
+                              // space, free once the walk is done)
     uint16_t* tile_hist;      // [tile][GPZ_NSYM] symbol counts of the tile's tokens
     uint32_t* tile_ntok;      // tokens per tile
     uint32_t* tile_bitoff;    // tile's first token bit within its member's DEFLATE stream
@@ -104,6 +112,8 @@ struct LaunchShape {
     int emit_grid;
     int segtab_grid;
     int huff_grid;
+    int zblock_grid;  // zstd stages (0: one CTA per item)
+    int zcopy_grid;
 };
 
 // Host-mapped pinned destinations of k_drain.
@@ -156,3 +166,8 @@ size_t gpz_inflate_smem_bytes();
 int gpz_occupancy(LaunchShape* persistent);
 int gpz_kernel_smem_setup();
 size_t gpz_lookup_smem_bytes();
+// zstd stages after the walk (gpz_zstd.cu): k_zblock (blocks, placement in
+// its last CTA) and k_zcopy; events[4..5] as in gpz_launch_batch.
+int gpz_launch_zstd(const BatchParams& bp, void* stream, void* const* events, int grid_blocks, int grid_copy);
+int gpz_zstd_setup();
+int gpz_zstd_occupancy(int* grid_blocks, int* grid_copy);

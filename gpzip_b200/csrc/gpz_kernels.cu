@@ -1597,7 +1597,7 @@ __global__ void __launch_bounds__(kHuffThreads) k_huff(BatchParams bp) {
             mo.total_bits = tot;
             mo.header_bits = sm.hbits;
             mo.len = md.len;
-            mo.pad = 0;
+            mo.frame_bytes = 18;
             bp.member_out[m] = mo;
         }
         for (int q = tid; q < GPZ_NSYM; q += kHuffThreads) bp.member_codes[(size_t)m * GPZ_NSYM + q] = sm.codes[q];
@@ -1609,8 +1609,8 @@ __global__ void __launch_bounds__(kHuffThreads) k_huff(BatchParams bp) {
 
 // ========================================================== member placement
 
-// Byte offset of every gzip member in the batch output: exclusive scan of
-// (18 + DEFLATE bytes) in member order, one CTA.
+// Byte offset of every member in the batch output: exclusive scan of
+// (framing + payload bytes) in member order, one CTA.
 
 template <int T>
 __device__ void place_members(const BatchParams& bp, unsigned long long* wsum, unsigned long long& carry) {
@@ -1622,7 +1622,9 @@ __device__ void place_members(const BatchParams& bp, unsigned long long* wsum, u
     for (uint32_t base = 0; base < nmembers; base += T) {
         const uint32_t m = base + tid;
         // written by other CTAs of the producing kernel: read past L1
-        const unsigned long long v = m < nmembers ? 18ull + __ldcg(&bp.member_out[m].deflate_bytes) : 0ull;
+        const unsigned long long v =
+            m < nmembers ? (unsigned long long)__ldcg(&bp.member_out[m].frame_bytes) + __ldcg(&bp.member_out[m].deflate_bytes)
+                         : 0ull;
         unsigned long long x = v;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -1823,7 +1825,7 @@ __global__ void k_drain(BatchParams bp, uint8_t* h_out, MemberOut* h_mout, uint3
     unsigned long long total = 0;
     if (nmembers) {
         const MemberOut last = bp.member_out[nmembers - 1];
-        total = last.gz_off + 18ull + last.deflate_bytes - bp.out_base;
+        total = last.gz_off + last.frame_bytes + last.deflate_bytes - bp.out_base;
     }
     const uint4* src = reinterpret_cast<const uint4*>(bp.out_words);
     uint4* dst = reinterpret_cast<uint4*>(h_out);
@@ -1917,6 +1919,7 @@ int gpz_kernel_smem_setup() {
     tab[0] = x8;
     for (int k = 1; k < 32; k++) tab[k] = mul(tab[k - 1], tab[k - 1]);
     if (cudaMemcpyToSymbol(c_x8pow2, tab, sizeof tab) != cudaSuccess) return -1;
+    if (gpz_zstd_setup() != 0) return -1;
     if (cudaFuncSetAttribute(k_segtab<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SegtabSmem::kBytes) !=
         cudaSuccess)
         return -1;
@@ -1966,6 +1969,12 @@ int gpz_launch_batch(const BatchParams& bp, const LaunchShape& ls, void* stream,
             break;
     }
     mark(3);
+    if (bp.flags & GPZ_BATCH_ZSTD) {
+        // zstd blocks in place of the Huffman stages (gpz_zstd.cu)
+        if (gpz_launch_zstd(bp, stream, events, ls.zblock_grid, ls.zcopy_grid) != 0) return -1;
+        if (drain) k_drain<<<drain->grid, 256, 0, s>>>(bp, drain->h_out, drain->h_mout, drain->h_err);
+        return cudaGetLastError() == cudaSuccess ? 0 : -1;
+    }
     const int gh = grid_of(ls.huff_grid, bp.nmembers);
     k_huff<<<gh, kHuffThreads, 0, s>>>(bp);
     k_frame<<<gh, kFrameThreads, 0, s>>>(bp);
@@ -2003,6 +2012,8 @@ int gpz_occupancy(LaunchShape* persistent) {
                                                              : (const void*)k_walk_mark_warp<512>;
     persistent->walk_grid = sms * occ(walk_fn, persistent->walk_threads == 1024 ? 512 : persistent->walk_threads, 0);
     persistent->huff_grid = sms * occ((const void*)k_huff, kHuffThreads, 0);
+    if (gpz_zstd_occupancy(&persistent->zblock_grid, &persistent->zcopy_grid) != 0)
+        persistent->zblock_grid = persistent->zcopy_grid = 0;
     persistent->emit_grid = sms * occ(persistent->emit_threads == 256 ? (const void*)k_emit<256>
                                                                        : (const void*)k_emit<512>,
                                       persistent->emit_threads, 0);

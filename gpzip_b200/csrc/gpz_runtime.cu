@@ -264,6 +264,7 @@ struct gpz_ctx {
     size_t pool_cap = kDefaultPool;
     size_t batch_bytes = kDefaultBatch;
     int flags = 0;
+    int codec = GPZ_CODEC_GZIP;
     int sms = 0;
     // bound of every host wait for the device in the calling thread, ms
     std::atomic<int> wait_ms{kDefaultWaitMs};
@@ -417,7 +418,7 @@ void plan(const gpz_ctx* c, Slot& sl) {
             md.len = (uint32_t)std::min(c->member_bytes, s.n - std::min(s.n, j * c->member_bytes));
             md.tile_base = (uint32_t)sl.tiles.size();
             md.ntiles = (md.len + GPZ_SEG - 1) / GPZ_SEG;
-            md.level = 0;
+            md.frame = (j == 0 ? GPZ_MEMBER_FIRST : 0u) | (j + 1 == nm ? GPZ_MEMBER_LAST : 0u);
             md.out_slot = sl.members.size();
             for (uint32_t t = 0; t < md.ntiles; t++) sl.tiles.push_back(TileDesc{(uint32_t)sl.members.size(), t});
             sl.members.push_back(md);
@@ -516,6 +517,11 @@ BatchParams params_of(const gpz_ctx* c, Slot& sl, const uint8_t* d_in, uint8_t* 
     bp.ntiles = (uint32_t)sl.tiles.size();
     bp.out_base = 0;
     bp.flags = (c->flags & GPZ_FLAG_FIXED_BLOCKS) ? GPZ_BATCH_FIXED : 0u;
+    if (c->codec == GPZ_CODEC_ZSTD) {
+        bp.flags = GPZ_BATCH_ZSTD;
+        // 4 bytes per tile inside the exit tables (516 bytes per tile)
+        bp.tile_zinfo = static_cast<uint32_t*>(sl.d_texit.p);
+    }
     return bp;
 }
 
@@ -808,6 +814,7 @@ int submit_slot(gpz_ctx* c, Slot& sl, const gpz_desc* d, size_t count, const Lau
 void frame_members(const MemberOut* mo, size_t first, size_t count, uint8_t* dst, uint64_t base) {
     static const uint8_t hdr[10] = {0x1f, 0x8b, 0x08, 0x00, 0x00, 0x00, 0x00, 0x00, 0x00, 0xff};
     for (size_t m = first; m < first + count; m++) {
+        if (mo[m].frame_bytes != 18) continue;  // zstd frames are complete on the device
         uint8_t* p = dst + (mo[m].gz_off - base);
         std::memcpy(p, hdr, 10);
         uint8_t* t = p + 10 + mo[m].deflate_bytes;
@@ -847,7 +854,7 @@ int finish_slot(gpz_ctx* c, Slot& sl, gpz_out* outs, size_t first_item) {
         const Span& sp = sl.spans[i];
         const MemberOut& a = sl.h_mout[sp.first_member];
         const MemberOut& z = sl.h_mout[sp.first_member + sp.nmembers - 1];
-        const uint64_t beg = a.gz_off, end = z.gz_off + 18 + z.deflate_bytes;
+        const uint64_t beg = a.gz_off, end = z.gz_off + z.frame_bytes + z.deflate_bytes;
         gpz_out& o = outs[first_item + i];
         o.out_len = end - beg;
         if (!o.out || o.out_cap < end - beg) {
@@ -1378,7 +1385,7 @@ struct ServeEngine {
                 const Span& sp = sl.spans[i];
                 const MemberOut& a = sl.h_mout[sp.first_member];
                 const MemberOut& z = sl.h_mout[sp.first_member + sp.nmembers - 1];
-                outs[i].assign(sl.h_out + a.gz_off, sl.h_out + z.gz_off + 18 + z.deflate_bytes);
+                outs[i].assign(sl.h_out + a.gz_off, sl.h_out + z.gz_off + z.frame_bytes + z.deflate_bytes);
             }
         }
         const double t = now_ms();
@@ -1452,10 +1459,12 @@ int gpz_create(const gpz_config* cfg, gpz_ctx** out) {
     c->pool_cap = cfg->pool_bytes ? cfg->pool_bytes : kDefaultPool;
     c->batch_bytes = cfg->batch_bytes ? cfg->batch_bytes : kDefaultBatch;
     c->flags = cfg->flags;
-    if (cfg->wait_ms < 0) {
+    if (cfg->wait_ms < 0 || (cfg->codec != GPZ_CODEC_GZIP && cfg->codec != GPZ_CODEC_ZSTD) ||
+        (cfg->codec == GPZ_CODEC_ZSTD && (cfg->flags & GPZ_FLAG_FIXED_BLOCKS))) {
         delete c;
         return GPZ_E_ARG;
     }
+    c->codec = cfg->codec;
     c->wait_ms = cfg->wait_ms ? cfg->wait_ms : kDefaultWaitMs;
     if (cudaSetDevice(c->device) != cudaSuccess || gpz_kernel_smem_setup() != 0) {
         cudaGetLastError();
@@ -1621,7 +1630,7 @@ int gpz_compress_device(gpz_ctx* c, const void* d_in, const uint64_t* in_off, co
     if (*sl.h_err) return fail(c, GPZ_E_INTERNAL, "device self-check");
     for (size_t i = 0; i < count; i++) out_off[i] = c->mout[sl.spans[i].first_member].gz_off;
     const MemberOut& l = c->mout.back();
-    out_off[count] = l.gz_off + 18 + l.deflate_bytes;
+    out_off[count] = l.gz_off + l.frame_bytes + l.deflate_bytes;
     return GPZ_OK;
 }
 
@@ -1785,7 +1794,7 @@ int gpz_frame_host(gpz_ctx* c, uint8_t* host_out, size_t cap) {
     std::lock_guard<std::mutex> lk(c->mu);
     if (c->mout.empty()) return GPZ_E_ARG;
     const MemberOut& l = c->mout.back();
-    if (l.gz_off + 18 + l.deflate_bytes > cap) return GPZ_E_SPACE;
+    if (l.gz_off + l.frame_bytes + l.deflate_bytes > cap) return GPZ_E_SPACE;
     frame_members(c->mout.data(), 0, c->mout.size(), host_out, 0);
     return GPZ_OK;
 }
@@ -1793,6 +1802,7 @@ int gpz_frame_host(gpz_ctx* c, uint8_t* host_out, size_t cap) {
 int gpz_debug_chunk(gpz_ctx* c, const uint8_t* in, size_t n, uint32_t* pp, uint32_t* tokens, size_t* ntok,
                     uint8_t* out, size_t out_cap, size_t* out_len) {
     if (!c || (!in && n)) return GPZ_E_ARG;
+    if (pp && c->codec == GPZ_CODEC_ZSTD) return GPZ_E_ARG;  // the zstd stages reuse pp as block scratch
     std::lock_guard<std::mutex> lk(c->mu);
     cudaSetDevice(c->device);
     gpz_desc d{in, n, 0};

@@ -86,7 +86,7 @@ __global__ void k_static_setup(uint8_t* base, uint32_t n) {
         d.len = n;
         d.tile_base = 0;
         d.ntiles = nt;
-        d.level = 0;
+        d.frame = GPZ_MEMBER_FIRST | GPZ_MEMBER_LAST;
         d.out_slot = 0;
         md[0] = d;
     }

@@ -27,6 +27,8 @@ GPZ_E_PENDING = 9
 GPZ_E_BUSY = 8
 GPZ_E_ADMISSION = 2
 GPZ_E_TIMEOUT = 3
+GPZ_CODEC_GZIP = 0
+GPZ_CODEC_ZSTD = 1
 GPZ_FLAG_NO_GRAPHS = 1
 GPZ_FLAG_NO_AUTOTUNE = 2
 GPZ_FLAG_STAGE_TIMING = 4
@@ -34,6 +36,8 @@ GPZ_FLAG_SM_PARTITION = 8
 GPZ_FLAG_FIXED_BLOCKS = 16
 # gpz_stage_times order (GPZ_STAGES values): the kernels each stage covers
 STAGE_NAMES = ["k_segtab", "k_lookup", "k_walk", "k_huff", "k_emit"]
+# the same stages of a zstd context (the last two: blocks + placement, copy)
+STAGE_NAMES_ZSTD = ["k_segtab", "k_lookup", "k_walk", "k_zblock", "k_zcopy"]
 
 # Every symbol include/gpz.h declares.
 EXPORTS = [
@@ -58,7 +62,7 @@ class GpzError(RuntimeError):
 class Config(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("member_bytes", ctypes.c_size_t), ("pool_bytes", ctypes.c_size_t),
                 ("batch_bytes", ctypes.c_size_t), ("streams", ctypes.c_int), ("flags", ctypes.c_int),
-                ("wait_ms", ctypes.c_int)]
+                ("wait_ms", ctypes.c_int), ("codec", ctypes.c_int)]
 
 
 class HybridConfig(ctypes.Structure):
@@ -221,12 +225,12 @@ class Context:
     """One gpz_ctx (device pool, streams, launch shapes) on one CUDA device."""
 
     def __init__(self, device: int = 0, member_bytes: int = 128 * 1024, pool_bytes: int = 0,
-                 batch_bytes: int = 0, flags: int = 0, wait_ms: int = 0):
+                 batch_bytes: int = 0, flags: int = 0, wait_ms: int = 0, codec: int = GPZ_CODEC_GZIP):
         L = load()
         cfg = Config()
         L.gpz_config_default(ctypes.byref(cfg))
         cfg.device, cfg.member_bytes, cfg.pool_bytes = device, member_bytes, pool_bytes
-        cfg.batch_bytes, cfg.flags, cfg.wait_ms = batch_bytes, flags, wait_ms
+        cfg.batch_bytes, cfg.flags, cfg.wait_ms, cfg.codec = batch_bytes, flags, wait_ms, codec
         h = ctypes.c_void_p()
         rc = L.gpz_create(ctypes.byref(cfg), ctypes.byref(h))
         if rc != GPZ_OK:

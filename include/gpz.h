@@ -62,7 +62,21 @@ typedef struct gpz_config {
     int streams;           /* reserved (0) */
     int flags;             /* GPZ_FLAG_* */
     int wait_ms;           /* bound of every wait of a calling thread for the device, ms (0: 60000) */
+    int codec;             /* GPZ_CODEC_GZIP (0) or GPZ_CODEC_ZSTD */
 } gpz_config;
+
+/* Codecs.  GZIP: the reference GPU path's gzip members (everything above).
+ * ZSTD: the chunk-parallel zstd codec of the reference
+ * (ZstdCompressor::chunk_fn, crates/gpzip-codec-cpu/src/compress.rs:76-126):
+ * every input becomes one RFC 8878 zstd frame (no content size, no
+ * checksum, 64 KiB window), from the same segmented-hash matches and lazy
+ * walk as the gzip path; one block per 4 KiB of input, raw literals, the
+ * predefined FSE distributions for the sequences, raw blocks where that is
+ * not smaller.  Concatenated frames decode as one stream, as the reference's
+ * .tar.zst does.  The compress calls, the writer and serving work the same;
+ * gpz_debug_chunk cannot return pp, and GPZ_FLAG_FIXED_BLOCKS does not apply. */
+#define GPZ_CODEC_GZIP 0
+#define GPZ_CODEC_ZSTD 1
 
 #define GPZ_FLAG_NO_GRAPHS 1    /* launch kernels directly instead of per-bucket CUDA graphs */
 #define GPZ_FLAG_NO_AUTOTUNE 2  /* keep the default launch shapes */
