@@ -1104,10 +1104,22 @@ struct ServeEngine {
     static constexpr int kLaneSlots = 3;
     // requests submitted and not yet polled: beyond this, submit says busy
     static constexpr size_t kMaxRequests = 1u << 20;
+    // Overload.  Small requests are kept within a few ms of work: a small
+    // request is admitted while the small lane's queue (not yet launched)
+    // holds at most kSmallBacklog bytes.  Large requests yield first: one is
+    // admitted only while the pool has kSmallReserve bytes to spare for the
+    // small lane and the small lane's queue is below half its limit, and a
+    // large batch is launched only while no small work waits (for at most
+    // kLargeHoldMs, so the large lane always moves).
+    static constexpr size_t kSmallBacklog = 24u << 20;
+    static constexpr size_t kSmallReserve = 1ull << 30;
+    static constexpr double kLargeHoldMs = 20.0;
 
     struct Lane {
         int nslots = 2;         // pipeline slots in use (at most kLaneSlots)
         size_t batch_cap = 0;   // input bytes per batch
+        size_t batch_cap_busy = 0;  // input bytes per batch while more than one batch waits
+        size_t backlog = 0;     // bytes queued and not yet launched
         size_t max_units = 0;   // units per batch
         LaunchPolicy pol;
         Slot slots[kLaneSlots];
@@ -1157,11 +1169,15 @@ struct ServeEngine {
         Lane& sm = lanes[0];
         sm.nslots = 3;
         sm.batch_cap = 1u << 20;  // <= 256 tiles + one per unit: the low-latency buckets
+        // a backlog is worked off in 4 MiB batches: more bytes per launch
+        // while the queue, not the batch, sets the small requests' latency
+        sm.batch_cap_busy = 4u << 20;
         sm.max_units = 1024;
         sm.pol = LaunchPolicy{false, false, true, true, 100};  // persistent default shape, graphs, k_fetch
         Lane& lg = lanes[1];
         lg.nslots = 2;
         lg.batch_cap = 16u << 20;
+        lg.batch_cap_busy = lg.batch_cap;
         lg.max_units = 16;
         // without partitions: persistent grids on 60 % of the GPU, the rest
         // stays free for the small lane's CTAs; copy-engine upload.  Against
@@ -1180,7 +1196,7 @@ struct ServeEngine {
             for (int k = 0; k < lanes[l].nslots && !rc; k++) {
                 Slot& s = lanes[l].slots[k];
                 rc = init_slot(c, s, l == 0 ? greatest : least);
-                if (!rc) rc = reserve_limits(c, s, lanes[l].batch_cap, lanes[l].max_units);
+                if (!rc) rc = reserve_limits(c, s, lanes[l].batch_cap_busy, lanes[l].max_units);
             }
         }
         if (partitioned) green_api().set_cur(primary);
@@ -1229,7 +1245,10 @@ struct ServeEngine {
         r->pieces.resize(r->units);
         {
             std::lock_guard<std::mutex> lk(mu);
-            if (queued_bytes + d->n > c->pool_cap) {
+            const size_t reserve = r->small ? 0 : std::min(kSmallReserve, c->pool_cap / 4);
+            const bool small_full = r->small ? lanes[0].backlog + d->n > kSmallBacklog
+                                             : lanes[0].backlog > kSmallBacklog / 2;
+            if (queued_bytes + d->n + reserve > c->pool_cap || small_full) {
                 rejected++;
                 return GPZ_E_ADMISSION;
             }
@@ -1251,6 +1270,7 @@ struct ServeEngine {
         r->id = next_id++;
         for (size_t u = 0; u < r->units; u++)
             L.q.push_back(Unit{r, u, u * kUnit, std::min(kUnit, d->n - std::min(d->n, u * kUnit))});
+        L.backlog += d->n;
         reqs[r->id] = r;
         *ticket = r->id;
         L.cv_work.notify_one();
@@ -1293,11 +1313,13 @@ struct ServeEngine {
     static std::vector<Unit> take_batch(Lane& L) {
         std::vector<Unit> b;
         size_t bytes = 0;
-        while (!L.q.empty() && b.size() < L.max_units && (b.empty() || bytes + L.q.front().n <= L.batch_cap)) {
+        const size_t cap = L.backlog > L.batch_cap ? L.batch_cap_busy : L.batch_cap;
+        while (!L.q.empty() && b.size() < L.max_units && (b.empty() || bytes + L.q.front().n <= cap)) {
             bytes += L.q.front().n;
             b.push_back(L.q.front());
             L.q.pop_front();
         }
+        L.backlog -= std::min(L.backlog, bytes);
         return b;
     }
 
@@ -1316,8 +1338,18 @@ struct ServeEngine {
                 std::unique_lock<std::mutex> lk(mu);
                 L.cv_work.wait(lk, [&] { return stop || (!L.q.empty() && free_slot_of(L) >= 0); });
                 if (stop) return;
+                if (&L == &lanes[1]) {
+                    // small work first: a large batch waits while small
+                    // requests are queued, up to kLargeHoldMs
+                    const double t_hold = now_ms();
+                    while (!stop && lanes[0].backlog > 0 && now_ms() - t_hold < kLargeHoldMs)
+                        L.cv_work.wait_for(lk, std::chrono::microseconds(200));
+                    if (stop) return;
+                    if (L.q.empty() || free_slot_of(L) < 0) continue;
+                }
                 k = free_slot_of(L);
                 batch = take_batch(L);
+                if (&L == &lanes[0] && lanes[0].backlog == 0) lanes[1].cv_work.notify_one();
                 L.slot_free[k] = false;
                 const double tl = now_ms(), q = tl - batch.front().req->t_arrive;
                 max_queue_ms = std::max(max_queue_ms, q);
