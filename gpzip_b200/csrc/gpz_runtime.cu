@@ -40,6 +40,7 @@
 #include "../../include/gpz.h"
 #include "gpz_inflate_core.h"
 #include "gpz_internal.h"
+#include "gpz_stream.h"
 
 namespace {
 
@@ -936,6 +937,85 @@ int run_host_items(gpz_ctx* c, const gpz_desc* d, size_t count, gpz_out* outs, b
     for (int q = 0; q < kSyncSlots; q++) settle((c->next_slot + q) % kSyncSlots);
     return fatal != GPZ_OK ? fatal : first_bad;
 }
+
+}  // namespace
+
+// The device writer's pass loop (gpz_stream.h).  Slots are used round robin
+// and settled in submission order, as run_host_items does, but the passes
+// are formed from whatever chunks the writer has ready, so consecutive
+// passes of a stream overlap on the device without a call boundary between
+// them; results go to the feed straight from the slot's mapped output.
+int gpz_stream_run(gpz_ctx* c, GpzStreamFeed& feed) {
+    if (!c) return GPZ_E_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    cudaSetDevice(c->device);
+    int fatal = settle_stale(c);
+    if (fatal) return fatal;
+    std::deque<int> pend;  // slots in submission order
+    auto settle = [&]() {
+        const int k = pend.front();
+        pend.pop_front();
+        Slot& sl = c->slots[k];
+        int r = wait_slot(c, sl);
+        const double t0 = now_ms();
+        if (r == GPZ_OK && fatal == GPZ_OK) {
+            frame_members(sl.h_mout, 0, sl.members.size(), sl.h_out, 0);
+            for (size_t i = 0; i < sl.spans.size() && r == GPZ_OK; i++) {
+                const Span& sp = sl.spans[i];
+                const MemberOut& a = sl.h_mout[sp.first_member];
+                const MemberOut& z = sl.h_mout[sp.first_member + sp.nmembers - 1];
+                const uint64_t end = z.gz_off + z.frame_bytes + z.deflate_bytes;
+                if (feed.deliver(sl.h_out + a.gz_off, end - a.gz_off) != 0) r = fail(c, GPZ_E_SINK, "sink");
+            }
+        }
+        add_time(c, 4, now_ms() - t0);
+        if (r != GPZ_OK && fatal == GPZ_OK) fatal = r;
+    };
+    std::vector<gpz_desc> items;
+    for (int pass = 0; fatal == GPZ_OK;) {
+        if ((int)pend.size() == kSyncSlots) {
+            settle();
+            continue;
+        }
+        const size_t cap = c->batch_bytes >> (pass < 2 ? 4 - 2 * pass : 0);
+        const bool busy = !pend.empty();
+        items.clear();
+        feed.take(items, cap, busy ? std::min<size_t>(cap, 8u << 20) : 1, false);
+        if (items.empty()) {
+            if (!busy) break;  // nothing ready and nothing on the device
+            settle();
+            continue;
+        }
+        const int k = c->next_slot;  // not pending: fewer than kSyncSlots are, in round-robin order
+        const int rc = submit_slot(c, c->slots[k], items.data(), items.size(), kPolicyBatched, c->kstream);
+        if (rc) {
+            fatal = rc;
+            break;
+        }
+        pend.push_back(k);
+        c->next_slot = (k + 1) % kSyncSlots;
+        pass++;
+    }
+    while (!pend.empty()) settle();
+    return fatal;
+}
+
+uint8_t* gpz_pinned_alloc(size_t n) {
+    void* p = nullptr;
+    if (cudaHostAlloc(&p, std::max<size_t>(n, 1), cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return static_cast<uint8_t*>(p);
+}
+
+void gpz_pinned_free(uint8_t* p) {
+    if (p) cudaFreeHost(p);
+}
+
+void gpz_parallel_copy(void* dst, const void* src, size_t n) { copy_pool().run({CopyPool::Copy{dst, src, n}}, true); }
+
+namespace {
 
 // priority: a CUDA stream priority (lower is more urgent; 0 is the default)
 int init_slot(gpz_ctx* c, Slot& sl, int priority = 0) {

@@ -12,11 +12,15 @@
 // Writer.  Written bytes are cut into chunk_size chunks; the first error is
 // sticky (parallel.rs:70-89): every later call returns it, and nothing after
 // the failed chunk reaches the sink.
-//  - With a device context, full chunks collect into a batch of up to
-//    max_in_flight chunks; a full batch goes to the writer's thread, which
-//    compresses it with one gpz_compress_batch call and hands the members to
-//    the sink in input order while the caller fills the next batch.  At
-//    most one batch waits behind the one being compressed.
+//  - With a device context, chunks live in page-locked buffers (pooled), so
+//    the device reads them without a staging copy, and large writes are
+//    copied in by the host copy threads.  Every full chunk joins a queue
+//    that the writer's thread feeds to the context's pass loop
+//    (gpz_stream_run): passes of whatever is ready, overlapped on the
+//    device across the whole stream, the members going to the sink in
+//    input order straight from the pass's output.  At most
+//    max(max_in_flight, 128 MiB / chunk_size) chunks are queued, on the
+//    device or waiting for the sink; the caller waits beyond that.
 //  - With a chunk function, every full chunk is handed to a pool of
 //    max_in_flight worker threads at once, as the reference spawns one rayon
 //    task per chunk (parallel.rs:91-129); up to max_in_flight chunks are
@@ -27,6 +31,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cstring>
 #include <condition_variable>
 #include <deque>
 #include <memory>
@@ -37,6 +42,7 @@
 #include <vector>
 
 #include "gpz.h"
+#include "gpz_stream.h"
 
 using Chunk = std::vector<uint8_t>;
 using Batch = std::vector<Chunk>;
@@ -88,6 +94,36 @@ void out_give(std::unique_ptr<uint8_t[]>& p, size_t cap) {
     p.reset();
 }
 
+// Page-locked chunk buffers, kept across writers: cudaHostAlloc takes about
+// a millisecond per 2 MiB buffer.  Bounded at kPoolPinned buffers.
+constexpr size_t kPoolPinned = 160;
+std::vector<std::pair<uint8_t*, size_t>> g_pinned;
+
+uint8_t* pinned_take(size_t n) {
+    {
+        std::lock_guard<std::mutex> lk(g_pool_mu);
+        for (size_t i = g_pinned.size(); i-- > 0;)
+            if (g_pinned[i].second == n) {
+                uint8_t* p = g_pinned[i].first;
+                g_pinned.erase(g_pinned.begin() + (std::ptrdiff_t)i);
+                return p;
+            }
+    }
+    return gpz_pinned_alloc(n);
+}
+
+void pinned_give(uint8_t* p, size_t n) {
+    if (!p) return;
+    {
+        std::lock_guard<std::mutex> lk(g_pool_mu);
+        if (g_pinned.size() < kPoolPinned) {
+            g_pinned.emplace_back(p, n);
+            return;
+        }
+    }
+    gpz_pinned_free(p);
+}
+
 void pool_give(std::vector<Chunk>& chunks) {
     std::lock_guard<std::mutex> lk(g_pool_mu);
     for (Chunk& ch : chunks)
@@ -108,7 +144,6 @@ struct gpz_writer {
     void* sink_user = nullptr;
     size_t chunk_size = 0, max_in_flight = 0;
     Chunk current;  // the chunk being filled (caller's thread only)
-    Batch filling;  // device mode: full chunks of the open batch (caller's thread only)
     bool finished = false;
 
     std::mutex mu;
@@ -117,12 +152,50 @@ struct gpz_writer {
     int sticky = GPZ_OK;
     std::vector<Chunk> spare;  // chunk buffers of finished chunks, reused (no page faults)
 
-    // ---- device mode: one thread compressing whole batches
-    std::deque<Batch> queue;  // batches handed over, not yet taken
-    bool busy = false;        // the thread is compressing a batch
-    std::thread worker;
-    std::unique_ptr<uint8_t[]> out;  // the thread's output buffer, from and back to the pool
-    size_t out_cap = 0;
+    // ---- device mode: page-locked chunks fed to the context's pass loop
+    struct PChunk {
+        uint8_t* p = nullptr;
+        size_t n = 0;
+    };
+    PChunk pcur;                 // the chunk being filled (caller's thread only)
+    std::deque<PChunk> ready;    // full chunks not yet taken by the pass loop
+    std::deque<PChunk> taken;    // taken, not yet delivered (in input order)
+    std::vector<uint8_t*> pfree; // this writer's spare chunk buffers
+    size_t outstanding = 0;      // ready + taken
+    size_t max_outstanding = 0;
+    bool ending = false;         // finish: the partial chunk is queued, nothing more comes
+    bool running = false;        // the streamer is inside a pass loop
+    std::thread streamer;
+
+    struct Feed : GpzStreamFeed {
+        gpz_writer* w;
+        explicit Feed(gpz_writer* wr) : w(wr) {}
+        bool take(std::vector<gpz_desc>& out, size_t max_bytes, size_t min_bytes, bool) override {
+            std::lock_guard<std::mutex> lk(w->mu);
+            size_t have = 0;
+            for (const PChunk& c : w->ready) have += c.n;
+            if (w->ready.empty() || (have < min_bytes && !w->ending)) return !(w->ending && w->ready.empty());
+            size_t bytes = 0;
+            while (!w->ready.empty() && (out.empty() || bytes + w->ready.front().n <= max_bytes)) {
+                PChunk c = w->ready.front();
+                w->ready.pop_front();
+                bytes += c.n;
+                out.push_back(gpz_desc{c.p, c.n, 5});
+                w->taken.push_back(c);
+            }
+            return true;
+        }
+        int deliver(const uint8_t* data, size_t n) override {
+            const int rc = w->sink(w->sink_user, data, n);
+            std::lock_guard<std::mutex> lk(w->mu);
+            PChunk c = w->taken.front();
+            w->taken.pop_front();
+            w->pfree.push_back(c.p);
+            w->outstanding--;
+            w->cv.notify_all();
+            return rc;
+        }
+    };
 
     // ---- chunk-function mode: one job per chunk, workers in a pool
     struct Job {
@@ -145,54 +218,41 @@ struct gpz_writer {
         }
     }
 
-    int compress(Batch& b) {
-        size_t cap = 0;
-        for (const Chunk& ch : b) cap += gpz_bound_ctx(ctx, ch.size());
-        if (out_cap < cap) {
-            out_give(out, out_cap);
-            auto o = out_take(cap);
-            out = std::move(o.first);
-            out_cap = out ? o.second : 0;
-            if (!out) return GPZ_E_NOMEM;
-        }
-        std::vector<gpz_out> outs(b.size());
-        std::vector<gpz_desc> ds(b.size());
-        size_t off = 0;
-        for (size_t i = 0; i < b.size(); i++) {
-            const size_t c = gpz_bound_ctx(ctx, b[i].size());
-            outs[i] = gpz_out{out.get() + off, c, 0, 0};
-            ds[i] = gpz_desc{b[i].data(), b[i].size(), 5};
-            off += c;
-        }
-        const int rc = gpz_compress_batch(ctx, ds.data(), ds.size(), outs.data());
-        if (rc != GPZ_OK) return rc;
-        for (size_t i = 0; i < b.size(); i++)
-            if (sink(sink_user, outs[i].out, outs[i].out_len) != 0) return GPZ_E_SINK;
-        return GPZ_OK;
-    }
-
-    void run_batches() {
+    // The device mode's thread: whenever chunks are ready, runs the pass
+    // loop until nothing is ready and nothing is on the device.  After an
+    // error, queued chunks are dropped, not written.
+    void run_stream() {
+        Feed feed(this);
         for (;;) {
-            Batch b;
-            int failed;
             {
                 std::unique_lock<std::mutex> lk(mu);
-                cv.wait(lk, [&] { return stop || !queue.empty(); });
-                if (queue.empty()) return;
-                b = std::move(queue.front());
-                queue.pop_front();
-                busy = true;
-                failed = sticky;
-                cv.notify_all();
+                cv.wait(lk, [&] { return stop || !ready.empty(); });
+                if (ready.empty()) return;
+                if (sticky != GPZ_OK) {
+                    drop_queued();
+                    continue;
+                }
+                running = true;
             }
-            // after an error the remaining batches are dropped, not written
-            const int rc = failed != GPZ_OK ? failed : compress(b);
+            const int rc = gpz_stream_run(ctx, feed);
             std::lock_guard<std::mutex> lk(mu);
+            running = false;
             if (rc != GPZ_OK && sticky == GPZ_OK) sticky = rc;
-            for (Chunk& ch : b) recycle(ch);
-            busy = false;
+            if (sticky != GPZ_OK) drop_queued();
             cv.notify_all();
         }
+    }
+
+    // (mu held) returns every queued or undelivered chunk buffer
+    void drop_queued() {
+        for (auto* q : {&ready, &taken}) {
+            for (PChunk& c : *q) {
+                pfree.push_back(c.p);
+                outstanding--;
+            }
+            q->clear();
+        }
+        cv.notify_all();
     }
 
     // One worker of the chunk-function pool: takes the oldest job nobody
@@ -252,14 +312,40 @@ struct gpz_writer {
         }
     }
 
-    // hands a full chunk over: device mode batches it, chunk-function mode
-    // queues it for the pool once fewer than max_in_flight are outstanding
-    void dispatch(Chunk&& ch) {
-        if (ctx) {
-            filling.push_back(std::move(ch));
-            if (filling.size() >= max_in_flight) submit();
-            return;
+    // device mode: queues the full (or last) chunk for the streamer once
+    // fewer than max_outstanding are queued
+    void dispatch_pinned() {
+        std::unique_lock<std::mutex> lk(mu);
+        cv.wait(lk, [&] { return outstanding < max_outstanding || sticky != GPZ_OK; });
+        if (sticky != GPZ_OK) {
+            pfree.push_back(pcur.p);
+        } else {
+            ready.push_back(pcur);
+            outstanding++;
         }
+        pcur = PChunk{};
+        cv.notify_all();
+    }
+
+    // a page-locked chunk buffer, from this writer's spares or the pool
+    bool fresh_pinned() {
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            if (!pfree.empty()) {
+                pcur.p = pfree.back();
+                pfree.pop_back();
+                pcur.n = 0;
+                return true;
+            }
+        }
+        pcur.p = pinned_take(chunk_size);
+        pcur.n = 0;
+        return pcur.p != nullptr;
+    }
+
+    // chunk-function mode: queues a full chunk for the pool once fewer than
+    // max_in_flight are outstanding
+    void dispatch(Chunk&& ch) {
         auto j = std::unique_ptr<Job>(new (std::nothrow) Job());
         std::unique_lock<std::mutex> lk(mu);
         if (!j) {
@@ -272,22 +358,12 @@ struct gpz_writer {
         cv.notify_all();
     }
 
-    // device mode: hands the open batch to the thread once fewer than one
-    // batch waits
-    void submit() {
-        if (filling.empty()) return;
-        std::unique_lock<std::mutex> lk(mu);
-        cv.wait(lk, [&] { return queue.empty(); });
-        queue.push_back(std::move(filling));
-        filling = Batch{};
-        cv.notify_all();
-    }
-
     // waits until every chunk handed over has been written or dropped
     void drain() {
-        if (ctx) submit();
         std::unique_lock<std::mutex> lk(mu);
-        cv.wait(lk, [&] { return queue.empty() && !busy && jobs.empty(); });
+        ending = true;
+        cv.notify_all();
+        cv.wait(lk, [&] { return jobs.empty() && outstanding == 0 && !running; });
     }
 
     int status() {
@@ -328,9 +404,10 @@ int open_writer(gpz_ctx* ctx, gpz_chunk_fn fn, void* fn_user, size_t chunk_size,
     w->sink_user = sink_user;
     w->chunk_size = chunk_size;
     w->max_in_flight = max_in_flight;
+    w->max_outstanding = std::max(max_in_flight, (size_t)(128u << 20) / chunk_size + 1);
     try {
         if (ctx) {
-            w->worker = std::thread([w] { w->run_batches(); });
+            w->streamer = std::thread([w] { w->run_stream(); });
         } else {
             for (size_t i = 0; i < max_in_flight; i++) w->pool.emplace_back([w] { w->run_jobs(); });
         }
@@ -372,6 +449,23 @@ int gpz_writer_write(gpz_writer* w, const uint8_t* buf, size_t n) {
     if (!w || (!buf && n) || w->finished) return GPZ_E_ARG;
     int rc = w->status();
     if (rc != GPZ_OK) return rc;
+    if (w->ctx) {
+        while (n) {
+            if (!w->pcur.p && !w->fresh_pinned()) {
+                std::lock_guard<std::mutex> lk(w->mu);
+                if (w->sticky == GPZ_OK) w->sticky = GPZ_E_NOMEM;
+                return w->sticky;
+            }
+            const size_t take = std::min(n, w->chunk_size - w->pcur.n);
+            if (take >= (256u << 10)) gpz_parallel_copy(w->pcur.p + w->pcur.n, buf, take);
+            else std::memcpy(w->pcur.p + w->pcur.n, buf, take);
+            w->pcur.n += take;
+            buf += take;
+            n -= take;
+            if (w->pcur.n == w->chunk_size) w->dispatch_pinned();
+        }
+        return w->status();
+    }
     while (n) {
         if (w->current.capacity() < w->chunk_size) w->fresh_chunk();
         const size_t take = std::min(n, w->chunk_size - w->current.size());
@@ -395,8 +489,12 @@ int gpz_writer_finish(gpz_writer* w) {
     if (!w) return GPZ_E_ARG;
     if (!w->finished) {
         w->finished = true;
-        if (!w->current.empty()) w->dispatch(std::move(w->current));
-        w->current = Chunk{};
+        if (w->ctx) {
+            if (w->pcur.p && w->pcur.n) w->dispatch_pinned();
+        } else {
+            if (!w->current.empty()) w->dispatch(std::move(w->current));
+            w->current = Chunk{};
+        }
         w->drain();
     }
     return w->status();
@@ -410,10 +508,11 @@ void gpz_writer_close(gpz_writer* w) {
         w->stop = true;
     }
     w->cv.notify_all();
-    if (w->worker.joinable()) w->worker.join();
+    if (w->streamer.joinable()) w->streamer.join();
     for (auto& t : w->pool) t.join();
     pool_give(w->spare);
-    out_give(w->out, w->out_cap);
+    if (w->pcur.p) w->pfree.push_back(w->pcur.p);
+    for (uint8_t* p : w->pfree) pinned_give(p, w->chunk_size);
     delete w;
 }
 
