@@ -967,6 +967,7 @@ int gpz_stream_run(gpz_ctx* c, GpzStreamFeed& feed) {
                 const uint64_t end = z.gz_off + z.frame_bytes + z.deflate_bytes;
                 if (feed.deliver(sl.h_out + a.gz_off, end - a.gz_off) != 0) r = fail(c, GPZ_E_SINK, "sink");
             }
+            feed.pass_done();
         }
         add_time(c, 4, now_ms() - t0);
         if (r != GPZ_OK && fatal == GPZ_OK) fatal = r;
@@ -1636,10 +1637,65 @@ size_t gpz_bound_ctx(const gpz_ctx* c, size_t n) {
 // its result.  A lone caller runs its chunk at once.  This takes the place
 // of BatchedLz77's submitter thread (batch.rs:48-141), which batches the
 // chunks that ParallelChunkedWriter's workers submit concurrently.
+namespace {
+
+// The queue of waiting gpz_compress_chunk calls as a stream feed: the
+// leader's pass loop takes queued calls into passes and hands each call its
+// result; one pass's results are copied out on the copy threads together.
+struct CombineFeed : GpzStreamFeed {
+    gpz_ctx* c;
+    std::deque<gpz_ctx::ChunkCall*> taken;
+    std::vector<CopyPool::Copy> copies;
+    std::vector<gpz_ctx::ChunkCall*> finished;
+    explicit CombineFeed(gpz_ctx* ctx) : c(ctx) {}
+    bool take(std::vector<gpz_desc>& out, size_t max_bytes, size_t min_bytes, bool) override {
+        std::lock_guard<std::mutex> lk(c->comb_mu);
+        size_t have = 0;
+        for (auto* q : c->comb_q) have += q->d.n;
+        if (c->comb_q.empty() || have < min_bytes) return true;
+        size_t bytes = 0;
+        while (!c->comb_q.empty() && (out.empty() || bytes + c->comb_q.front()->d.n <= max_bytes)) {
+            gpz_ctx::ChunkCall* q = c->comb_q.front();
+            c->comb_q.pop_front();
+            bytes += q->d.n;
+            out.push_back(q->d);
+            taken.push_back(q);
+        }
+        return true;
+    }
+    int deliver(const uint8_t* data, size_t n) override {
+        gpz_ctx::ChunkCall* q = taken.front();
+        taken.pop_front();
+        q->o.out_len = n;
+        if (!q->o.out || q->o.out_cap < n) {
+            q->rc = GPZ_E_SPACE;  // this caller's buffer; the others go on
+        } else {
+            q->rc = GPZ_OK;
+            copies.push_back(CopyPool::Copy{q->o.out, data, n});
+        }
+        finished.push_back(q);
+        return GPZ_OK;
+    }
+    void pass_done() override {
+        copy_pool().run(copies);
+        copies.clear();
+        std::lock_guard<std::mutex> lk(c->comb_mu);
+        for (auto* q : finished) q->done = true;
+        finished.clear();
+        c->comb_cv.notify_all();
+    }
+};
+
+}  // namespace
+
+// Concurrent calls are combined: each call queues itself; a caller that
+// finds no leader becomes one and runs the pass loop over the queue until
+// it is empty and nothing is on the device, so the calls that arrive while
+// passes run join later passes without the pipeline draining in between
+// (BatchedLz77's submitter and completer threads, batch.rs:48-141).
 int gpz_compress_chunk(gpz_ctx* c, const uint8_t* in, size_t n, int level, uint8_t* out, size_t out_cap,
                        size_t* out_len) {
     if (!c || (!in && n) || !out_len) return GPZ_E_ARG;
-    constexpr int kNotRun = -1000;
     gpz_ctx::ChunkCall me;
     me.d = gpz_desc{in, n, level};
     me.o = gpz_out{out, out_cap, 0, 0};
@@ -1651,33 +1707,25 @@ int gpz_compress_chunk(gpz_ctx* c, const uint8_t* in, size_t n, int level, uint8
             continue;
         }
         c->comb_busy = true;
-        std::vector<gpz_ctx::ChunkCall*> batch;
-        size_t bytes = 0;
-        while (!c->comb_q.empty() && (batch.empty() || bytes + c->comb_q.front()->d.n <= c->batch_bytes)) {
-            batch.push_back(c->comb_q.front());
-            bytes += c->comb_q.front()->d.n;
-            c->comb_q.pop_front();
-        }
         q.unlock();
-        std::vector<gpz_desc> ds(batch.size());
-        std::vector<gpz_out> os(batch.size());
-        for (size_t i = 0; i < batch.size(); i++) {
-            ds[i] = batch[i]->d;
-            os[i] = batch[i]->o;
-            os[i].status = kNotRun;
-        }
-        int rc;
-        {
-            std::lock_guard<std::mutex> lk(c->mu);
-            cudaSetDevice(c->device);
-            rc = run_host_items(c, ds.data(), ds.size(), os.data(), false);
-        }
+        CombineFeed feed(c);
+        const int rc = gpz_stream_run(c, feed);
         q.lock();
-        for (size_t i = 0; i < batch.size(); i++) {
-            batch[i]->o = os[i];
-            // an item the batch never reached takes the batch's failure
-            batch[i]->rc = os[i].status != kNotRun ? os[i].status : (rc != GPZ_OK ? rc : GPZ_E_INTERNAL);
-            batch[i]->done = true;
+        // calls taken by a failed loop get its status; queued ones wait for
+        // the next leader
+        for (auto* t : feed.taken) {
+            t->rc = rc != GPZ_OK ? rc : GPZ_E_INTERNAL;
+            t->done = true;
+        }
+        for (auto* t : feed.finished) t->done = true;
+        if (rc != GPZ_OK) {
+            // the calls still queued would meet the same failure (a wait
+            // that timed out, an allocation): they return it too
+            for (auto* t : c->comb_q) {
+                t->rc = rc;
+                t->done = true;
+            }
+            c->comb_q.clear();
         }
         c->comb_busy = false;
         c->comb_cv.notify_all();

@@ -13,11 +13,14 @@
 // large), and only when at least min_bytes are ready or the stream has
 // ended; with `block` set it waits until that holds.  It returns false once
 // the stream has ended and every chunk has been taken.  deliver() gets each
-// taken chunk's compressed stream, in take order, from memory that is valid
-// only during the call; a nonzero return stops the stream.
+// taken chunk's compressed stream, in take order, from memory that stays
+// valid until pass_done() returns (after the deliveries of that pass); a
+// nonzero return stops the stream.
 struct GpzStreamFeed {
     virtual bool take(std::vector<gpz_desc>& out, size_t max_bytes, size_t min_bytes, bool block) = 0;
     virtual int deliver(const uint8_t* data, size_t n) = 0;
+    // after the deliveries of one pass, before its memory is reused
+    virtual void pass_done() {}
     virtual ~GpzStreamFeed() {}
 };
 
