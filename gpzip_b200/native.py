@@ -516,12 +516,12 @@ class Writer:
     """ParallelChunkedWriter over the library (gpz_writer_*): a file-like
     object whose bytes are cut into `chunk_size` chunks and written as gzip
     members, in order, to `dst` (anything with a write method).  With `ctx`
-    the chunks go through the device, `max_in_flight` at a time as one batch
-    on the writer's thread; with `chunk_fn` (bytes -> gzip bytes) through
-    that function instead, as the reference's writer takes any ChunkFn, and
-    with `hybrid` (a Hybrid) through the hybrid CPU + GPU chunk function; in
-    both, up to `max_in_flight` chunk calls run at once on the writer's
-    worker threads.  flush() does not cut a chunk; close() writes the last
+    the chunks go through the device: page-locked chunk buffers, streamed
+    by the writer's thread through the context's pass loop; with `chunk_fn`
+    (bytes -> gzip bytes) through that function instead, as the reference's
+    writer takes any ChunkFn, and with `hybrid` (a Hybrid) through the hybrid
+    CPU + GPU chunk function; in both, up to `max_in_flight` chunk calls run
+    at once on the writer's worker threads.  flush() does not cut a chunk; close() writes the last
     partial chunk and raises the first error the writer met."""
 
     def __init__(self, dst, ctx: "Context" = None, chunk_fn=None, chunk_size: int = 2 << 20, max_in_flight: int = 16,

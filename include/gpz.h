@@ -303,9 +303,13 @@ GPZ_API int gpz_stage_times(gpz_ctx* ctx, float* ms);
  * around the archive file (crates/gpzip-core/src/archive/pack.rs:144-176):
  * bytes written are cut into chunk_size chunks, the chunks are compressed
  * into independent gzip members, and the members reach `sink` in input
- * order.  With a device context, up to max_in_flight chunks are compressed
- * together as one batch on an internal thread while the caller fills the
- * next batch.
+ * order.  With a device context the chunks are page-locked buffers that an
+ * internal thread streams through the context's pipeline as they fill
+ * (passes of whatever is ready, overlapped on the device), while the caller
+ * fills the next ones; up to max(max_in_flight, 128 MiB / chunk_size)
+ * chunks are queued before gpz_writer_write waits.  The writer holds its
+ * context while it has chunks on the device: the sink must not call into
+ * that context.
  *
  *  - sink(user, buf, n) returns 0 on success; it is called from the
  *    writer's internal threads, never concurrently, and with members in
