@@ -981,7 +981,8 @@ int gpz_stream_run(gpz_ctx* c, GpzStreamFeed& feed) {
         const size_t cap = c->batch_bytes >> (pass < 2 ? 4 - 2 * pass : 0);
         const bool busy = !pend.empty();
         items.clear();
-        feed.take(items, cap, busy ? std::min<size_t>(cap, 8u << 20) : 1, false);
+        // an idle device takes whatever is queued, empty inputs included
+        feed.take(items, cap, busy ? std::min<size_t>(cap, 8u << 20) : 0, false);
         if (items.empty()) {
             if (!busy) break;  // nothing ready and nothing on the device
             settle();

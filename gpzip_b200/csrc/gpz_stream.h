@@ -12,7 +12,8 @@
 // are delivered): at most max_bytes of them (at least one chunk, however
 // large), and only when at least min_bytes are ready or the stream has
 // ended; with `block` set it waits until that holds.  It returns false once
-// the stream has ended and every chunk has been taken.  deliver() gets each
+// the stream has ended and every chunk has been taken.  With min_bytes 0
+// any queued chunk is ready, an empty one included.  deliver() gets each
 // taken chunk's compressed stream, in take order, from memory that stays
 // valid until pass_done() returns (after the deliveries of that pass); a
 // nonzero return stops the stream.
@@ -30,7 +31,7 @@ struct GpzStreamFeed {
 // grow from 1/16 of the pass size to the whole of it, every pass holds
 // whatever is ready up to that size, and a pass is started while others are
 // on the device only when at least 8 MiB (or the rest of the stream) is
-// ready.  Holds the context for as long as it runs.  The first failure is
+// ready; with nothing on the device, any ready chunk starts one.  Holds the context for as long as it runs.  The first failure is
 // returned; chunks after it are not delivered.
 int gpz_stream_run(gpz_ctx* ctx, GpzStreamFeed& feed);
 
