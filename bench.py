@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--cpu-sample-mib", type=int, default=0,
                     help="MiB of the workload the CPU port times per step (0: all of it)")
     ap.add_argument("--no-configs", action="store_true", help="skip the per-config (text, binary) lines")
+    ap.add_argument("--codec", default="gzip", choices=["gzip", "zstd"],
+                    help="codec of the device-resident measurement (zstd: for profiling its kernels)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baselines (quick runs)")
     ap.add_argument("--no-uneven", action="store_true", help="skip the uneven-file batched vs plain measurement")
     ap.add_argument("--device-only", action="store_true",
@@ -751,9 +753,11 @@ def main():
     data, desc = workload(args.workload)
     stream = torch.cuda.current_stream()
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=f"cuda:{local}")
-    ctx = native.Context(device=local, member_bytes=MEMBER, flags=native.GPZ_FLAG_STAGE_TIMING)
+    zstd_main = args.codec == "zstd"
+    ctx = native.Context(device=local, member_bytes=MEMBER, flags=native.GPZ_FLAG_STAGE_TIMING,
+                         codec=native.GPZ_CODEC_ZSTD if zstd_main else native.GPZ_CODEC_GZIP)
     dev = device_measure(ctx, data, args.workload, args.steps, args.warmup, stream, flush, local, rank, barrier,
-                         clocks=True)
+                         clocks=True, check=zstd_check if zstd_main else gzip_check)
     ratio, parity, clk = dev["ratio"], dev["parity"], dev["clocks"]
     launches = dev["launches"] * args.steps
     t = torch.tensor([dev["total_ms"]], device=f"cuda:{local}", dtype=torch.float64)
@@ -778,7 +782,7 @@ def main():
     chunk_fn = None if args.device_only else chunk_fn_rate(ectx, [np.ascontiguousarray(data[o:o + n]) for o, n in spans])
 
     stage_ms = dev["stage_ms"]
-    names = native.STAGE_NAMES
+    names = native.STAGE_NAMES_ZSTD if zstd_main else native.STAGE_NAMES
     dom = int(np.argmax(stage_ms))
     roofline = roofline_of(names[dom], stage_ms[dom], data.size, ratio, clk)
 
