@@ -1188,12 +1188,16 @@ struct ServeEngine {
     static constexpr size_t kMaxRequests = 1u << 20;
     // Overload.  Small requests are kept within a few ms of work: a small
     // request is admitted while the small lane's queue (not yet launched)
-    // holds at most kSmallBacklog bytes.  Large requests yield first: one is
-    // admitted only while the pool has kSmallReserve bytes to spare for the
-    // small lane and the small lane's queue is below half its limit, and a
-    // large batch is launched only while no small work waits (for at most
-    // kLargeHoldMs, so the large lane always moves).
-    static constexpr size_t kSmallBacklog = 24u << 20;
+    // holds at most kSmallBacklog bytes (about 2 ms of the small lane's
+    // measured rate).  Large requests yield first: one is admitted only while
+    // the pool has kSmallReserve bytes to spare for the small lane and the
+    // small lane's queue is below half its limit, and while more than one
+    // small batch waits, a large batch is launched only after that backlog
+    // clears (for at most kLargeHoldMs, so the large lane always moves).
+    // Measured over 60 s at 50k req/s with a 24 MiB limit and a hold on any
+    // waiting small work: p99 of small requests 6.6 ms, and the large lane
+    // lost throughput at 10k req/s.
+    static constexpr size_t kSmallBacklog = 12u << 20;
     static constexpr size_t kSmallReserve = 1ull << 30;
     static constexpr double kLargeHoldMs = 20.0;
 
@@ -1424,14 +1428,14 @@ struct ServeEngine {
                     // small work first: a large batch waits while small
                     // requests are queued, up to kLargeHoldMs
                     const double t_hold = now_ms();
-                    while (!stop && lanes[0].backlog > 0 && now_ms() - t_hold < kLargeHoldMs)
+                    while (!stop && lanes[0].backlog > lanes[0].batch_cap && now_ms() - t_hold < kLargeHoldMs)
                         L.cv_work.wait_for(lk, std::chrono::microseconds(200));
                     if (stop) return;
                     if (L.q.empty() || free_slot_of(L) < 0) continue;
                 }
                 k = free_slot_of(L);
                 batch = take_batch(L);
-                if (&L == &lanes[0] && lanes[0].backlog == 0) lanes[1].cv_work.notify_one();
+                if (&L == &lanes[0] && lanes[0].backlog <= lanes[0].batch_cap) lanes[1].cv_work.notify_one();
                 L.slot_free[k] = false;
                 const double tl = now_ms(), q = tl - batch.front().req->t_arrive;
                 max_queue_ms = std::max(max_queue_ms, q);
