@@ -19,11 +19,14 @@
 // stored raw.  The last block of the frame carries the last-block flag; an
 // empty input is one empty raw block.
 //
-//   k_zblock  one warp per tile: literal and match counts (the tile's
-//             symbol histogram), the literals scattered by ballots, and the
-//             FSE bitstream by one lane walking the tokens backwards.  The
-//             block content goes to the tile's slice of `pp` (free after
-//             the walk).  The last CTA places every member and tile.
+//   k_zblock  one CTA per tile, in shared memory: literal and match
+//             counts and the literals scattered by ballots; each sequence's
+//             codes; the three FSE state chains (literal lengths, match
+//             lengths, offsets) run last sequence to first, one lane each,
+//             recording the states; then every thread packs a run of
+//             sequences' bits at offsets from a block scan.  The block
+//             content goes to the tile's slice of `pp` (free after the
+//             walk).  The last CTA places every member and tile.
 //   k_zcopy   per tile: the block header and content (or the raw input) to
 //             the batch output; per input, the frame header.
 #include <cuda_runtime.h>
@@ -41,94 +44,111 @@ struct ZTab {
     uint32_t nbits[53];  // (max bits << 16) - (count << max bits)
     int32_t log;
 };
-__constant__ ZTab c_zt[3];  // literal lengths, match lengths, offsets
-__constant__ uint8_t c_ll_code[64];
-__constant__ uint8_t c_ml_code[128];
-__constant__ uint32_t c_ll_base[36];
-__constant__ uint8_t c_ll_bits[36];
-__constant__ uint32_t c_ml_base[53];
-__constant__ uint8_t c_ml_bits[53];
+// Every table the block encoder reads.  Each CTA keeps a copy in shared
+// memory: the threads of a warp index it with different symbols.
+struct ZConst {
+    ZTab t[3];  // literal lengths, match lengths, offsets
+    uint32_t ll_base[36];
+    uint32_t ml_base[53];
+    uint8_t ll_code[64];
+    uint8_t ml_code[128];
+    uint8_t ll_bits[36];
+    uint8_t ml_bits[53];
+    uint8_t pad[3];
+};
+static_assert(sizeof(ZConst) % 4 == 0, "ZConst is copied in words");
+__constant__ ZConst c_z;
 
-constexpr int kZWarps = 4;
-constexpr int kZThreads = kZWarps * 32;
+constexpr int kZThreads = 128;  // one CTA per tile
+constexpr int kZWarps = kZThreads / 32;
 constexpr int kCopyThreads = 128;
 constexpr uint32_t kCompressed = 1u << 31;
+constexpr uint32_t kZMaxSeq = (GPZ_SEG + 2u) / 3u;  // a tile's matches start at least 3 bytes apart
+constexpr uint32_t kZBuf = GPZ_SEG + 320u;          // content bytes; a tile decodes to at most 4096 + 257
 
 // literal-length and match-length codes (RFC 8878 3.1.1.3.2.1.1)
-__device__ __forceinline__ uint32_t ll_code(uint32_t ll) {
-    return ll < 64u ? c_ll_code[ll] : 31u - __clz(ll) + 19u;
+__device__ __forceinline__ uint32_t ll_code(const ZConst& z, uint32_t ll) {
+    return ll < 64u ? z.ll_code[ll] : 31u - __clz(ll) + 19u;
 }
-__device__ __forceinline__ uint32_t ml_code(uint32_t ml) {
+__device__ __forceinline__ uint32_t ml_code(const ZConst& z, uint32_t ml) {
     const uint32_t m = ml - 3u;
-    return m < 128u ? c_ml_code[m] : 31u - __clz(m) + 36u;
+    return m < 128u ? z.ml_code[m] : 31u - __clz(m) + 36u;
 }
 
-// LSB-first bit writer into a byte buffer bounded by cap (overflow is
-// recorded, nothing is written past cap).
-struct BitW {
-    uint8_t* p;
-    uint32_t n, cap;
-    unsigned long long acc;
-    uint32_t fill;
-    bool over;
-
-    __device__ __forceinline__ void add(uint32_t v, uint32_t nb) {
-        acc |= (unsigned long long)(v & ((nb >= 32u) ? 0xFFFFFFFFu : ((1u << nb) - 1u))) << fill;
-        fill += nb;
-        while (fill >= 8u) {
-            if (n < cap) p[n] = (uint8_t)acc;
-            else over = true;
-            n++;
-            acc >>= 8;
-            fill -= 8u;
-        }
-    }
+// Shared memory of k_zblock: one tile at a time.
+struct ZBlockSmem {
+    ZConst z;
+    uint32_t out[kZBuf / 4];   // the block content, little-endian
+    uint16_t mpos[kZMaxSeq];   // token index of each match, in order
+    uint8_t sym[3][kZMaxSeq];  // literal-length, match-length and offset code of each sequence
+    uint8_t st[3][kZMaxSeq];   // each stream's state before the sequence is encoded, minus the table size
+    uint32_t cnt[kZWarps][2];  // literals and matches of each warp's share of the tokens
+    uint32_t part[kZWarps];    // bit counts of each warp's sequences
+    uint32_t fin[3];           // the streams' states after the first sequence
+    uint32_t tile;
 };
 
-__device__ __forceinline__ uint32_t fse_init(const ZTab& t, uint32_t s) {
-    const uint32_t nb = (t.nbits[s] + (1u << 15)) >> 16;
-    const uint32_t v = (nb << 16) - t.nbits[s];
-    return t.state[(int32_t)(v >> nb) + t.find[s]];
+// ORs the n low bits of f into `out` at bit g (LSB first); n <= 64.
+__device__ __forceinline__ void or_bits(uint32_t* out, uint32_t g, unsigned long long f, uint32_t n) {
+    if (!n) return;
+    const uint32_t w = g >> 5, s = g & 31u;
+    const unsigned long long lo = f << s;
+    atomicOr(&out[w], (uint32_t)lo);
+    if (s + n > 32u) atomicOr(&out[w + 1], (uint32_t)(lo >> 32));
+    if (s + n > 64u) atomicOr(&out[w + 2], (uint32_t)(f >> (64u - s)));
 }
 
-__device__ __forceinline__ void fse_enc(BitW& w, const ZTab& t, uint32_t& state, uint32_t s) {
-    const uint32_t nb = (state + t.nbits[s]) >> 16;
-    w.add(state, nb);
-    state = t.state[(int32_t)(state >> nb) + t.find[s]];
+// Bits of stream j's state for sequence k: the value and its width.
+__device__ __forceinline__ uint32_t state_bits(const ZBlockSmem& sm, int j, uint32_t k, uint32_t& nb) {
+    const ZTab& tb = sm.z.t[j];
+    const uint32_t state = sm.st[j][k] + (1u << tb.log);
+    nb = (state + tb.nbits[sm.sym[j][k]]) >> 16;
+    return state & ((1u << nb) - 1u);
 }
 
-// The encoder's state over the sequences of one block, last to first.
-struct SeqEnc {
-    BitW w;
-    uint32_t sll, sml, sof;
-    bool started;
-
-    // sequence (literal length ll, match length ml, distance d)
-    __device__ __forceinline__ void put(uint32_t ll, uint32_t ml, uint32_t d) {
-        const uint32_t llc = ll_code(ll), mlc = ml_code(ml), off = d + 3u, ofc = 31u - __clz(off);
-        if (!started) {
-            sml = fse_init(c_zt[1], mlc);
-            sof = fse_init(c_zt[2], ofc);
-            sll = fse_init(c_zt[0], llc);
-            started = true;
-        } else {
-            fse_enc(w, c_zt[2], sof, ofc);
-            fse_enc(w, c_zt[1], sml, mlc);
-            fse_enc(w, c_zt[0], sll, llc);
+// Bits that sequence k adds to the stream (the last sequence, which is
+// encoded first, only sets the states and adds no state bits).
+__device__ __forceinline__ uint32_t seq_nbits(const ZBlockSmem& sm, uint32_t k, bool first) {
+    uint32_t n = sm.z.ll_bits[sm.sym[0][k]] + sm.z.ml_bits[sm.sym[1][k]] + sm.sym[2][k];
+    if (!first) {
+        uint32_t nb;
+        for (int j = 0; j < 3; j++) {
+            state_bits(sm, j, k, nb);
+            n += nb;
         }
-        w.add(ll - c_ll_base[llc], c_ll_bits[llc]);
-        w.add(ml - c_ml_base[mlc], c_ml_bits[mlc]);
-        w.add(off - (1u << ofc), ofc);
     }
+    return n;
+}
 
-    __device__ __forceinline__ void close() {
-        w.add(sml, (uint32_t)c_zt[1].log);
-        w.add(sof, (uint32_t)c_zt[2].log);
-        w.add(sll, (uint32_t)c_zt[0].log);
-        w.add(1u, 1u);
-        if (w.fill) w.add(0u, 8u - w.fill);
+// The fields of sequence k in stream order: the offset, match-length and
+// literal-length state bits, then the literal-length, match-length and
+// offset extra bits.
+__device__ __forceinline__ unsigned long long seq_fields(const ZBlockSmem& sm, const uint32_t* tok, uint32_t k,
+                                                         bool first, uint32_t& n) {
+    const ZConst& z = sm.z;
+    const uint32_t i = sm.mpos[k];
+    const uint32_t ll = i - (k ? sm.mpos[k - 1] + 1u : 0u);
+    const uint32_t v = tok[i];
+    const uint32_t ml = v >> 16, off = (v & 0xFFFFu) + 3u;
+    const uint32_t llc = sm.sym[0][k], mlc = sm.sym[1][k], ofc = sm.sym[2][k];
+    unsigned long long f = 0;
+    n = 0;
+    if (!first) {
+        for (int j = 2; j >= 0; j--) {
+            uint32_t nb;
+            const uint32_t x = state_bits(sm, j, k, nb);
+            f |= (unsigned long long)x << n;
+            n += nb;
+        }
     }
-};
+    f |= (unsigned long long)(ll - z.ll_base[llc]) << n;
+    n += z.ll_bits[llc];
+    f |= (unsigned long long)(ml - z.ml_base[mlc]) << n;
+    n += z.ml_bits[mlc];
+    f |= (unsigned long long)(off - (1u << ofc)) << n;
+    n += ofc;
+    return f;
+}
 
 // True in the last CTA of the grid to finish (its global writes, and every
 // other CTA's, are visible to it).
@@ -193,16 +213,22 @@ __device__ void z_place(const BatchParams& bp) {
 // ------------------------------------------------------------------ k_zblock
 
 __global__ void __launch_bounds__(kZThreads) k_zblock(BatchParams bp) {
-    __shared__ uint32_t s_tile[kZWarps];
-    __shared__ uint32_t s_tok[kZWarps][32];
-    const int lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+    __shared__ ZBlockSmem sm;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t lt = (1u << lane) - 1u;
+    {
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(&c_z);
+        uint32_t* d = reinterpret_cast<uint32_t*>(&sm.z);
+        for (uint32_t i = tid; i < sizeof(ZConst) / 4; i += kZThreads) d[i] = src[i];
+    }
+    const ZConst& z = sm.z;
+    uint8_t* ob = reinterpret_cast<uint8_t*>(sm.out);
     const uint32_t ntiles = bp.dims[0];
     for (;;) {
-        if (lane == 0) s_tile[wi] = atomicAdd(&bp.counters[GPZ_CNT_HUFF], 1u);
-        __syncwarp();
-        const uint32_t t = s_tile[wi];
-        __syncwarp();
+        if (tid == 0) sm.tile = atomicAdd(&bp.counters[GPZ_CNT_HUFF], 1u);
+        for (uint32_t i = tid; i < kZBuf / 4; i += kZThreads) sm.out[i] = 0u;
+        __syncthreads();
+        const uint32_t t = sm.tile;
         if (t >= ntiles) break;
         const TileDesc td = bp.tiles[t];
         const MemberDesc md = bp.members[td.member];
@@ -214,114 +240,157 @@ __global__ void __launch_bounds__(kZThreads) k_zblock(BatchParams bp) {
         const uint32_t rawlen = b1 > b0 ? b1 - b0 : 0u;
         const uint32_t ntok = min(bp.tile_ntok[t], GPZ_SEG);
         const uint32_t* tok = bp.tok + md.in_off + start;
-        // literals and matches of the tile, from its symbol histogram
-        const uint16_t* hist = bp.tile_hist + (size_t)t * GPZ_NSYM;
-        uint32_t nlit = 0, nseq = 0;
-        for (uint32_t s = lane; s < 256u; s += 32u) nlit += hist[s];
-        if (lane < 29) nseq = hist[257 + lane];
-#pragma unroll
-        for (int o = 16; o; o >>= 1) {
-            nlit += __shfl_xor_sync(0xFFFFFFFFu, nlit, o);
-            nseq += __shfl_xor_sync(0xFFFFFFFFu, nseq, o);
+        // each warp takes a quarter of the tokens and counts its literals
+        // and matches
+        const uint32_t span = (ntok + kZThreads - 1u) / kZThreads * 32u;
+        const uint32_t w0 = min(ntok, (uint32_t)warp * span), w1 = min(ntok, w0 + span);
+        uint32_t nl = 0, nm = 0;
+        for (uint32_t c = w0; c < w1; c += 32u) {
+            const uint32_t i = c + lane;
+            const uint32_t v = i < w1 ? tok[i] : 0u;
+            nl += __popc(__ballot_sync(0xFFFFFFFFu, i < w1 && (v >> 16) == 0u));
+            nm += __popc(__ballot_sync(0xFFFFFFFFu, i < w1 && (v >> 16) != 0u));
+        }
+        if (lane == 0) {
+            sm.cnt[warp][0] = nl;
+            sm.cnt[warp][1] = nm;
+        }
+        __syncthreads();
+        uint32_t nlit = 0, nseq = 0, lbase = 0, mbase = 0;
+        for (int w = 0; w < kZWarps; w++) {
+            if (w == warp) {
+                lbase = nlit;
+                mbase = nseq;
+            }
+            nlit += sm.cnt[w][0];
+            nseq += sm.cnt[w][1];
         }
         const uint32_t lh = nlit < 32u ? 1u : nlit < 4096u ? 2u : 3u;
         const uint32_t sh = nseq < 128u ? 1u : nseq < 0x7F00u ? 2u : 3u;
-        // the content must be smaller than rawlen to be used; the tile's
-        // slice of pp (4 bytes per position of the tile) holds it
-        uint8_t* dst = reinterpret_cast<uint8_t*>(bp.pp + md.in_off + start);
-        const uint32_t cap = rawlen;
-        bool comp = lh + nlit + sh + (nseq ? 1u : 0u) < cap;
-        uint32_t csize = 0;
-        if (comp) {
-            if (lane == 0) {
-                if (lh == 1u) {
-                    dst[0] = (uint8_t)(nlit << 3);
-                } else if (lh == 2u) {
-                    dst[0] = (uint8_t)(((nlit & 15u) << 4) | 4u);
-                    dst[1] = (uint8_t)(nlit >> 4);
-                } else {
-                    dst[0] = (uint8_t)(((nlit & 15u) << 4) | 12u);
-                    dst[1] = (uint8_t)(nlit >> 4);
-                    dst[2] = (uint8_t)(nlit >> 12);
-                }
-            }
-            // literals in token order, ranked by ballots
-            uint32_t lbase = lh;
-            for (uint32_t c = 0; c < ntok; c += 32u) {
-                const uint32_t i = c + lane;
-                const uint32_t v = i < ntok ? tok[i] : 0xFFFFFFFFu;
-                const bool lit = i < ntok && (v >> 16) == 0u;
-                const uint32_t m = __ballot_sync(0xFFFFFFFFu, lit);
-                if (lit) dst[lbase + __popc(m & lt)] = (uint8_t)v;
-                lbase += __popc(m);
-            }
-            // sequences section header
-            const uint32_t q = lh + nlit;
-            if (lane == 0) {
-                if (sh == 1u) {
-                    dst[q] = (uint8_t)nseq;
-                } else if (sh == 2u) {
-                    dst[q] = (uint8_t)((nseq >> 8) + 0x80u);
-                    dst[q + 1] = (uint8_t)nseq;
-                } else {
-                    dst[q] = 0xFF;
-                    dst[q + 1] = (uint8_t)(nseq - 0x7F00u);
-                    dst[q + 2] = (uint8_t)((nseq - 0x7F00u) >> 8);
-                }
-                if (nseq) dst[q + sh] = 0;  // predefined modes
-            }
-            csize = q + sh;
-            if (nseq) {
-                // FSE: one lane walks the tokens backwards.  A match waits
-                // until the match before it is reached: the literals in
-                // between are its literal length.  Tokens come 32 at a
-                // time through shared memory.
-                SeqEnc e{};
-                e.w = BitW{dst + q + sh + 1u, 0u, cap - (q + sh + 1u), 0ull, 0u, false};
-                bool pend = false;
-                uint32_t pml = 0, pd = 0, run = 0;
-                const uint32_t top = (ntok + 31u) & ~31u;
-                for (uint32_t c = top; c > 0; c -= 32u) {
-                    const uint32_t c0 = c - 32u, i = c0 + lane;
-                    const uint32_t v = i < ntok ? tok[i] : 0u;
-                    s_tok[wi][lane] = v;
-                    const bool valid = i < ntok;
-                    const uint32_t mm = __ballot_sync(0xFFFFFFFFu, valid && (v >> 16) != 0u);
-                    const uint32_t lm = __ballot_sync(0xFFFFFFFFu, valid && (v >> 16) == 0u);
-                    __syncwarp();
-                    if (lane == 0) {
-                        uint32_t left = mm, upper = 32u;
-                        while (left) {
-                            // the literals strictly between match j and
-                            // the match (or chunk end) above it
-                            const uint32_t j = 31u - __clz(left);
-                            const uint32_t above_j = j >= 31u ? 0u : ~0u << (j + 1u);
-                            const uint32_t below_up = upper >= 32u ? ~0u : (1u << upper) - 1u;
-                            run += __popc(lm & above_j & below_up);
-                            if (pend) e.put(run, pml, pd);
-                            const uint32_t tv = s_tok[wi][j];
-                            pend = true;
-                            pml = tv >> 16;
-                            pd = tv & 0xFFFFu;
-                            run = 0;
-                            upper = j;
-                            left &= ~(1u << j);
-                        }
-                        run += __popc(lm & (upper >= 32u ? ~0u : ((1u << upper) - 1u)));
-                    }
-                    __syncwarp();
-                }
-                if (lane == 0) {
-                    if (pend) e.put(run, pml, pd);
-                    e.close();
-                    csize = q + sh + 1u + e.w.n;
-                    if (e.w.over) csize = cap;
-                }
-                csize = __shfl_sync(0xFFFFFFFFu, csize, 0);
-            }
-            comp = csize < cap;
+        const uint32_t q = lh + nlit;                      // the sequences section
+        const uint32_t body = q + sh + (nseq ? 1u : 0u);  // the FSE bitstream
+        // the content is used only when it is smaller than the bytes it
+        // decodes to
+        bool comp = body < rawlen;
+        if (rawlen > kZBuf || nseq > kZMaxSeq) {
+            // a tile decodes to at most 4096 + 257 bytes and its matches
+            // start at least 3 bytes apart, so this is never reached
+            if (tid == 0) atomicOr(bp.err, GPZ_ERRBIT_BITS);
+            comp = false;
         }
-        if (lane == 0) bp.tile_zinfo[t] = comp ? (csize | kCompressed) : rawlen;
+        uint32_t csize = body;
+        if (comp) {
+            // literals in token order, and the token index of each match
+            for (uint32_t c = w0; c < w1; c += 32u) {
+                const uint32_t i = c + lane;
+                const uint32_t v = i < w1 ? tok[i] : 0u;
+                const bool lit = i < w1 && (v >> 16) == 0u, mat = i < w1 && (v >> 16) != 0u;
+                const uint32_t bl = __ballot_sync(0xFFFFFFFFu, lit), bm = __ballot_sync(0xFFFFFFFFu, mat);
+                if (lit) ob[lh + lbase + __popc(bl & lt)] = (uint8_t)v;
+                if (mat) sm.mpos[mbase + __popc(bm & lt)] = (uint16_t)i;
+                lbase += __popc(bl);
+                mbase += __popc(bm);
+            }
+            if (tid == 0) {
+                if (lh == 1u) {
+                    ob[0] = (uint8_t)(nlit << 3);
+                } else if (lh == 2u) {
+                    ob[0] = (uint8_t)(((nlit & 15u) << 4) | 4u);
+                    ob[1] = (uint8_t)(nlit >> 4);
+                } else {
+                    ob[0] = (uint8_t)(((nlit & 15u) << 4) | 12u);
+                    ob[1] = (uint8_t)(nlit >> 4);
+                    ob[2] = (uint8_t)(nlit >> 12);
+                }
+                if (sh == 1u) {
+                    ob[q] = (uint8_t)nseq;
+                } else if (sh == 2u) {
+                    ob[q] = (uint8_t)((nseq >> 8) + 0x80u);
+                    ob[q + 1] = (uint8_t)nseq;
+                } else {
+                    ob[q] = 0xFF;
+                    ob[q + 1] = (uint8_t)(nseq - 0x7F00u);
+                    ob[q + 2] = (uint8_t)((nseq - 0x7F00u) >> 8);
+                }
+                if (nseq) ob[q + sh] = 0;  // predefined modes
+            }
+            __syncthreads();
+        }
+        if (comp && nseq) {
+            // each sequence's codes
+            for (uint32_t k = tid; k < nseq; k += kZThreads) {
+                const uint32_t i = sm.mpos[k];
+                const uint32_t v = tok[i];
+                sm.sym[0][k] = (uint8_t)ll_code(z, i - (k ? sm.mpos[k - 1] + 1u : 0u));
+                sm.sym[1][k] = (uint8_t)ml_code(z, v >> 16);
+                sm.sym[2][k] = (uint8_t)(31u - __clz((v & 0xFFFFu) + 3u));
+            }
+            __syncthreads();
+            // the three FSE state chains, last sequence to first: one lane
+            // each (literal lengths, match lengths, offsets)
+            if (warp == 0 && lane < 3) {
+                const ZTab& tb = z.t[lane];
+                const uint32_t size = 1u << tb.log;
+                const uint8_t* sy = sm.sym[lane];
+                uint8_t* so = sm.st[lane];
+                uint32_t s = sy[nseq - 1u];
+                const uint32_t nb0 = (tb.nbits[s] + (1u << 15)) >> 16;
+                uint32_t state = tb.state[(int32_t)(((nb0 << 16) - tb.nbits[s]) >> nb0) + tb.find[s]];
+#pragma unroll 4
+                for (int k = (int)nseq - 2; k >= 0; k--) {
+                    s = sy[k];
+                    const uint32_t nb = (state + tb.nbits[s]) >> 16;
+                    so[k] = (uint8_t)(state - size);
+                    state = tb.state[(int32_t)(state >> nb) + tb.find[s]];
+                }
+                sm.fin[lane] = state;
+            }
+            __syncthreads();
+            // bit offsets: every thread takes a run of sequences in stream
+            // order (slot p holds sequence nseq - 1 - p), then a block scan
+            const uint32_t per = (nseq + kZThreads - 1u) / kZThreads;
+            const uint32_t p0 = min(nseq, (uint32_t)tid * per), p1 = min(nseq, p0 + per);
+            uint32_t mine = 0;
+            for (uint32_t p = p0; p < p1; p++) mine += seq_nbits(sm, nseq - 1u - p, p == 0u);
+            uint32_t x = mine;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+                if (lane >= o) x += y;
+            }
+            if (lane == 31) sm.part[warp] = x;
+            __syncthreads();
+            uint32_t before = x - mine, total = 0;
+            for (int w = 0; w < kZWarps; w++) {
+                if (w < warp) before += sm.part[w];
+                total += sm.part[w];
+            }
+            // the stream ends with the three final states and a 1 bit
+            csize = body + ((total + 18u + 7u) >> 3);
+            comp = csize < rawlen;
+            if (comp) {
+                uint32_t g = body * 8u + before;
+                for (uint32_t p = p0; p < p1; p++) {
+                    uint32_t n;
+                    const unsigned long long f = seq_fields(sm, tok, nseq - 1u - p, p == 0u, n);
+                    or_bits(sm.out, g, f, n);
+                    g += n;
+                }
+                if (tid == 0) {
+                    const unsigned long long f = (unsigned long long)(sm.fin[1] & 63u) |
+                                                 ((unsigned long long)(sm.fin[2] & 31u) << 6) |
+                                                 ((unsigned long long)(sm.fin[0] & 63u) << 11) | (1ull << 17);
+                    or_bits(sm.out, body * 8u + total, f, 18u);
+                }
+            }
+            __syncthreads();
+        }
+        if (comp) {
+            uint32_t* dst = bp.pp + md.in_off + start;  // the tile's slice of pp, free after the walk
+            for (uint32_t i = tid; i < (csize + 3u) / 4u; i += kZThreads) dst[i] = sm.out[i];
+        }
+        if (tid == 0) bp.tile_zinfo[t] = comp ? (csize | kCompressed) : rawlen;
+        __syncthreads();
     }
     if (z_last_cta(&bp.counters[GPZ_CNT_HUFF_DONE])) z_place(bp);
 }
@@ -421,28 +490,29 @@ int gpz_zstd_setup() {
     static const uint8_t ml_bits[53] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0,
                                         0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 1, 1, 1, 1,
                                         2, 2, 3, 3, 4, 4, 5, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16};
-    ZTab tabs[3];
-    build_tab(tabs[0], ll_norm, 36, 6);
-    build_tab(tabs[1], ml_norm, 53, 6);
-    build_tab(tabs[2], of_norm, 29, 5);
-    uint8_t llc[64], mlc[128];
+    ZConst z{};
+    build_tab(z.t[0], ll_norm, 36, 6);
+    build_tab(z.t[1], ml_norm, 53, 6);
+    build_tab(z.t[2], of_norm, 29, 5);
     for (uint32_t v = 0; v < 64; v++) {
         int c = 35;
         while (ll_base[c] > v) c--;
-        llc[v] = (uint8_t)c;
+        z.ll_code[v] = (uint8_t)c;
     }
     for (uint32_t m = 0; m < 128; m++) {
         int c = 52;
         while (ml_base[c] > m + 3u) c--;
-        mlc[m] = (uint8_t)c;
+        z.ml_code[m] = (uint8_t)c;
     }
-    if (cudaMemcpyToSymbol(c_zt, tabs, sizeof tabs) != cudaSuccess ||
-        cudaMemcpyToSymbol(c_ll_code, llc, sizeof llc) != cudaSuccess ||
-        cudaMemcpyToSymbol(c_ml_code, mlc, sizeof mlc) != cudaSuccess ||
-        cudaMemcpyToSymbol(c_ll_base, ll_base, sizeof ll_base) != cudaSuccess ||
-        cudaMemcpyToSymbol(c_ll_bits, ll_bits, sizeof ll_bits) != cudaSuccess ||
-        cudaMemcpyToSymbol(c_ml_base, ml_base, sizeof ml_base) != cudaSuccess ||
-        cudaMemcpyToSymbol(c_ml_bits, ml_bits, sizeof ml_bits) != cudaSuccess)
+    for (int i = 0; i < 36; i++) {
+        z.ll_base[i] = ll_base[i];
+        z.ll_bits[i] = ll_bits[i];
+    }
+    for (int i = 0; i < 53; i++) {
+        z.ml_base[i] = ml_base[i];
+        z.ml_bits[i] = ml_bits[i];
+    }
+    if (cudaMemcpyToSymbol(c_z, &z, sizeof z) != cudaSuccess)
         return -1;
     return 0;
 }
@@ -463,7 +533,7 @@ int gpz_launch_zstd(const BatchParams& bp, void* stream, void* const* events, in
     auto mark = [&](int i) {
         if (events) cudaEventRecord(static_cast<cudaEvent_t>(events[i]), s);
     };
-    const int gb = grid_blocks > 0 ? grid_blocks : (int)((bp.ntiles + kZWarps - 1) / kZWarps + 1);
+    const int gb = grid_blocks > 0 ? grid_blocks : (int)(bp.ntiles ? bp.ntiles : 1u);
     const int gc = grid_copy > 0 ? grid_copy : (int)(bp.ntiles ? bp.ntiles : 1u);
     k_zblock<<<gb, kZThreads, 0, s>>>(bp);
     mark(4);
