@@ -325,7 +325,9 @@ static_assert(kRowEntries % 4 == 0 && kRowEntries / 2 >= GPZ_SEG, "four passes m
 
 // One CTA per 4 KiB tile S of a member (persistent over tiles); two CTAs
 // share an SM, so one's barriers and loads overlap the other's candidate
-// evaluation.  The window [S-8, S] plus 320 bytes of lookahead is staged in
+// evaluation.  The launch bound holds every form to two CTAs per SM:
+// 56 registers at 512 threads, 40 at 768, 32 at 1024 (48 and 64 warps per
+// SM), none of them spilling; the shared memory (115,008 bytes) fits twice.  The window [S-8, S] plus 320 bytes of lookahead is staged in
 // shared memory, and the tile's hash set is rebuilt from its keys.  The
 // keys of segments S-1 .. S-8 are looked up in that set, which gives, for
 // every hash of the tile, the newest and oldest position in each of those
@@ -339,7 +341,7 @@ static_assert(kRowEntries % 4 == 0 && kRowEntries / 2 >= GPZ_SEG, "four passes m
 // the back segments are joined and evaluated a few at a time, in order,
 // with each position's best carried between passes.
 template <int T>
-__global__ void __launch_bounds__(T, 1024 / T) k_lookup(BatchParams bp) {
+__global__ void __launch_bounds__(T, 2) k_lookup(BatchParams bp) {
     extern __shared__ __align__(16) uint8_t smem[];
     uint8_t* win = smem + LookupSmem::kWin;
     const uint32_t* w32 = reinterpret_cast<const uint32_t*>(win);
@@ -348,7 +350,7 @@ __global__ void __launch_bounds__(T, 1024 / T) k_lookup(BatchParams bp) {
     uint16_t* own_old = reinterpret_cast<uint16_t*>(smem + LookupSmem::kOwnOld);
     uint32_t* bestv = reinterpret_cast<uint32_t*>(smem + LookupSmem::kBest);
     uint32_t* rows = reinterpret_cast<uint32_t*>(smem + LookupSmem::kRows);
-    constexpr int PER = GPZ_SEG / T;
+    constexpr int PER = (GPZ_SEG + T - 1) / T;  // keys per thread in the join
     __shared__ uint32_t s_tile;
     const int tid = threadIdx.x;
 
@@ -1923,10 +1925,13 @@ int gpz_kernel_smem_setup() {
     if (cudaFuncSetAttribute(k_segtab<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SegtabSmem::kBytes) !=
         cudaSuccess)
         return -1;
+    // two lookup CTAs per SM need the largest shared-memory carveout
     const int smem = (int)LookupSmem::kBytes;
-    if (cudaFuncSetAttribute(k_lookup<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) return -1;
-    if (cudaFuncSetAttribute(k_lookup<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
-        return -1;
+    for (const void* f : {(const void*)k_lookup<512>, (const void*)k_lookup<768>, (const void*)k_lookup<1024>})
+        if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess ||
+            cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared) !=
+                cudaSuccess)
+            return -1;
     return 0;
 }
 
@@ -1948,6 +1953,7 @@ int gpz_launch_batch(const BatchParams& bp, const LaunchShape& ls, void* stream,
     mark(1);
     switch (ls.lookup_threads) {
         case 512: k_lookup<512><<<gl, 512, LookupSmem::kBytes, s>>>(bp); break;
+        case 768: k_lookup<768><<<gl, 768, LookupSmem::kBytes, s>>>(bp); break;
         default: k_lookup<1024><<<gl, 1024, LookupSmem::kBytes, s>>>(bp); break;
     }
     mark(2);
@@ -2004,9 +2010,10 @@ int gpz_occupancy(LaunchShape* persistent) {
         return n;
     };
     persistent->segtab_grid = sms * occ((const void*)k_segtab<512>, 512, SegtabSmem::kBytes);
-    persistent->lookup_grid = sms * occ(persistent->lookup_threads == 512 ? (const void*)k_lookup<512>
-                                                                           : (const void*)k_lookup<1024>,
-                                        persistent->lookup_threads, LookupSmem::kBytes);
+    const void* lookup_fn = persistent->lookup_threads == 512   ? (const void*)k_lookup<512>
+                            : persistent->lookup_threads == 768 ? (const void*)k_lookup<768>
+                                                                : (const void*)k_lookup<1024>;
+    persistent->lookup_grid = sms * occ(lookup_fn, persistent->lookup_threads, LookupSmem::kBytes);
     const void* walk_fn = persistent->walk_threads == 1024 ? (const void*)k_walk_mark_blk<512>
                           : persistent->walk_threads == 256  ? (const void*)k_walk_mark_warp<256>
                                                              : (const void*)k_walk_mark_warp<512>;

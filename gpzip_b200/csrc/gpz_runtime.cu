@@ -627,16 +627,17 @@ void default_shapes(gpz_ctx* c) {
 // also loads its module, which would otherwise count against whichever
 // candidate uses it first.
 int autotune(gpz_ctx* c, Slot& sl, const BatchParams& bp, const DrainTarget* dt, cudaStream_t s) {
-    const int lt[2] = {1024, 512}, wt[2] = {512, 1024}, et[2] = {512, 256};
+    const int lt[3] = {1024, 768, 512}, wt[2] = {512, 1024}, et[2] = {512, 256};
+    constexpr int kCands = 12;
     float best = 1e30f;
     LaunchShape best_s = c->shape[sl.bucket];
     cudaEvent_t a, b;
     CU(c, cudaEventCreate(&a));
     CU(c, cudaEventCreate(&b));
     int rc = GPZ_OK;
-    for (int i = 0; i < 16 && rc == GPZ_OK; i++) {
-        const int k = i & 7;
-        LaunchShape cand{lt[k & 1], 0, wt[(k >> 1) & 1], 0, et[(k >> 2) & 1], 0, 0, 0};
+    for (int i = 0; i < 2 * kCands && rc == GPZ_OK; i++) {
+        const int k = i % kCands;
+        LaunchShape cand{lt[k % 3], 0, wt[(k / 3) & 1], 0, et[(k / 6) & 1], 0, 0, 0};
         gpz_occupancy(&cand);
         cudaEventRecord(a, s);
         rc = launch(c, sl, bp, cand, false, dt, false, s);
@@ -645,7 +646,7 @@ int autotune(gpz_ctx* c, Slot& sl, const BatchParams& bp, const DrainTarget* dt,
         if (rc == GPZ_E_TIMEOUT && cudaEventRecord(sl.done, s) == cudaSuccess) sl.stale = true;
         float ms = 0;
         cudaEventElapsedTime(&ms, a, b);
-        if (rc == GPZ_OK && i >= 8 && ms < best) {
+        if (rc == GPZ_OK && i >= kCands && ms < best) {
             best = ms;
             best_s = cand;
         }
@@ -2121,7 +2122,7 @@ int gpz_get_shape(gpz_ctx* c, gpz_shape* s) {
 int gpz_set_shape(gpz_ctx* c, const gpz_shape* s) {
     if (!c || !s) return GPZ_E_ARG;
     auto ok_t = [](int t) { return t == 256 || t == 512; };
-    if (!(s->lookup_threads == 512 || s->lookup_threads == 1024) ||
+    if (!(s->lookup_threads == 512 || s->lookup_threads == 768 || s->lookup_threads == 1024) ||
         !(s->walk_threads == 256 || s->walk_threads == 512 || s->walk_threads == 1024) || !ok_t(s->emit_threads) || s->lookup_grid < 0 || s->walk_grid < 0 || s->emit_grid < 0)
         return GPZ_E_ARG;
     std::lock_guard<std::mutex> lk(c->mu);

@@ -215,7 +215,7 @@ GPZ_API const char* gpz_strerror(int status);
 /* Last CUDA / device diagnostic of this context (static storage). */
 GPZ_API const char* gpz_last_error(gpz_ctx* ctx);
 
-/* Launch geometry in use: threads per CTA for lookup (512, 1024) and emit
+/* Launch geometry in use: threads per CTA for lookup (512, 768, 1024) and emit
  * (256, 512) and the persistent grid sizes (0 = one CTA per tile).  The walk
  * has two forms with identical output: walk_threads 256 or 512 walks one
  * tile per warp (throughput), 1024 walks one tile per 512-thread CTA by

@@ -69,10 +69,12 @@ def test_graph_reuse_across_batch_sizes(ctx):
 
 
 def test_every_launch_shape_gives_the_same_bytes(ctx):
-    data = W.logs(700_000, seed=9).tobytes()
+    # logs, and binary data whose tiles hold more distinct hashes than one
+    # join pass takes
+    data = W.logs(700_000, seed=9).tobytes() + W.binary(300_000, seed=19).tobytes()
     want = O.gzip_chunk(data, 131072)
     keep = ctx.get_shape()
-    for lt in (1024, 512):
+    for lt in (1024, 768, 512):
         for wt in (1024, 512, 256):
             for et in (512, 256):
                 ctx.set_shape(native.Shape(lt, 0, wt, 0, et, 0))
