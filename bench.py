@@ -772,8 +772,8 @@ def main():
     # end to end through the public host API (host buffers, copies inside),
     # on a context with the production settings (graphs, autotuned shapes)
     ectx = native.Context(device=local, member_bytes=MEMBER)
-    e2e = e2e_measure(ectx, data, args.workload, 1 if args.device_only else max(2, args.steps // 2),
-                      0 if args.device_only else max(args.warmup, 2), stream, local, rank, world, barrier, dist)
+    e2e = None if args.device_only else e2e_measure(ectx, data, args.workload, max(2, args.steps // 2),
+                                                    max(args.warmup, 2), stream, local, rank, world, barrier, dist)
     spans = W.chunk_spans(data.size, CHUNK)
     inflate = None
     writer = None if args.device_only else writer_rate(ectx, data)
@@ -783,7 +783,6 @@ def main():
         hybrid["no_warmup"] = hybrid_rate(ectx, data, warmup_chunks=0)
     if not args.device_only:
         inflate = inflate_rates(ectx, e2e.pop("_gz"), data.size)
-    e2e.pop("_gz", None)
     # pageable chunks, as a writer hands them over
     chunk_fn = None if args.device_only else chunk_fn_rate(ectx, [np.ascontiguousarray(data[o:o + n]) for o, n in spans])
 
