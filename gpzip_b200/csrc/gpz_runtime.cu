@@ -135,15 +135,18 @@ class CopyPool {
         {
             std::lock_guard<std::mutex> lk(mu_);
             stop_ = true;
+            stop_flag_ = true;
         }
         cv_.notify_all();
         for (auto& t : th_) t.join();
     }
 
     void run(const std::vector<Copy>& copies, bool streaming = false) {
-        constexpr size_t kPiece = 1u << 20;
         size_t total = 0;
         for (auto& c : copies) total += c.n;
+        // 1 MiB pieces; 256 KiB ones for copies under 4 MiB (a writer's
+        // 1 MiB writes), which then take four copiers instead of one
+        const size_t kPiece = total < (4u << 20) ? (256u << 10) : (1u << 20);
         if (total < 2 * kPiece || th_.empty()) {
             for (auto& c : copies) (streaming ? copy_streaming : copy_cached)(c.dst, c.src, c.n);
             return;
@@ -158,7 +161,7 @@ class CopyPool {
         {
             std::lock_guard<std::mutex> lk(mu_);
             job_ = job;
-            gen_++;
+            gen_.fetch_add(1);
         }
         cv_.notify_all();
         drain(*job);
@@ -186,15 +189,23 @@ class CopyPool {
             }
         }
     }
+    // A worker polls for the next job for up to kSpinUs after each one
+    // before it sleeps: back-to-back copies (a writer's) then skip the
+    // wake-up latency of the condition variable.
+    static constexpr int64_t kSpinUs = 200;
     void work() {
         uint64_t seen = 0;
         for (;;) {
+            const auto t0 = std::chrono::steady_clock::now();
+            while (gen_.load() == seen && !stop_flag_.load() &&
+                   std::chrono::steady_clock::now() - t0 < std::chrono::microseconds(kSpinUs))
+                _mm_pause();
             std::shared_ptr<Job> job;
             {
                 std::unique_lock<std::mutex> lk(mu_);
-                cv_.wait(lk, [&] { return stop_ || gen_ != seen; });
+                cv_.wait(lk, [&] { return stop_ || gen_.load() != seen; });
                 if (stop_) return;
-                seen = gen_;
+                seen = gen_.load();
                 job = job_;
             }
             if (job) drain(*job);
@@ -204,7 +215,8 @@ class CopyPool {
     std::mutex mu_;
     std::condition_variable cv_;
     std::shared_ptr<Job> job_;
-    uint64_t gen_ = 0;
+    std::atomic<uint64_t> gen_{0};
+    std::atomic<bool> stop_flag_{false};
     bool stop_ = false;
 };
 
@@ -675,6 +687,11 @@ struct LaunchPolicy {
 };
 constexpr LaunchPolicy kPolicyBatched{false, true, true, false, 100};
 constexpr LaunchPolicy kPolicyPlain{true, false, false, false, 100};
+// The streaming pass loop never stops to tune: its passes change size as
+// chunks arrive, and tuning a new bucket (every shape run twice) held a
+// writer's stream for 60-120 ms.  It uses the tuned shape where a bucket
+// has one and the default shape otherwise.
+constexpr LaunchPolicy kPolicyStream{false, false, true, false, 100};
 
 // True when every non-empty input of the batch starts in page-locked host
 // memory (cudaHostAlloc or cudaHostRegister), so the copy engine can read
@@ -990,7 +1007,7 @@ int gpz_stream_run(gpz_ctx* c, GpzStreamFeed& feed) {
             continue;
         }
         const int k = c->next_slot;  // not pending: fewer than kSyncSlots are, in round-robin order
-        const int rc = submit_slot(c, c->slots[k], items.data(), items.size(), kPolicyBatched, c->kstream);
+        const int rc = submit_slot(c, c->slots[k], items.data(), items.size(), kPolicyStream, c->kstream);
         if (rc) {
             fatal = rc;
             break;
