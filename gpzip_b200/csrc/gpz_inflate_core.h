@@ -67,13 +67,16 @@ struct Table {
     uint16_t sym[320];              // symbols ordered by (length, value)
 };
 
+// The ring comes last: the token form (TOK) never touches it, and its
+// kernel allocates only the bytes before it (kSharedTokBytes).
 struct Shared {
-    uint8_t ring[kRing];
     alignas(4) uint8_t stage[kStage + 16];
     Table lit, dist;
     uint8_t lens[320];
     uint32_t bcast;  // a value lane 0 computed, for every lane
+    uint8_t ring[kRing];
 };
+constexpr size_t kSharedTokBytes = sizeof(Shared) - kRing;
 
 #if defined(GPZI_HOST_LANES)
 // Host test build with NL host threads standing in for the lanes of a warp
@@ -275,33 +278,59 @@ GPZI_FN uint32_t decode_entry(Shared& s, Bits<NL>& b, const Table& t, uint32_t k
 
 
 // Output state: bytes [0, o) of the member are produced, [0, flushed) of
-// them already copied to dst; the ring holds the last kRing bytes.
-template <int NL>
+// them already copied to dst; the ring holds the last kRing bytes.  In the
+// token form (TOK) nothing is copied: every literal and match goes to
+// tok[nt++] instead (a literal as its byte, a match as length << 16 |
+// distance), and expand_tokens or the device's expansion kernel makes the
+// bytes later.
+template <int NL, bool TOK>
 struct Out {
     uint8_t* dst;
     uint32_t cap;  // ISIZE
     uint32_t o;
     uint32_t flushed;
     uint32_t lane;
+    uint32_t* tok;
+    uint32_t nt;
 
     GPZI_FN void flush(Shared& s, uint32_t upto) {
-        lane_sync();
-        for (uint32_t k = flushed + lane; k < upto; k += NL) dst[k] = s.ring[k & (kRing - 1)];
-        flushed = upto;
+        if constexpr (!TOK) {
+            lane_sync();
+            for (uint32_t k = flushed + lane; k < upto; k += NL) dst[k] = s.ring[k & (kRing - 1)];
+            flushed = upto;
+        }
     }
     GPZI_FN void maybe_flush(Shared& s) {
-        if (o - flushed >= kFlush) flush(s, flushed + kFlush);
+        if constexpr (!TOK)
+            if (o - flushed >= kFlush) flush(s, flushed + kFlush);
     }
 };
 
-// Decodes one member's deflate data src[0, len) into dst[0, isize).
-// Returns a status code; on kOk exactly isize bytes were written and the
-// data ended exactly at len.
-template <int NL>
+// The bytes of a token stream (serial; the host check of the token form).
+GPZI_FN void expand_tokens(const uint32_t* tok, uint32_t nt, uint8_t* dst) {
+    uint32_t o = 0;
+    for (uint32_t i = 0; i < nt; i++) {
+        const uint32_t v = tok[i], l = v >> 16;
+        if (!l) {
+            dst[o++] = (uint8_t)v;
+            continue;
+        }
+        const uint32_t d = v & 0xFFFFu;
+        for (uint32_t q = 0; q < l; q++) dst[o + q] = dst[o - d + q];
+        o += l;
+    }
+}
+
+// Decodes one member's deflate data src[0, len) into dst[0, isize), or, in
+// the token form (TOK), into its tokens tok[0, *ntok) (at most isize of
+// them; dst is not written).  Returns a status code; on kOk exactly isize
+// bytes were produced and the data ended exactly at len.  Both forms make
+// the same checks and return the same status.
+template <int NL, bool TOK = false>
 GPZI_FN uint32_t inflate_member(Shared& s, uint32_t lane, const uint8_t* src, uint32_t len, uint8_t* dst,
-                                uint32_t isize) {
+                                uint32_t isize, uint32_t* tok = nullptr, uint32_t* ntok = nullptr) {
     Bits<NL> b{src, len, 0u, 0ull, 0u, lane, 0u};
-    Out<NL> out{dst, isize, 0u, 0u, lane};
+    Out<NL, TOK> out{dst, isize, 0u, 0u, lane, tok, 0u};
     b.restage(s, 0);
     uint32_t err = kOk;
     bool last = false;
@@ -330,10 +359,14 @@ GPZI_FN uint32_t inflate_member(Shared& s, uint32_t lane, const uint8_t* src, ui
             // whole bytes still in the bit buffer come first
             uint32_t k = 0;
             for (; k < ln && b.cnt >= 8; k++) {
-                if (lane == 0) s.ring[(out.o + k) & (kRing - 1)] = (uint8_t)b.peek(8);
+                if (lane == 0) {
+                    if constexpr (TOK) out.tok[out.nt + k] = (uint32_t)b.peek(8);
+                    else s.ring[(out.o + k) & (kRing - 1)] = (uint8_t)b.peek(8);
+                }
                 b.drop(8);
             }
             out.o += k;
+            out.nt += k;
             // then straight from the input, at most kFlush / 2 bytes a round
             // so that the unflushed part always fits the ring; the bit
             // buffer is empty and its look-ahead stale from here
@@ -343,11 +376,14 @@ GPZI_FN uint32_t inflate_member(Shared& s, uint32_t lane, const uint8_t* src, ui
                 lane_sync();
                 for (uint32_t q = lane; q < step; q += NL) {
                     const uint32_t p = b.pos + q;
-                    s.ring[(out.o + q) & (kRing - 1)] = p < len ? src[p] : (uint8_t)0;
+                    const uint8_t v = p < len ? src[p] : (uint8_t)0;
+                    if constexpr (TOK) out.tok[out.nt + q] = v;
+                    else s.ring[(out.o + q) & (kRing - 1)] = v;
                 }
                 b.pos += step;
                 k += step;
                 out.o += step;
+                out.nt += step;
                 out.maybe_flush(s);
             }
             if (b.overrun()) err = kErrInput;
@@ -459,7 +495,12 @@ GPZI_FN uint32_t inflate_member(Shared& s, uint32_t lane, const uint8_t* src, ui
                     err = kErrOutput;
                     break;
                 }
-                s.ring[out.o & (kRing - 1)] = (uint8_t)(e >> 8);  // every lane, the same byte
+                if constexpr (TOK) {
+                    if (lane == 0) out.tok[out.nt] = (e >> 8) & 0xFFu;
+                    out.nt++;
+                } else {
+                    s.ring[out.o & (kRing - 1)] = (uint8_t)(e >> 8);  // every lane, the same byte
+                }
                 out.o++;
                 out.maybe_flush(s);
                 continue;
@@ -491,7 +532,10 @@ GPZI_FN uint32_t inflate_member(Shared& s, uint32_t lane, const uint8_t* src, ui
                 err = kErrOutput;
                 break;
             }
-            if (d >= NL && d <= kRing - NL) {
+            if constexpr (TOK) {
+                if (lane == 0) out.tok[out.nt] = (mlen << 16) | d;
+                out.nt++;
+            } else if (d >= NL && d <= kRing - NL) {
                 // byte o + k = byte o + k - d, which precedes this step of
                 // NL bytes, and no write of a step hits a slot that the same
                 // step reads
@@ -522,6 +566,7 @@ GPZI_FN uint32_t inflate_member(Shared& s, uint32_t lane, const uint8_t* src, ui
         else if ((b.consumed() + 7u) / 8u != len) err = kErrTrailing;
     }
     if (err == kOk) out.flush(s, out.o);
+    if (ntok) *ntok = out.nt;
     lane_sync();
     return err;
 }

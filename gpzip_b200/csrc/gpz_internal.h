@@ -156,11 +156,12 @@ struct InflateMember {
     uint32_t crc;      // CRC-32 of the trailer
     uint32_t pad;
 };
-// k_inflate (one warp per member) then k_inflate_crc (gpz_inflate.cu);
-// status[m] = 0 or the member's gpzi status code.  events: NULL or two
-// cudaEvent_t recorded before and after.
-int gpz_launch_inflate(const uint8_t* in, uint8_t* out, const InflateMember* members, uint32_t* status,
-                       uint32_t count, void* stream, void* const* events);
+// k_inflate_tok (one warp per member: tokens into tok, indexed like out,
+// and their count into ntok), k_inflate_expand (tokens to bytes), then
+// k_inflate_crc (gpz_inflate.cu); status[m] = 0 or the member's gpzi status
+// code.  events: NULL or two cudaEvent_t recorded before and after.
+int gpz_launch_inflate(const uint8_t* in, uint8_t* out, uint32_t* tok, const InflateMember* members,
+                       uint32_t* status, uint32_t* ntok, uint32_t count, void* stream, void* const* events);
 size_t gpz_inflate_smem_bytes();
 // Persistent grid sizes (SMs x resident CTAs) for the shape's thread counts.
 int gpz_occupancy(LaunchShape* persistent);

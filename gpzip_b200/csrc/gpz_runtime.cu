@@ -1914,9 +1914,12 @@ int gpz_inflate(gpz_ctx* c, const uint8_t* in, size_t n, uint8_t* out, size_t ou
     if (ms.empty()) return GPZ_OK;
     Slot& sl = c->inf;
     const size_t nm = ms.size();
+    // tokens: at most one per output byte, 4 bytes each; d_cnt holds the
+    // members' statuses, then their token counts
     if ((rc = ensure_dev(c, sl, sl.d_in, n + 16)) || (rc = ensure_dev(c, sl, sl.d_out, total + 16)) ||
+        (rc = ensure_dev(c, sl, sl.d_tok, (total + 16) * 4)) ||
         (rc = ensure_dev(c, sl, sl.d_members, nm * sizeof(InflateMember))) ||
-        (rc = ensure_dev(c, sl, sl.d_cnt, nm * 4)))
+        (rc = ensure_dev(c, sl, sl.d_cnt, nm * 8)))
         return rc;
     for (auto& e : c->inf_ev)
         if (!e) CU(c, cudaEventCreate(&e));
@@ -1937,7 +1940,8 @@ int gpz_inflate(gpz_ctx* c, const uint8_t* in, size_t n, uint8_t* out, size_t ou
     }
     CU(c, cudaMemcpyAsync(sl.d_members.p, ms.data(), nm * sizeof(InflateMember), cudaMemcpyHostToDevice, s));
     if (gpz_launch_inflate(static_cast<const uint8_t*>(sl.d_in.p), static_cast<uint8_t*>(sl.d_out.p),
-                           static_cast<const InflateMember*>(sl.d_members.p), static_cast<uint32_t*>(sl.d_cnt.p),
+                           static_cast<uint32_t*>(sl.d_tok.p), static_cast<const InflateMember*>(sl.d_members.p),
+                           static_cast<uint32_t*>(sl.d_cnt.p), static_cast<uint32_t*>(sl.d_cnt.p) + nm,
                            (uint32_t)nm, s, reinterpret_cast<void* const*>(c->inf_ev)) != 0)
         return fail(c, GPZ_E_CUDA, "inflate launch", cudaGetLastError());
     const bool out_locked = cudaPointerGetAttributes(&a, out) == cudaSuccess && a.type == cudaMemoryTypeHost;

@@ -36,6 +36,23 @@ int main(int argc, char** argv) {
         for (auto& t : th) t.join();
         for (int l = 1; l < NL; l++)
             if (st[l] != st[0]) return 4;  // lanes disagree
+        // the token form on the same lanes: same status, same bytes
+        std::vector<uint32_t> tok(hdr[1] + 1u);
+        uint32_t nt = 0, st2[NL];
+        std::vector<std::thread> th2;
+        for (int l = 0; l < NL; l++)
+            th2.emplace_back([&, l] {
+                st2[l] = gpzi::inflate_member<NL, true>(g_shared, (uint32_t)l, in.data(), hdr[0], nullptr, hdr[1],
+                                                        tok.data(), l == 0 ? &nt : nullptr);
+            });
+        for (auto& t : th2) t.join();
+        for (int l = 0; l < NL; l++)
+            if (st2[l] != st[0]) return 4;
+        if (st[0] == gpzi::kOk) {
+            std::vector<uint8_t> again(hdr[1]);
+            gpzi::expand_tokens(tok.data(), nt, again.data());
+            if (again != out) return 5;
+        }
         const uint32_t n = st[0] == gpzi::kOk ? hdr[1] : 0u;
         std::fwrite(&st[0], 4, 1, g);
         std::fwrite(&n, 4, 1, g);

@@ -1,7 +1,8 @@
 """GPU decompression of gpzip-written gzip streams (gpz_inflate) through the C
 ABI: the output equals the input that was compressed, for the device
 compressor's own streams, the oracle's, fixed-block members and zlib-built
-members of every block type; damaged streams fail with GPZ_E_DATA."""
+members of every block type, overlapping and chained matches; damaged
+streams fail with GPZ_E_DATA."""
 import struct
 import zlib
 
@@ -49,6 +50,24 @@ def test_fixed_blocks_and_zlib_members(ctx):
     for d in data:
         for level, strat in ((0, 0), (1, 0), (6, zlib.Z_FIXED), (9, zlib.Z_RLE), (6, zlib.Z_HUFFMAN_ONLY)):
             parts.append(member(raw_deflate(d, level, strat), d))
+            want.append(d)
+    assert bytes(ctx.inflate(b"".join(parts))) == b"".join(want)
+
+
+def test_overlapping_and_chained_matches(ctx):
+    # runs whose matches overlap their own output (distance 1 or 3) and
+    # chains of matches that copy from earlier matches: the expansion
+    # kernel resolves them in order
+    rng = np.random.default_rng(13)
+    block = rng.integers(0, 256, 3000, dtype=np.uint8).tobytes()
+    data = [b"\0" * 300_000, b"abc" * 100_001, (b"x" * 5 + b"yz") * 40_000, block * 60,
+            b"".join(block[: int(k)] for k in rng.integers(1, 3000, size=80))]
+    parts, want = [], []
+    for d in data:
+        parts.append(bytes(ctx.compress_chunk(d)))
+        want.append(d)
+        for level in (1, 9):
+            parts.append(member(raw_deflate(d, level), d))
             want.append(d)
     assert bytes(ctx.inflate(b"".join(parts))) == b"".join(want)
 
