@@ -321,6 +321,96 @@ GPZI_FN void expand_tokens(const uint32_t* tok, uint32_t nt, uint8_t* dst) {
     }
 }
 
+// The code tables of one block into s.lit and s.dist: the fixed codes for
+// type 1 (RFC 1951 3.2.6), the codes of the header read from b for type 2
+// (3.2.7).  Returns a status; lit_empty / dist_empty tell whether a table
+// has no code at all (an error only once it is used).
+template <int NL>
+GPZI_FN uint32_t read_block_tables(Shared& s, Bits<NL>& b, uint32_t lane, uint32_t type, bool& lit_empty,
+                                   bool& dist_empty) {
+    uint32_t err = kOk;
+    if (type == 1) {
+        lane_sync();
+        if (lane == 0) {
+            for (int i = 0; i < 144; i++) s.lens[i] = 8;
+            for (int i = 144; i < 256; i++) s.lens[i] = 9;
+            for (int i = 256; i < 280; i++) s.lens[i] = 7;
+            for (int i = 280; i < 288; i++) s.lens[i] = 8;
+            for (int i = 288; i < 320; i++) s.lens[i] = 5;
+        }
+        lane_sync();
+        build_table<NL>(s, s.lit, kTabLit, s.lens, 288, lane, lit_empty);
+        build_table<NL>(s, s.dist, kTabDist, s.lens + 288, 32, lane, dist_empty);
+    } else {
+        const uint32_t hlit = b.take(s, 5) + 257, hdist = b.take(s, 5) + 1, hclen = b.take(s, 4) + 4;
+        lane_sync();
+        if (lane == 0)
+            for (int i = 0; i < 19; i++) s.lens[i] = 0;
+        for (uint32_t i = 0; i < hclen; i++) {
+            const uint32_t v = b.take(s, 3);
+            if (lane == 0) s.lens[meta_order(i)] = (uint8_t)v;
+        }
+        lane_sync();
+        if (hlit > 286 || hdist > 30) {
+            return kErrCodeLens;
+        }
+        bool cl_empty = false;
+        if (build_table<NL>(s, s.lit, kTabMeta, s.lens, 19, lane, cl_empty) != kOk || cl_empty) {
+            return kErrCodeLens;
+        }
+        // the litlen and distance code lengths as one sequence (3.2.7)
+        uint32_t i = 0, prev = 0;
+        const uint32_t nl = hlit + hdist;
+        while (i < nl) {
+            const uint32_t sym = (decode_entry<NL>(s, b, s.lit, kTabMeta, err) >> 8) & 255u;
+            if (err) return err;
+            uint32_t rep = 1, val = sym;
+            if (sym == 16) {
+                if (i == 0) {
+                    return kErrCodeLens;
+                }
+                val = prev;
+                rep = 3 + b.take(s, 2);
+            } else if (sym == 17) {
+                val = 0;
+                rep = 3 + b.take(s, 3);
+            } else if (sym == 18) {
+                val = 0;
+                rep = 11 + b.take(s, 7);
+            }
+            if (i + rep > nl) {
+                return kErrCodeLens;
+            }
+            lane_sync();
+            if (lane == 0)
+                for (uint32_t r = 0; r < rep; r++) s.lens[i + r] = (uint8_t)val;
+            lane_sync();
+            prev = val;
+            i += rep;
+        }
+        if (err) return err;
+        if (b.far_past_end()) {
+            return kErrInput;
+        }
+        if (s.lens[256] == 0) {  // no end-of-block code
+            return kErrCodeLens;
+        }
+        // distance lengths moved to s.lens[288, 318) (from the top down:
+        // the ranges may overlap and the target lies above), litlen
+        // lengths stay in s.lens[0, hlit)
+        if (lane == 0) {
+            for (uint32_t q = 30; q-- > 0;) s.lens[288 + q] = q < hdist ? s.lens[hlit + q] : (uint8_t)0;
+            s.lens[318] = s.lens[319] = 0;
+        }
+        lane_sync();
+        if (build_table<NL>(s, s.lit, kTabLit, s.lens, hlit, lane, lit_empty) != kOk ||
+            build_table<NL>(s, s.dist, kTabDist, s.lens + 288, 30, lane, dist_empty) != kOk) {
+            return kErrCodeSet;
+        }
+    }
+    return kOk;
+}
+
 // Decodes one member's deflate data src[0, len) into dst[0, isize), or, in
 // the token form (TOK), into its tokens tok[0, *ntok) (at most isize of
 // them; dst is not written).  Returns a status code; on kOk exactly isize
@@ -395,92 +485,8 @@ GPZI_FN uint32_t inflate_member(Shared& s, uint32_t lane, const uint8_t* src, ui
             break;
         }
         bool lit_empty = false, dist_empty = false;
-        if (type == 1) {
-            lane_sync();
-            if (lane == 0) {
-                for (int i = 0; i < 144; i++) s.lens[i] = 8;
-                for (int i = 144; i < 256; i++) s.lens[i] = 9;
-                for (int i = 256; i < 280; i++) s.lens[i] = 7;
-                for (int i = 280; i < 288; i++) s.lens[i] = 8;
-                for (int i = 288; i < 320; i++) s.lens[i] = 5;
-            }
-            lane_sync();
-            build_table<NL>(s, s.lit, kTabLit, s.lens, 288, lane, lit_empty);
-            build_table<NL>(s, s.dist, kTabDist, s.lens + 288, 32, lane, dist_empty);
-        } else {
-            const uint32_t hlit = b.take(s, 5) + 257, hdist = b.take(s, 5) + 1, hclen = b.take(s, 4) + 4;
-            lane_sync();
-            if (lane == 0)
-                for (int i = 0; i < 19; i++) s.lens[i] = 0;
-            for (uint32_t i = 0; i < hclen; i++) {
-                const uint32_t v = b.take(s, 3);
-                if (lane == 0) s.lens[meta_order(i)] = (uint8_t)v;
-            }
-            lane_sync();
-            if (hlit > 286 || hdist > 30) {
-                err = kErrCodeLens;
-                break;
-            }
-            bool cl_empty = false;
-            if (build_table<NL>(s, s.lit, kTabMeta, s.lens, 19, lane, cl_empty) != kOk || cl_empty) {
-                err = kErrCodeLens;
-                break;
-            }
-            // the litlen and distance code lengths as one sequence (3.2.7)
-            uint32_t i = 0, prev = 0;
-            const uint32_t nl = hlit + hdist;
-            while (i < nl) {
-                const uint32_t sym = (decode_entry<NL>(s, b, s.lit, kTabMeta, err) >> 8) & 255u;
-                if (err) break;
-                uint32_t rep = 1, val = sym;
-                if (sym == 16) {
-                    if (i == 0) {
-                        err = kErrCodeLens;
-                        break;
-                    }
-                    val = prev;
-                    rep = 3 + b.take(s, 2);
-                } else if (sym == 17) {
-                    val = 0;
-                    rep = 3 + b.take(s, 3);
-                } else if (sym == 18) {
-                    val = 0;
-                    rep = 11 + b.take(s, 7);
-                }
-                if (i + rep > nl) {
-                    err = kErrCodeLens;
-                    break;
-                }
-                lane_sync();
-                if (lane == 0)
-                    for (uint32_t r = 0; r < rep; r++) s.lens[i + r] = (uint8_t)val;
-                lane_sync();
-                prev = val;
-                i += rep;
-            }
-            if (err) break;
-            if (b.far_past_end()) {
-                err = kErrInput;
-                break;
-            }
-            if (s.lens[256] == 0) {  // no end-of-block code
-                err = kErrCodeLens;
-                break;
-            }
-            // distance lengths moved to s.lens[288, 318) (from the top down:
-            // the ranges may overlap and the target lies above), litlen
-            // lengths stay in s.lens[0, hlit)
-            if (lane == 0) {
-                for (uint32_t q = 30; q-- > 0;) s.lens[288 + q] = q < hdist ? s.lens[hlit + q] : (uint8_t)0;
-                s.lens[318] = s.lens[319] = 0;
-            }
-            lane_sync();
-            if (build_table<NL>(s, s.lit, kTabLit, s.lens, hlit, lane, lit_empty) != kOk ||
-                build_table<NL>(s, s.dist, kTabDist, s.lens + 288, 30, lane, dist_empty) != kOk) {
-                err = kErrCodeSet;
-                break;
-            }
-        }
+        err = read_block_tables<NL>(s, b, lane, type, lit_empty, dist_empty);
+        if (err) break;
         // symbols up to the end of the block
         for (;;) {
             if (b.far_past_end()) {
@@ -570,5 +576,323 @@ GPZI_FN uint32_t inflate_member(Shared& s, uint32_t lane, const uint8_t* src, ui
     lane_sync();
     return err;
 }
+
+
+// ---- Parallel decode of a member that is one dynamic block ----
+//
+// gpzip writes every member as one dynamic-Huffman block, and a member's
+// serial decode (one symbol after another, each needing the last one's
+// length) is the whole cost of k_inflate_tok.  The block's symbol bits,
+// from the end of its header to the end of the data, are therefore cut into
+// R spans of equal bit length, one per lane, and every lane decodes its span
+// on its own.  A lane that starts in the middle of a code decodes garbage at
+// first, but Huffman codes resynchronise within a few symbols, so its exit
+// -- the first symbol start at or after the next span's first bit -- is
+// almost always the true one.  Rounds repeat with each lane starting at its
+// left neighbour's exit from the round before, until no start changes.
+// Then every start is a true symbol boundary (lane 0's is, and a lane's
+// exit from a true start is true), and the last round's token and byte
+// counts are exact.  A final pass writes the tokens at offsets from a scan
+// of those counts and checks every distance against the output position.
+// Whatever the serial decoder would reject, and a member that does not
+// settle within kParRounds, is left to the serial decoder, so failing
+// members get exactly its status codes.
+
+constexpr uint64_t kSpanEnd = ~0ull;      // the end-of-block code came first
+constexpr uint64_t kSpanBad = ~0ull - 1;  // an invalid code, distance or length
+constexpr uint32_t kParRounds = 4;        // rounds before the unsettled rest is decoded by one lane
+constexpr uint64_t kParMinSpanBits = 256; // shortest span worth a lane of its own
+// The rest of a block that has not settled (the tail) is cut into sub-spans
+// of kSubBits, and each sub-span is decoded from each of the kCands bit
+// offsets after its first bit.  Walking the sub-spans in order then picks,
+// for each, the candidate that starts where the one before it ended.  A
+// symbol takes at most kMaxSymBits = 15 + 5 + 15 + 13 bits, so the true
+// start lies less than that after the first bit; on gpzip's members it lay
+// within 24 bits at 99.8 % of the boundaries, and the walk decodes a
+// sub-span itself where it lies further.
+constexpr uint64_t kSubBits = 4096;
+constexpr uint32_t kCands = 32;
+constexpr uint32_t kMaxSymBits = 48;
+
+
+// Per-lane bit reader straight from the member's bytes (zeros past len).
+struct LaneBits {
+    const uint8_t* src;
+    uint32_t len;
+    uint32_t pos;  // next byte not yet in buf
+    uint32_t cnt;  // valid bits in buf
+    uint64_t buf;
+
+    // afterwards at least 56 bits are valid.  Away from the end, eight
+    // bytes come from three aligned words loaded at once; in the last 12
+    // bytes they are read one by one.
+    GPZI_FN void refill() {
+        if (pos + 12u <= len) {
+            const uintptr_t at = (uintptr_t)(src + pos);
+            const uint32_t* w = reinterpret_cast<const uint32_t*>(at & ~(uintptr_t)3);
+            const uint32_t sh = (uint32_t)(at & 3u) * 8u;
+            uint64_t v = ((uint64_t)w[1] << 32 | w[0]) >> sh;
+            if (sh) v |= (uint64_t)w[2] << (64u - sh);
+            buf |= v << cnt;
+            const uint32_t nb = (63u - cnt) >> 3;
+            pos += nb;
+            cnt += nb * 8u;
+            return;
+        }
+        while (cnt <= 56u) {
+            buf |= (uint64_t)(pos < len ? src[pos] : 0u) << cnt;
+            pos++;
+            cnt += 8u;
+        }
+    }
+    GPZI_FN void seek(uint64_t bit) {
+        pos = (uint32_t)(bit >> 3);
+        buf = 0;
+        cnt = 0;
+        refill();
+        drop((uint32_t)(bit & 7u));
+    }
+    GPZI_FN uint32_t peek(uint32_t n) const { return (uint32_t)(buf & ((1ull << n) - 1ull)); }
+    GPZI_FN void drop(uint32_t n) {
+        buf >>= n;
+        cnt -= n;
+    }
+    GPZI_FN uint32_t take(uint32_t n) {  // n <= 32
+        if (cnt < n) refill();
+        const uint32_t v = peek(n);
+        drop(n);
+        return v;
+    }
+    GPZI_FN uint64_t bitpos() const { return 8ull * pos - cnt; }
+};
+
+// One code's entry from t (see Table), as decode_entry; bad if no symbol
+// has the code.
+GPZI_FN uint32_t lane_entry(const Table& t, LaneBits& b, uint32_t kind, bool& bad) {
+    if (b.cnt < 15) b.refill();
+    const uint32_t e = t.fast[b.peek(kFastBits)];
+    if (e) {
+        b.drop(e & 15u);
+        return e;
+    }
+    uint32_t code = 0, first = 0, index = 0;
+    for (uint32_t l = 1; l < 16; l++) {
+        code |= (uint32_t)(b.buf >> (l - 1)) & 1u;
+        const uint32_t c = t.count[l];
+        if (code - first < c) {
+            b.drop(l);
+            return pack_entry(kind, t.sym[index + code - first], 0u);
+        }
+        index += c;
+        first += c;
+        first <<= 1;
+        code <<= 1;
+    }
+    bad = true;
+    return 0;
+}
+
+// What a lane found in its span: its exit (the first symbol start at or
+// after the span's stop bit, or kSpanEnd / kSpanBad), the bit after the
+// end-of-block code (with kSpanEnd), and the tokens and bytes of the
+// symbols that start in the span.
+struct Span {
+    uint64_t exit;
+    uint64_t end;
+    uint32_t ntok;
+    uint32_t nbytes;
+};
+
+// A candidate's result packed into 64 bits: the exit as an offset from the
+// next sub-span's first bit (< kMaxSymBits; kCandEnd: the end-of-block code
+// came first, kCandBad: anything else), the end-of-block code's end bit as an
+// offset from the sub-span's first bit, and its tokens and bytes.
+constexpr uint32_t kCandEnd = 254u, kCandBad = 255u;
+GPZI_FN uint64_t pack_cand(const Span& r, uint64_t first, uint64_t next_first) {
+    uint64_t code = kCandBad, endoff = 0;
+    if (r.exit == kSpanEnd) {
+        code = kCandEnd;
+        endoff = r.end - first;
+    } else if (r.exit != kSpanBad && r.exit >= next_first && r.exit - next_first < kMaxSymBits) {
+        code = r.exit - next_first;
+    }
+    if (endoff >= (1u << 13) || r.ntok >= (1u << 13) || r.nbytes >= (1u << 21)) code = kCandBad;
+    return code | endoff << 8 | (uint64_t)r.ntok << 21 | (uint64_t)r.nbytes << 34;
+}
+
+// Decodes the symbols of the block (tables lit, dist) that start at bit
+// `start` and below `stop`.  A start of kSpanEnd or kSpanBad is passed
+// on as the exit.  Spans never count more than isize bytes.  With tok (the
+// final pass) the tokens are written to tok[0, ntok) (a literal as its
+// byte, a match as length << 16 | distance), and every match is checked to
+// reach no further back than the member's start and no further than ISIZE:
+// obase is the number of bytes before the span.
+GPZI_FN Span decode_span(const Table& lit, const Table& dist, const uint8_t* src, uint32_t len, uint64_t start,
+                         uint64_t stop, uint32_t* tok, uint32_t obase, uint32_t isize) {
+    Span r{kSpanBad, 0ull, 0u, 0u};
+    if (start == kSpanEnd || start == kSpanBad) {
+        r.exit = start;
+        return r;
+    }
+    LaneBits b{src, len, 0u, 0u, 0ull};
+    b.seek(start);
+    const uint64_t data_bits = 8ull * len;
+    uint64_t p = start;
+    // every symbol takes at least one bit, so the loop ends within
+    // data_bits + 1 rounds
+    while (p < stop) {
+        if (p >= data_bits) return r;  // the data ended without an end-of-block code
+        bool bad = false;
+        const uint32_t e = lane_entry(lit, b, kTabLit, bad);
+        if (bad) return r;
+        const uint32_t kind = (e >> 4) & 3u;
+        if (kind == 0u) {
+            if (r.nbytes >= isize || (tok && (uint64_t)obase + r.nbytes >= isize)) return r;
+            if (tok) tok[r.ntok] = (e >> 8) & 0xFFu;
+            r.ntok++;
+            r.nbytes++;
+        } else if (kind == 2u) {
+            r.exit = kSpanEnd;
+            r.end = b.bitpos();
+            return r;
+        } else if (kind == 3u) {
+            return r;
+        } else {
+            const uint32_t lx = (e >> 17) & 7u;
+            const uint32_t mlen = ((e >> 8) & 511u) + (lx ? b.take(lx) : 0u);
+            const uint32_t de = lane_entry(dist, b, kTabDist, bad);
+            if (bad || ((de >> 4) & 3u) == 3u) return r;
+            const uint32_t dx = (de >> 24) & 15u;
+            const uint32_t d = ((de >> 8) & 0x7FFFu) + (dx ? b.take(dx) : 0u);
+            if (r.nbytes > isize || isize - r.nbytes < mlen) return r;
+            if (tok) {
+                const uint64_t o = (uint64_t)obase + r.nbytes;  // output bytes before this match
+                if (d > o || o > isize || isize - o < mlen) return r;
+                tok[r.ntok] = (mlen << 16) | d;
+            }
+            r.ntok++;
+            r.nbytes += mlen;
+        }
+        p = b.bitpos();
+    }
+    r.exit = p;
+    return r;
+}
+
+// The block's first symbol bit when the member is one final dynamic block
+// whose header and tables are valid (tables built in s.lit, s.dist), else
+// 0: the serial decoder takes the member.
+template <int NL>
+GPZI_FN uint64_t par_header(Shared& s, uint32_t lane, const uint8_t* src, uint32_t len) {
+    Bits<NL> b{src, len, 0u, 0ull, 0u, lane, 0u};
+    b.restage(s, 0);
+    const bool last = b.take(s, 1) != 0;
+    const uint32_t type = b.take(s, 2);
+    if (!last || type != 2u) return 0;
+    bool lit_empty = false, dist_empty = false;
+    if (read_block_tables<NL>(s, b, lane, type, lit_empty, dist_empty) != kOk || lit_empty || b.overrun()) return 0;
+    return b.consumed();
+}
+
+// Lanes used for a block whose symbols take `bits` bits: spans of at least
+// kParMinSpanBits, at most max_lanes of them.
+GPZI_FN uint32_t par_lanes(uint64_t bits, uint32_t max_lanes) {
+    const uint64_t r = bits / kParMinSpanBits;
+    return r < 1u ? 1u : r > max_lanes ? max_lanes : (uint32_t)r;
+}
+
+#if !defined(__CUDACC__)
+#include <vector>
+
+// The parallel decode with its lanes run one after another (the host check
+// of the device's path in gpz_inflate.cu, which runs the same steps with
+// one thread per lane): true when it takes the member, with the tokens in
+// tok[0, *ntok); false when the member is left to the serial decoder.
+inline bool inflate_member_par(Shared& s, const uint8_t* src, uint32_t len, uint32_t isize, uint32_t max_lanes,
+                               uint32_t* tok, uint32_t* ntok) {
+    constexpr uint32_t kMax = 128;
+    if (max_lanes < 1u || max_lanes > kMax) return false;
+    const uint64_t h = par_header<1>(s, 0, src, len);
+    if (!h || h >= 8ull * len) return false;
+    const uint64_t bits = 8ull * len - h;
+    const uint32_t R = par_lanes(bits, max_lanes);
+    const uint64_t span = (bits + R - 1) / R;
+    uint64_t start[kMax], stop[kMax], next[kMax];
+    Span res[kMax];
+    for (uint32_t k = 0; k < R; k++) {
+        start[k] = h + k * span;
+        stop[k] = k + 1 < R ? h + (k + 1) * span : kSpanBad - 1;
+    }
+    for (uint32_t round = 0; round < kParRounds; round++) {
+        for (uint32_t k = 0; k < R; k++) res[k] = decode_span(s.lit, s.dist, src, len, start[k], stop[k], nullptr, 0u, isize);
+        bool settled = true;
+        for (uint32_t k = 0; k < R; k++) {
+            next[k] = k ? res[k - 1].exit : start[k];
+            settled = settled && next[k] == start[k];
+        }
+        if (settled || round + 1 == kParRounds) break;
+        for (uint32_t k = 0; k < R; k++) start[k] = next[k];
+    }
+    // lanes before the first one whose start moved decoded from true starts;
+    // one lane decodes the rest from that lane's next (true) start
+    uint32_t f = R;
+    for (uint32_t k = 0; k < R && f == R; k++)
+        if (next[k] != start[k]) f = k;
+    uint64_t end = 0, bytes = 0, toks = 0;
+    bool ended = false, fits = true;
+    for (uint32_t k = 0; k < f && fits; k++) {
+        const Span g = decode_span(s.lit, s.dist, src, len, start[k], stop[k], tok + toks, (uint32_t)bytes, isize);
+        fits = g.exit == res[k].exit && g.ntok == res[k].ntok && g.nbytes == res[k].nbytes && bytes <= isize;
+        if (start[k] != kSpanEnd && g.exit == kSpanEnd) {
+            end = g.end;
+            ended = true;
+        }
+        toks += g.ntok;
+        bytes += g.nbytes;
+    }
+    if (fits && f < R && !ended && bytes <= isize && next[f] != kSpanEnd) {
+        // the tail from next[f] (a true start): every sub-span from each of
+        // its kCands first bits, then the walk that picks one per sub-span
+        const uint64_t t0 = next[f];
+        const uint64_t tail = t0 < 8ull * len ? 8ull * len - t0 : 0ull;
+        const uint32_t Q = (uint32_t)((tail + kSubBits - 1) / kSubBits);
+        std::vector<uint64_t> cand((size_t)Q * kCands);
+        for (uint32_t q = 0; q < Q; q++) {
+            const uint64_t first = t0 + q * kSubBits, nf = first + kSubBits;
+            for (uint32_t j = 0; j < kCands; j++)
+                cand[(size_t)q * kCands + j] = pack_cand(
+                    decode_span(s.lit, s.dist, src, len, first + j, q + 1 < Q ? nf : kSpanBad - 1, nullptr, 0u, isize),
+                    first, nf);
+        }
+        uint64_t e = t0;
+        fits = t0 != kSpanBad;
+        for (uint32_t q = 0; q < Q && fits && !ended; q++) {
+            const uint64_t first = t0 + q * kSubBits, nf = first + kSubBits, stop = q + 1 < Q ? nf : kSpanBad - 1;
+            const uint64_t c = e - first < kCands ? cand[(size_t)q * kCands + (e - first)]
+                                                  : pack_cand(decode_span(s.lit, s.dist, src, len, e, stop, nullptr,
+                                                                          0u, isize),
+                                                              first, nf);
+            const uint32_t code = (uint32_t)(c & 255u);
+            if (code == kCandBad || bytes > isize) {
+                fits = false;
+                break;
+            }
+            const Span g = decode_span(s.lit, s.dist, src, len, e, stop, tok + toks, (uint32_t)bytes, isize);
+            fits = pack_cand(g, first, nf) == c;
+            toks += g.ntok;
+            bytes += g.nbytes;
+            if (code == kCandEnd) {
+                end = first + ((c >> 8) & 8191u);
+                ended = true;
+            } else {
+                e = nf + code;
+            }
+        }
+    }
+    if (!fits || !ended || end > 8ull * len || (end + 7) / 8 != len || bytes != isize) return false;
+    *ntok = (uint32_t)toks;
+    return true;
+}
+#endif
 
 }  // namespace gpzi

@@ -156,12 +156,33 @@ struct InflateMember {
     uint32_t crc;      // CRC-32 of the trailer
     uint32_t pad;
 };
-// k_inflate_tok (one warp per member: tokens into tok, indexed like out,
-// and their count into ntok), k_inflate_expand (tokens to bytes), then
-// k_inflate_crc (gpz_inflate.cu); status[m] = 0 or the member's gpzi status
-// code.  events: NULL or two cudaEvent_t recorded before and after.
+// Device scratch of the parallel decode's tails (gpz_inflate.cu): one
+// record of gpz_inflate_tail_bytes() per member, gpz_inflate_cands() packed
+// candidate results per sub-span, three u32 per sub-span (sub_start: the
+// owning tail, until k_inflate_chain puts the chosen start offset there;
+// the token and byte offsets), two counters (tails, sub-spans taken).
+// sub_cap = deflate bytes / 512 + members + 1 sub-spans always suffice.
+struct InflateScratch {
+    void* tails;
+    uint64_t* cands;
+    uint32_t* sub_start;
+    uint32_t* sub_tok;
+    uint32_t* sub_byte;
+    uint32_t* counters;
+    uint32_t sub_cap;
+};
+// k_inflate_par (the parallel decode of single-block members; done[m] = 1
+// for the members it decoded, 2 for those whose tail it left to
+// k_inflate_cand and k_inflate_chain), k_inflate_tok (one warp per
+// remaining member: tokens into tok, indexed like out, and their count into
+// ntok), k_inflate_expand (tokens to bytes), then k_inflate_crc
+// (gpz_inflate.cu); status[m] = 0 or the member's gpzi status code.
+// events: NULL or two cudaEvent_t recorded before and after.
 int gpz_launch_inflate(const uint8_t* in, uint8_t* out, uint32_t* tok, const InflateMember* members,
-                       uint32_t* status, uint32_t* ntok, uint32_t count, void* stream, void* const* events);
+                       uint32_t* status, uint32_t* ntok, uint32_t* done, const InflateScratch& sc, uint32_t count,
+                       void* stream, void* const* events);
+size_t gpz_inflate_tail_bytes();
+uint32_t gpz_inflate_cands();
 size_t gpz_inflate_smem_bytes();
 // Persistent grid sizes (SMs x resident CTAs) for the shape's thread counts.
 int gpz_occupancy(LaunchShape* persistent);

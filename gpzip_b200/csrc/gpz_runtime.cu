@@ -235,6 +235,7 @@ struct Span {
 struct Slot {
     DevArena d_in, d_pp, d_tok, d_out, d_skeys, d_son, d_snkeys, d_tentry, d_texit, d_thist, d_tntok,
         d_tbit, d_mcodes, d_mhdr, d_mout, d_cnt, d_members, d_tiles, d_dims;
+    DevArena d_itail, d_icand, d_isub;  // inflate: the parallel decode's tail scratch
     uint8_t* h_in = nullptr;
     size_t h_in_cap = 0;
     uint8_t* h_desc = nullptr;
@@ -1053,7 +1054,8 @@ void free_slot(gpz_ctx* c, Slot& sl) {
         if (g.exec) cudaGraphExecDestroy(g.exec);
     for (DevArena* a : {&sl.d_in, &sl.d_pp, &sl.d_tok, &sl.d_out, &sl.d_skeys, &sl.d_son, &sl.d_snkeys,
                         &sl.d_tentry, &sl.d_texit, &sl.d_thist, &sl.d_tntok, &sl.d_tbit, &sl.d_mcodes, &sl.d_mhdr,
-                        &sl.d_mout, &sl.d_cnt, &sl.d_members, &sl.d_tiles, &sl.d_dims})
+                        &sl.d_mout, &sl.d_cnt, &sl.d_members, &sl.d_tiles, &sl.d_dims, &sl.d_itail, &sl.d_icand,
+                        &sl.d_isub})
         if (a->p) {
             cudaFree(a->p);
             c->pool_used -= a->cap;
@@ -1915,12 +1917,28 @@ int gpz_inflate(gpz_ctx* c, const uint8_t* in, size_t n, uint8_t* out, size_t ou
     Slot& sl = c->inf;
     const size_t nm = ms.size();
     // tokens: at most one per output byte, 4 bytes each; d_cnt holds the
-    // members' statuses, then their token counts
+    // members' statuses, their token counts and which members the parallel
+    // decode took
     if ((rc = ensure_dev(c, sl, sl.d_in, n + 16)) || (rc = ensure_dev(c, sl, sl.d_out, total + 16)) ||
         (rc = ensure_dev(c, sl, sl.d_tok, (total + 16) * 4)) ||
         (rc = ensure_dev(c, sl, sl.d_members, nm * sizeof(InflateMember))) ||
-        (rc = ensure_dev(c, sl, sl.d_cnt, nm * 8)))
+        (rc = ensure_dev(c, sl, sl.d_cnt, nm * 12)))
         return rc;
+    // a tail of b deflate bytes has at most b / 512 + 1 sub-spans of 4096 bits
+    const size_t sub_cap = n / 512 + nm + 1;
+    if (sub_cap > 0xFFFFFFFFull / gpz_inflate_cands()) return fail(c, GPZ_E_ARG, "stream too large");
+    if ((rc = ensure_dev(c, sl, sl.d_itail, nm * gpz_inflate_tail_bytes())) ||
+        (rc = ensure_dev(c, sl, sl.d_icand, sub_cap * gpz_inflate_cands() * 8)) ||
+        (rc = ensure_dev(c, sl, sl.d_isub, sub_cap * 12 + 16)))
+        return rc;
+    InflateScratch sc{};
+    sc.tails = sl.d_itail.p;
+    sc.cands = static_cast<uint64_t*>(sl.d_icand.p);
+    sc.sub_start = static_cast<uint32_t*>(sl.d_isub.p);
+    sc.sub_tok = sc.sub_start + sub_cap;
+    sc.sub_byte = sc.sub_tok + sub_cap;
+    sc.counters = sc.sub_byte + sub_cap;
+    sc.sub_cap = (uint32_t)sub_cap;
     for (auto& e : c->inf_ev)
         if (!e) CU(c, cudaEventCreate(&e));
     if (!sl.done) CU(c, cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
@@ -1942,7 +1960,8 @@ int gpz_inflate(gpz_ctx* c, const uint8_t* in, size_t n, uint8_t* out, size_t ou
     if (gpz_launch_inflate(static_cast<const uint8_t*>(sl.d_in.p), static_cast<uint8_t*>(sl.d_out.p),
                            static_cast<uint32_t*>(sl.d_tok.p), static_cast<const InflateMember*>(sl.d_members.p),
                            static_cast<uint32_t*>(sl.d_cnt.p), static_cast<uint32_t*>(sl.d_cnt.p) + nm,
-                           (uint32_t)nm, s, reinterpret_cast<void* const*>(c->inf_ev)) != 0)
+                           static_cast<uint32_t*>(sl.d_cnt.p) + 2 * nm, sc, (uint32_t)nm, s,
+                           reinterpret_cast<void* const*>(c->inf_ev)) != 0)
         return fail(c, GPZ_E_CUDA, "inflate launch", cudaGetLastError());
     const bool out_locked = cudaPointerGetAttributes(&a, out) == cudaSuccess && a.type == cudaMemoryTypeHost;
     cudaGetLastError();

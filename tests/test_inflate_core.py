@@ -34,6 +34,9 @@ def decoder(tmp_path_factory):
     return exe
 
 
+PARALLEL = {}  # the last run's "parallel: <taken> of <records>" from inflate_host
+
+
 def run(decoder, tmp_path, cases):
     """cases: list of (deflate bytes, isize) -> list of (status, output)."""
     fin, fout = tmp_path / "in.bin", tmp_path / "out.bin"
@@ -43,6 +46,11 @@ def run(decoder, tmp_path, cases):
             f.write(data)
     r = subprocess.run([decoder, str(fin), str(fout)], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-3000:]
+    PARALLEL.clear()
+    for line in r.stderr.splitlines():
+        if line.startswith("parallel: "):
+            taken, _, records = line[len("parallel: "):].partition(" of ")
+            PARALLEL.update(taken=int(taken), records=int(records))
     res = []
     with open(fout, "rb") as f:
         for _ in cases:
@@ -102,6 +110,24 @@ def test_gpzip_members(decoder, tmp_path):
     got = run(decoder, tmp_path, cases)
     for (st, out), w in zip(got, want):
         assert st == 0 and out == w
+    # every gpzip member is one dynamic block: the parallel decode (128
+    # lanes, checked against the serial tokens by the harness) takes them all
+    assert PARALLEL == {"taken": len(cases), "records": len(cases)}
+
+
+def test_parallel_decode_of_zlib_members(decoder, tmp_path):
+    # single-block zlib members (one final dynamic block below ~16 KiB of
+    # output at level 6 on text) go the parallel way; the multi-block ones
+    # are left to the serial decoder; the harness exits 6 if the parallel
+    # tokens differ from the serial ones or a rejected member is taken
+    cases = []
+    for n in (1, 100, 3000, 20_000, 60_000, 200_000):
+        for kind in ("text", "logs", "binary"):
+            data = W.GENERATORS[kind](n, seed=n % 97).tobytes()
+            for level in (1, 6, 9):
+                cases.append((raw_deflate(data, level), len(data)))
+    run(decoder, tmp_path, cases)
+    assert 0 < PARALLEL["taken"] < PARALLEL["records"]
 
 
 def test_fixed_block_members(decoder, tmp_path):
