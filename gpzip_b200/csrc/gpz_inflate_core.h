@@ -600,7 +600,7 @@ GPZI_FN uint32_t inflate_member(Shared& s, uint32_t lane, const uint8_t* src, ui
 
 constexpr uint64_t kSpanEnd = ~0ull;      // the end-of-block code came first
 constexpr uint64_t kSpanBad = ~0ull - 1;  // an invalid code, distance or length
-constexpr uint32_t kParRounds = 4;        // rounds before the unsettled rest is decoded by one lane
+constexpr uint32_t kParRounds = 2;        // rounds before the unsettled rest becomes a tail
 constexpr uint64_t kParMinSpanBits = 256; // shortest span worth a lane of its own
 // The rest of a block that has not settled (the tail) is cut into sub-spans
 // of kSubBits, and each sub-span is decoded from each of the kCands bit
