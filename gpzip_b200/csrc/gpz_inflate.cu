@@ -384,9 +384,13 @@ __global__ void __launch_bounds__(32) k_inflate_tok(const uint8_t* in, uint32_t*
 
 constexpr int kExpandThreads = 256;
 
+// With host_out (a page-locked host buffer, as the device sees it), each
+// member's bytes are copied there as soon as they are all written, so the
+// copy over PCIe overlaps the members still being expanded.
 __global__ void __launch_bounds__(kExpandThreads) k_inflate_expand(const uint32_t* toks, const uint32_t* ntok,
                                                                    uint8_t* out, const InflateMember* members,
-                                                                   const uint32_t* status, uint32_t count) {
+                                                                   const uint32_t* status, uint8_t* host_out,
+                                                                   uint32_t count) {
     __shared__ uint32_t s_sum[kExpandThreads / 32];
     __shared__ uint32_t s_first;
     const uint32_t m = blockIdx.x, t = threadIdx.x, lane = t & 31u, warp = t >> 5;
@@ -444,6 +448,23 @@ __global__ void __launch_bounds__(kExpandThreads) k_inflate_expand(const uint32_
         }
         base += total;
     }
+    if (host_out) {
+        __syncthreads();  // every byte of the member is written
+        uint8_t* hd = host_out + im.out_off;
+        const uint32_t n = im.isize;
+        // 16-byte stores where both sides share an alignment, bytes elsewhere
+        const uint32_t head = (uint32_t)((16u - ((uintptr_t)dst & 15u)) & 15u);
+        if ((((uintptr_t)dst ^ (uintptr_t)hd) & 15u) == 0u && n >= head + 16u) {
+            for (uint32_t i = t; i < head; i += kExpandThreads) hd[i] = dst[i];
+            const uint32_t nv = (n - head) >> 4;
+            const uint4* s4 = reinterpret_cast<const uint4*>(dst + head);
+            uint4* d4 = reinterpret_cast<uint4*>(hd + head);
+            for (uint32_t i = t; i < nv; i += kExpandThreads) d4[i] = s4[i];
+            for (uint32_t i = head + (nv << 4) + t; i < n; i += kExpandThreads) hd[i] = dst[i];
+        } else {
+            for (uint32_t i = t; i < n; i += kExpandThreads) hd[i] = dst[i];
+        }
+    }
 }
 
 // The member's output is treated as front-padded with zeros to 256 equal
@@ -496,8 +517,8 @@ size_t gpz_inflate_tail_bytes() { return sizeof(InflateTail); }
 uint32_t gpz_inflate_cands() { return gpzi::kCands; }
 
 int gpz_launch_inflate(const uint8_t* in, uint8_t* out, uint32_t* tok, const InflateMember* members,
-                       uint32_t* status, uint32_t* ntok, uint32_t* done, const InflateScratch& sc, uint32_t count,
-                       void* stream, void* const* events) {
+                       uint32_t* status, uint32_t* ntok, uint32_t* done, const InflateScratch& sc, uint8_t* host_out,
+                       uint32_t count, void* stream, void* const* events) {
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     if (!count) return 0;
     int dev = 0, sms = 0;
@@ -510,7 +531,7 @@ int gpz_launch_inflate(const uint8_t* in, uint8_t* out, uint32_t* tok, const Inf
     k_inflate_cand<<<sms * (2048 / kCandThreads), kCandThreads, 0, s>>>(in, members, sc);
     k_inflate_chain<<<count, kCandThreads, 0, s>>>(in, tok, members, status, ntok, done, sc, count);
     k_inflate_tok<<<count, 32, gpzi::kSharedTokBytes, s>>>(in, tok, members, status, ntok, done, count);
-    k_inflate_expand<<<count, kExpandThreads, 0, s>>>(tok, ntok, out, members, status, count);
+    k_inflate_expand<<<count, kExpandThreads, 0, s>>>(tok, ntok, out, members, status, host_out, count);
     k_inflate_crc<<<count, kCrcThreads, 0, s>>>(out, members, status, count);
     if (events) cudaEventRecord(static_cast<cudaEvent_t>(events[1]), s);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;

@@ -177,10 +177,12 @@ struct InflateScratch {
 // remaining member: tokens into tok, indexed like out, and their count into
 // ntok), k_inflate_expand (tokens to bytes), then k_inflate_crc
 // (gpz_inflate.cu); status[m] = 0 or the member's gpzi status code.
-// events: NULL or two cudaEvent_t recorded before and after.
+// host_out: NULL, or a page-locked host buffer (its device address) that
+// receives each member's output as soon as it is expanded.  events: NULL or
+// two cudaEvent_t recorded before and after.
 int gpz_launch_inflate(const uint8_t* in, uint8_t* out, uint32_t* tok, const InflateMember* members,
-                       uint32_t* status, uint32_t* ntok, uint32_t* done, const InflateScratch& sc, uint32_t count,
-                       void* stream, void* const* events);
+                       uint32_t* status, uint32_t* ntok, uint32_t* done, const InflateScratch& sc, uint8_t* host_out,
+                       uint32_t count, void* stream, void* const* events);
 size_t gpz_inflate_tail_bytes();
 uint32_t gpz_inflate_cands();
 size_t gpz_inflate_smem_bytes();

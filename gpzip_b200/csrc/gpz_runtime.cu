@@ -1827,6 +1827,40 @@ uint32_t le32(const uint8_t* p) { return p[0] | (uint32_t)p[1] << 8 | (uint32_t)
 
 // Member boundaries as find_member_starts (parallel_decompress.rs:36-58):
 // every occurrence of the header, scanning on 10 bytes past each one.
+// Every offset at or after byte 10 where the 10-byte header starts, in
+// order.  A long stream is cut into pieces of at least 1 MiB of start
+// offsets, searched on half the host's threads (a search by one thread ran
+// at about 5.7 GB/s, most of an inflate call's host time).
+std::vector<size_t> header_hits(const uint8_t* in, size_t n) {
+    constexpr size_t kPiece = 1u << 20;
+    const size_t span = n - 10;  // start offsets [10, n)
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t pieces = span < 2 * kPiece ? 1 : std::min<size_t>(std::max(1u, hw / 2), span / kPiece);
+    std::vector<std::vector<size_t>> hits(pieces);
+    auto search = [&](size_t k) {
+        // starts in [b, e): the haystack ends 9 bytes past e
+        const size_t b = 10 + span * k / pieces, e = 10 + span * (k + 1) / pieces, end = std::min(n, e + 9);
+        for (size_t p = b; p < e && p + 10 <= end;) {
+            const void* q = memmem(in + p, end - p, kGzipHeader, 10);
+            if (!q) break;
+            const size_t at = static_cast<const uint8_t*>(q) - in;
+            hits[k].push_back(at);
+            p = at + 1;
+        }
+    };
+    if (pieces == 1) {
+        search(0);
+    } else {
+        std::vector<std::thread> th;
+        for (size_t k = 1; k < pieces; k++) th.emplace_back(search, k);
+        search(0);
+        for (auto& t : th) t.join();
+    }
+    std::vector<size_t> all;
+    for (auto& h : hits) all.insert(all.end(), h.begin(), h.end());
+    return all;
+}
+
 int split_members(const uint8_t* in, size_t n, std::vector<InflateMember>* ms, size_t* total, std::string* why) {
     if (ms) ms->clear();
     *total = 0;
@@ -1835,14 +1869,15 @@ int split_members(const uint8_t* in, size_t n, std::vector<InflateMember>* ms, s
         *why = "the stream does not start with gpzip's gzip header";
         return GPZ_E_DATA;
     }
+    // scanning on 10 bytes past each match: of all header occurrences at or
+    // after byte 10, in order, those at least 10 bytes past the last taken
     std::vector<size_t> starts{0};
-    for (size_t p = 10; p + 10 <= n;) {
-        const void* q = memmem(in + p, n - p, kGzipHeader, 10);
-        if (!q) break;
-        const size_t at = static_cast<const uint8_t*>(q) - in;
-        starts.push_back(at);
-        p = at + 10;
-    }
+    size_t p = 10;
+    for (const size_t at : header_hits(in, n))
+        if (at >= p) {
+            starts.push_back(at);
+            p = at + 10;
+        }
     uint64_t out = 0;
     for (size_t i = 0; i < starts.size(); i++) {
         const size_t b = starts[i], e = i + 1 < starts.size() ? starts[i + 1] : n;
@@ -1905,16 +1940,37 @@ int gpz_inflate(gpz_ctx* c, const uint8_t* in, size_t n, uint8_t* out, size_t ou
     if (!c || (!in && n) || !out_len) return GPZ_E_ARG;
     std::lock_guard<std::mutex> lk(c->mu);
     cudaSetDevice(c->device);
+    int rc;
+    if ((rc = settle_stale(c))) return rc;
+    Slot& sl = c->inf;
+    cudaStream_t s = c->kstream;
+    if (!sl.done) CU(c, cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
+    // a page-locked stream starts uploading before the host cuts it into
+    // members; a call that ends early waits for that copy first (bounded),
+    // since it reads the caller's buffer
+    cudaPointerAttributes a{};
+    const bool in_locked = n && cudaPointerGetAttributes(&a, in) == cudaSuccess && a.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+    bool uploading = false;
+    auto end_early = [&](int r) {
+        if (uploading && cudaEventRecord(sl.done, s) == cudaSuccess &&
+            wait_event(c, sl.done, "the upload of a stream that was refused") == GPZ_E_TIMEOUT)
+            sl.stale = true;
+        return r;
+    };
+    if (in_locked) {
+        if ((rc = ensure_dev(c, sl, sl.d_in, n + 16))) return rc;
+        CU(c, cudaMemcpyAsync(sl.d_in.p, in, n, cudaMemcpyHostToDevice, s));
+        uploading = true;
+    }
     std::vector<InflateMember> ms;
     std::string why;
     size_t total = 0;
-    int rc = split_members(in, n, &ms, &total, &why);
+    rc = split_members(in, n, &ms, &total, &why);
     *out_len = total;
-    if (rc) return fail(c, rc, why.c_str());
-    if ((rc = settle_stale(c))) return rc;
-    if (total > out_cap || (!out && total)) return fail(c, GPZ_E_SPACE, "output buffer too small");
-    if (ms.empty()) return GPZ_OK;
-    Slot& sl = c->inf;
+    if (rc) return end_early(fail(c, rc, why.c_str()));
+    if (total > out_cap || (!out && total)) return end_early(fail(c, GPZ_E_SPACE, "output buffer too small"));
+    if (ms.empty()) return end_early(GPZ_OK);
     const size_t nm = ms.size();
     // tokens: at most one per output byte, 4 bytes each; d_cnt holds the
     // members' statuses, their token counts and which members the parallel
@@ -1923,14 +1979,14 @@ int gpz_inflate(gpz_ctx* c, const uint8_t* in, size_t n, uint8_t* out, size_t ou
         (rc = ensure_dev(c, sl, sl.d_tok, (total + 16) * 4)) ||
         (rc = ensure_dev(c, sl, sl.d_members, nm * sizeof(InflateMember))) ||
         (rc = ensure_dev(c, sl, sl.d_cnt, nm * 12)))
-        return rc;
+        return end_early(rc);
     // a tail of b deflate bytes has at most b / 512 + 1 sub-spans of 4096 bits
     const size_t sub_cap = n / 512 + nm + 1;
-    if (sub_cap > 0xFFFFFFFFull / gpz_inflate_cands()) return fail(c, GPZ_E_ARG, "stream too large");
+    if (sub_cap > 0xFFFFFFFFull / gpz_inflate_cands()) return end_early(fail(c, GPZ_E_ARG, "stream too large"));
     if ((rc = ensure_dev(c, sl, sl.d_itail, nm * gpz_inflate_tail_bytes())) ||
         (rc = ensure_dev(c, sl, sl.d_icand, sub_cap * gpz_inflate_cands() * 8)) ||
         (rc = ensure_dev(c, sl, sl.d_isub, sub_cap * 12 + 16)))
-        return rc;
+        return end_early(rc);
     InflateScratch sc{};
     sc.tails = sl.d_itail.p;
     sc.cands = static_cast<uint64_t*>(sl.d_icand.p);
@@ -1941,35 +1997,29 @@ int gpz_inflate(gpz_ctx* c, const uint8_t* in, size_t n, uint8_t* out, size_t ou
     sc.sub_cap = (uint32_t)sub_cap;
     for (auto& e : c->inf_ev)
         if (!e) CU(c, cudaEventCreate(&e));
-    if (!sl.done) CU(c, cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming));
     // member statuses come back through page-locked memory, so the wait for
     // them is the bounded event wait below
-    if ((rc = ensure_host(c, sl, sl.h_err, sl.h_err_cap, nm, false))) return rc;
-    cudaStream_t s = c->kstream;
-    cudaPointerAttributes a{};
-    const bool in_locked = cudaPointerGetAttributes(&a, in) == cudaSuccess && a.type == cudaMemoryTypeHost;
-    cudaGetLastError();
-    if (in_locked) {
-        CU(c, cudaMemcpyAsync(sl.d_in.p, in, n, cudaMemcpyHostToDevice, s));
-    } else {
+    if ((rc = ensure_host(c, sl, sl.h_err, sl.h_err_cap, nm, false))) return end_early(rc);
+    if (!in_locked) {
         if ((rc = ensure_host(c, sl, sl.h_in, sl.h_in_cap, n, false))) return rc;
         copy_pool().run({CopyPool::Copy{sl.h_in, in, n}}, true);
         CU(c, cudaMemcpyAsync(sl.d_in.p, sl.h_in, n, cudaMemcpyHostToDevice, s));
     }
     CU(c, cudaMemcpyAsync(sl.d_members.p, ms.data(), nm * sizeof(InflateMember), cudaMemcpyHostToDevice, s));
+    // a page-locked output buffer receives each member from the expansion
+    // kernel as soon as it is done
+    const bool out_locked = cudaPointerGetAttributes(&a, out) == cudaSuccess && a.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+    uint8_t* host_out = out_locked ? mapped_dev(out) : nullptr;
     if (gpz_launch_inflate(static_cast<const uint8_t*>(sl.d_in.p), static_cast<uint8_t*>(sl.d_out.p),
                            static_cast<uint32_t*>(sl.d_tok.p), static_cast<const InflateMember*>(sl.d_members.p),
                            static_cast<uint32_t*>(sl.d_cnt.p), static_cast<uint32_t*>(sl.d_cnt.p) + nm,
-                           static_cast<uint32_t*>(sl.d_cnt.p) + 2 * nm, sc, (uint32_t)nm, s,
+                           static_cast<uint32_t*>(sl.d_cnt.p) + 2 * nm, sc, host_out, (uint32_t)nm, s,
                            reinterpret_cast<void* const*>(c->inf_ev)) != 0)
         return fail(c, GPZ_E_CUDA, "inflate launch", cudaGetLastError());
-    const bool out_locked = cudaPointerGetAttributes(&a, out) == cudaSuccess && a.type == cudaMemoryTypeHost;
-    cudaGetLastError();
     const uint32_t* status = sl.h_err;
     CU(c, cudaMemcpyAsync(sl.h_err, sl.d_cnt.p, nm * 4, cudaMemcpyDeviceToHost, s));
-    if (out_locked) {
-        CU(c, cudaMemcpyAsync(out, sl.d_out.p, total, cudaMemcpyDeviceToHost, s));
-    } else {
+    if (!host_out) {
         if ((rc = ensure_host(c, sl, sl.h_out, sl.h_out_cap, total, false))) return rc;
         CU(c, cudaMemcpyAsync(sl.h_out, sl.d_out.p, total, cudaMemcpyDeviceToHost, s));
     }
@@ -1985,7 +2035,7 @@ int gpz_inflate(gpz_ctx* c, const uint8_t* in, size_t n, uint8_t* out, size_t ou
                   inflate_reason(status[i]);
             return fail(c, GPZ_E_DATA, why.c_str());
         }
-    if (!out_locked) copy_pool().run({CopyPool::Copy{out, sl.h_out, total}});
+    if (!host_out) copy_pool().run({CopyPool::Copy{out, sl.h_out, total}});
     return GPZ_OK;
 }
 

@@ -238,8 +238,12 @@ GPZ_API uint64_t gpz_last_launches(gpz_ctx* ctx);
  * (crates/gpzip-codec-cpu/src/parallel_decompress.rs:63-113): the stream is
  * cut into members at every occurrence of the fixed 10-byte header that
  * gpzip writes (1f 8b 08 00 00 00 00 00 00 ff, parallel_decompress.rs:29-58),
- * and every member is decoded on the device, one warp each, into its place
- * in the output (offsets from the members' ISIZE trailers).
+ * and every member is decoded on the device into its place in the output
+ * (offsets from the members' ISIZE trailers): a member that is one dynamic
+ * block (every gpzip member) by many threads at once, any other by one warp.
+ * Page-locked input starts uploading while the stream is cut; a page-locked
+ * output buffer receives each member from the device as soon as it is
+ * decoded.
  *
  * gpz_inflate_size: host only, no context.  Scans in[0, n) and returns the
  * member count and the total output size.  GPZ_E_DATA when the stream does
@@ -255,7 +259,8 @@ GPZ_API uint64_t gpz_last_launches(gpz_ctx* ctx);
 GPZ_API int gpz_inflate_size(const uint8_t* in, size_t n, size_t* members, size_t* out_bytes);
 GPZ_API int gpz_inflate(gpz_ctx* ctx, const uint8_t* in, size_t n, uint8_t* out, size_t out_cap,
                         size_t* out_len);
-/* Device time of the last gpz_inflate's kernels (decode and CRC), in ms. */
+/* Device time of the last gpz_inflate's kernels (decode and CRC, and, with
+ * a page-locked output buffer, the members' copies to it), in ms. */
 GPZ_API float gpz_inflate_device_ms(const gpz_ctx* ctx);
 
 /* Largest input gpz_compress_member_static accepts (one 128 KiB member). */

@@ -207,6 +207,58 @@ def test_member_split_and_sizes_on_the_host():
         native.inflate_size(bytes(forged))
 
 
+def split_like_the_reference(buf: bytes):
+    """(members, output bytes) as parallel_decompress.rs:36-58 cuts a stream:
+    every header occurrence, scanning on 10 bytes past each one, then the
+    ISIZE trailers summed; None where gpz_inflate_size must refuse."""
+    from oracle import oracle as O
+    if not buf:
+        return (0, 0)
+    if len(buf) < 18 or buf[:10] != O.GZIP_HEADER:
+        return None
+    starts, p = [0], 10
+    while p + 10 <= len(buf):
+        q = buf.find(O.GZIP_HEADER, p)
+        if q < 0:
+            break
+        starts.append(q)
+        p = q + 10
+    total = 0
+    for i, b in enumerate(starts):
+        e = starts[i + 1] if i + 1 < len(starts) else len(buf)
+        if e - b < 18:
+            return None
+        isize = struct.unpack("<I", buf[e - 4:e])[0]
+        if isize > 1032 * (e - b - 18 + 1):
+            return None
+        total += isize
+    return (len(starts), total)
+
+
+def test_member_split_of_a_long_stream_in_pieces():
+    # streams of several MiB are searched in pieces on several threads;
+    # members of every size, headers right at piece edges (a member every
+    # few hundred bytes in one stretch), and members too short to be valid
+    from gpzip_b200 import native
+    from oracle import oracle as O
+    rng = np.random.default_rng(31)
+
+    def member(n):
+        body = rng.integers(0, 255, n, dtype=np.uint8).tobytes().replace(b"\x1f\x8b", b"\x1f\x8c")
+        return O.GZIP_HEADER + body + struct.pack("<II", 0, min(n, 1000))
+
+    sizes = [int(x) for x in rng.integers(0, 200_000, 60)] + [int(x) for x in rng.integers(0, 600, 4000)]
+    rng.shuffle(sizes)
+    stream = b"".join(member(n) for n in sizes)
+    assert len(stream) > 6 << 20
+    assert native.inflate_size(stream) == split_like_the_reference(stream)
+    # a member shorter than its header and trailer: both refuse
+    bad = stream[:3_000_000] + O.GZIP_HEADER + b"xy" + stream[3_000_000:]
+    assert split_like_the_reference(bad) is None
+    with pytest.raises(native.GpzError):
+        native.inflate_size(bad)
+
+
 @pytest.fixture(scope="module")
 def lanes_decoder(tmp_path_factory):
     cxx = shutil.which("g++")
