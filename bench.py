@@ -297,14 +297,15 @@ def writer_rate(ctx, data, rounds: int = 3):
     for r in range(rounds + 1):
         Count.n = 0
         t0 = _t.perf_counter()
-        with native.Writer(Count(), ctx=ctx, chunk_size=2 << 20, max_in_flight=16) as w:
+        with native.Writer(Count(), ctx=ctx, chunk_size=2 << 20, max_in_flight=16, sink_view=True) as w:
             for i in range(0, len(view), 1 << 20):
                 w.write(view[i:i + (1 << 20)])
         t = _t.perf_counter() - t0
         if r:
             best = t if best is None else min(best, t)
     return {"value": round(len(view) / best / 1e9, 4), "unit": "GB/s", "out_bytes": Count.n,
-            "what": "gpz_writer: 1 MiB writes, 2 MiB chunks, 16 in flight, wall clock"}
+            "what": "gpz_writer: 1 MiB writes, 2 MiB chunks, 16 in flight, wall clock; the sink takes each "
+                    "member run as a view of the library's buffer"}
 
 
 def chunk_fn_rate(ctx, chunks, threads: int = 16, rounds: int = 3):

@@ -522,10 +522,12 @@ class Writer:
     writer takes any ChunkFn, and with `hybrid` (a Hybrid) through the hybrid
     CPU + GPU chunk function; in both, up to `max_in_flight` chunk calls run
     at once on the writer's worker threads.  flush() does not cut a chunk; close() writes the last
-    partial chunk and raises the first error the writer met."""
+    partial chunk and raises the first error the writer met.  With sink_view, dst.write receives a
+    memoryview of the library's buffer instead of a bytes copy; it is valid only during the call, so
+    dst must consume it there (as a file's write does)."""
 
     def __init__(self, dst, ctx: "Context" = None, chunk_fn=None, chunk_size: int = 2 << 20, max_in_flight: int = 16,
-                 hybrid: "Hybrid" = None):
+                 hybrid: "Hybrid" = None, sink_view: bool = False):
         if sum(x is not None for x in (ctx, chunk_fn, hybrid)) != 1:
             raise ValueError("give exactly one of ctx, chunk_fn and hybrid")
         self.L = load()
@@ -536,7 +538,11 @@ class Writer:
 
         def sink(_user, buf, n):
             try:
-                self._dst.write(ctypes.string_at(buf, n))
+                if sink_view:
+                    at = ctypes.cast(buf, ctypes.c_void_p).value
+                    self._dst.write(memoryview((ctypes.c_char * n).from_address(at)).cast("B") if n else b"")
+                else:
+                    self._dst.write(ctypes.string_at(buf, n))
                 return 0
             except Exception as e:  # noqa: BLE001 -- reported by close()
                 self._err = self._err or e

@@ -82,6 +82,30 @@ def test_page_locked_buffers(ctx):
     assert bytes(ctx.inflate(src, out=dst)) == data
 
 
+def test_members_that_do_not_settle_page_locked(ctx):
+    # binary and text members: runs of codes of one length keep speculative
+    # decodes misaligned, so many members go through the tail kernels
+    # (candidate sub-spans and the walk); the output goes straight from the
+    # expansion kernel into the page-locked buffer
+    import torch
+    data = W.binary((8 << 20) + 777, seed=14).tobytes() + W.text(3 << 20, seed=15).tobytes()
+    gz = b"".join(bytes(ctx.compress_chunk(data[o:o + (2 << 20)])) for o in range(0, len(data), 2 << 20))
+    src = torch.empty(len(gz), dtype=torch.uint8, pin_memory=True).numpy()
+    src[:] = np.frombuffer(gz, dtype=np.uint8)
+    dst = torch.empty(len(data), dtype=torch.uint8, pin_memory=True).numpy()
+    for _ in range(2):  # the scratch of the first call is reused by the second
+        dst[:] = 0
+        assert bytes(ctx.inflate(src, out=dst)) == data
+    # a flipped bit inside a binary member's data: that member fails (the
+    # serial decoder gives the status), and the context stays usable
+    bad = bytearray(gz)
+    bad[len(gz) // 3] ^= 0x10
+    with pytest.raises(native.GpzError) as e:
+        ctx.inflate(bytes(bad))
+    assert e.value.status == native.GPZ_E_DATA
+    assert bytes(ctx.inflate(gz)) == data
+
+
 def test_damaged_streams_fail_and_leave_the_context_usable(ctx):
     data = W.text(600_000, seed=12).tobytes()
     gz = bytearray(ctx.compress_chunk(data))

@@ -41,6 +41,23 @@ def test_members_in_input_order(max_in_flight):
     assert gzip.decompress(out.getvalue()) == data
 
 
+def test_sink_view_gives_the_same_stream():
+    # the sink may take each run of members as a view of the library's
+    # buffer (valid during the call) instead of a bytes copy
+    data = W.text(4 * CHUNK + 999, seed=9).tobytes()
+    out, kinds = io.BytesIO(), set()
+
+    class Sink:
+        def write(self, b):
+            kinds.add(type(b).__name__)
+            return out.write(b)
+
+    with native.Writer(Sink(), chunk_fn=oracle_fn, chunk_size=CHUNK, max_in_flight=4, sink_view=True) as w:
+        w.write(data)
+    assert kinds == {"memoryview"}
+    assert out.getvalue() == expected(data, CHUNK)
+
+
 def test_flush_does_not_cut_chunks_and_empty_input_writes_nothing():
     data = W.text(3 * CHUNK - 7, seed=3).tobytes()
     out = io.BytesIO()
