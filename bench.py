@@ -656,7 +656,8 @@ def hybrid_rate(ctx, data, rounds: int = 2, warmup_chunks: int = 4):
         Count.n = 0
         with native.Hybrid(ctx=ctx, gpu_permits=16, warmup_chunks=warmup_chunks) as h:
             t0 = _t.perf_counter()
-            with native.Writer(Count(), hybrid=h, chunk_size=CHUNK, max_in_flight=cpu_workers + 16) as w:
+            with native.Writer(Count(), hybrid=h, chunk_size=CHUNK, max_in_flight=cpu_workers + 16,
+                               sink_view=True) as w:
                 for i in range(0, len(view), 1 << 20):
                     w.write(view[i:i + (1 << 20)])
             t = _t.perf_counter() - t0

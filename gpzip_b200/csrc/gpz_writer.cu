@@ -44,7 +44,27 @@
 #include "gpz.h"
 #include "gpz_stream.h"
 
-using Chunk = std::vector<uint8_t>;
+// An allocator whose resize leaves new bytes uninitialised: a chunk is
+// filled by copies right after it grows, so zeroing it first is wasted.
+template <class T>
+struct UninitAlloc : std::allocator<T> {
+    template <class U>
+    struct rebind {
+        using other = UninitAlloc<U>;
+    };
+    UninitAlloc() = default;
+    template <class U>
+    UninitAlloc(const UninitAlloc<U>&) noexcept {}
+    template <class U>
+    void construct(U* p) noexcept {
+        ::new (static_cast<void*>(p)) U;
+    }
+    template <class U, class... A>
+    void construct(U* p, A&&... a) {
+        ::new (static_cast<void*>(p)) U(std::forward<A>(a)...);
+    }
+};
+using Chunk = std::vector<uint8_t, UninitAlloc<uint8_t>>;
 using Batch = std::vector<Chunk>;
 
 namespace {
@@ -469,7 +489,10 @@ int gpz_writer_write(gpz_writer* w, const uint8_t* buf, size_t n) {
     while (n) {
         if (w->current.capacity() < w->chunk_size) w->fresh_chunk();
         const size_t take = std::min(n, w->chunk_size - w->current.size());
-        w->current.insert(w->current.end(), buf, buf + take);
+        const size_t at = w->current.size();
+        w->current.resize(at + take);  // within its capacity: no reallocation
+        if (take >= (256u << 10)) gpz_parallel_copy(w->current.data() + at, buf, take);
+        else std::memcpy(w->current.data() + at, buf, take);
         buf += take;
         n -= take;
         if (w->current.size() == w->chunk_size) {
