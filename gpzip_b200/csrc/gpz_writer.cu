@@ -491,8 +491,7 @@ int gpz_writer_write(gpz_writer* w, const uint8_t* buf, size_t n) {
         const size_t take = std::min(n, w->chunk_size - w->current.size());
         const size_t at = w->current.size();
         w->current.resize(at + take);  // within its capacity: no reallocation
-        if (take >= (256u << 10)) gpz_parallel_copy(w->current.data() + at, buf, take);
-        else std::memcpy(w->current.data() + at, buf, take);
+        std::memcpy(w->current.data() + at, buf, take);
         buf += take;
         n -= take;
         if (w->current.size() == w->chunk_size) {
