@@ -610,7 +610,7 @@ constexpr uint64_t kParMinSpanBits = 256; // shortest span worth a lane of its o
 // start lies less than that after the first bit; on gpzip's members it lay
 // within 24 bits at 99.8 % of the boundaries, and the walk decodes a
 // sub-span itself where it lies further.
-constexpr uint64_t kSubBits = 4096;
+constexpr uint64_t kSubBits = 2048;
 constexpr uint32_t kCands = 32;
 constexpr uint32_t kMaxSymBits = 48;
 

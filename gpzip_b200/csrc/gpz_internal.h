@@ -161,7 +161,8 @@ struct InflateMember {
 // candidate results per sub-span, three u32 per sub-span (sub_start: the
 // owning tail, until k_inflate_chain puts the chosen start offset there;
 // the token and byte offsets), two counters (tails, sub-spans taken).
-// sub_cap = deflate bytes / 512 + members + 1 sub-spans always suffice.
+// sub_cap = 8 x deflate bytes / gpzi::kSubBits + members + 1 sub-spans
+// always suffice.
 struct InflateScratch {
     void* tails;
     uint64_t* cands;

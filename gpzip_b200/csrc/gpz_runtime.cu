@@ -1980,8 +1980,8 @@ int gpz_inflate(gpz_ctx* c, const uint8_t* in, size_t n, uint8_t* out, size_t ou
         (rc = ensure_dev(c, sl, sl.d_members, nm * sizeof(InflateMember))) ||
         (rc = ensure_dev(c, sl, sl.d_cnt, nm * 12)))
         return end_early(rc);
-    // a tail of b deflate bytes has at most b / 512 + 1 sub-spans of 4096 bits
-    const size_t sub_cap = n / 512 + nm + 1;
+    // a tail of b deflate bytes has at most 8 b / kSubBits + 1 sub-spans
+    const size_t sub_cap = n * 8 / gpzi::kSubBits + nm + 1;
     if (sub_cap > 0xFFFFFFFFull / gpz_inflate_cands()) return end_early(fail(c, GPZ_E_ARG, "stream too large"));
     if ((rc = ensure_dev(c, sl, sl.d_itail, nm * gpz_inflate_tail_bytes())) ||
         (rc = ensure_dev(c, sl, sl.d_icand, sub_cap * gpz_inflate_cands() * 8)) ||
