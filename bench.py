@@ -797,7 +797,9 @@ def main():
 
     cpu = None
     zl = None
-    if rank == 0 and not (args.no_cpu or args.device_only):
+    # the CPU baselines, serving and the uneven-file comparison are
+    # single-GPU measurements: taken at N=1 only
+    if rank == 0 and world == 1 and not (args.no_cpu or args.device_only):
         threads = os.cpu_count() or 1
         r, cr, nb = cpu_port_rate(data, args.cpu_sample_mib, threads)
         cpu = {"value": round(r, 5), "unit": "GB/s", "cores": threads, "kind": "port",
@@ -837,14 +839,14 @@ def main():
             del cdata
 
     serving = None
-    if rank == 0 and args.serve_seconds > 0 and not args.device_only:
+    if rank == 0 and world == 1 and args.serve_seconds > 0 and not args.device_only:
         rates = [int(x) for x in args.serve_rates.split(",") if x]
         serving = run_serving(local, args.serve_seconds, rates)
 
     # the 1,000-file uneven mix: batched persistent path vs the plain
     # one-launch-per-chunk path through the host API
     uneven = None
-    if rank == 0 and not (args.device_only or args.no_uneven):
+    if rank == 0 and world == 1 and not (args.device_only or args.no_uneven):
         uctx = native.Context(device=local, member_bytes=MEMBER)
         uneven = run_uneven(uctx, argparse.Namespace(steps=2, warmup=1), torch.cuda.current_stream())
         uctx.close()
