@@ -6,6 +6,11 @@
 //     matches and flushing output.
 //   * host C++ (NL = 1): the same code on one thread, which the CPU tests
 //     check against zlib.
+// The decoder writes bytes, or (the token form) the member's tokens, which
+// the device expands into bytes in a kernel of its own.  The second half of
+// this file holds the parallel decode of a member that is one dynamic block
+// (decode_span and its helpers; inflate_member_par runs its steps on the
+// host for the tests), which the device uses for gpzip's members.
 //
 // It replaces, for gpzip-written archives, the per-member GzDecoder of
 // crates/gpzip-codec-cpu/src/parallel_decompress.rs:63-113 (flate2).  The
